@@ -1,0 +1,247 @@
+/*
+ * nuppn.h -- C ABI of the B200 reaction-network solver.
+ *
+ * Drop-in boundary for NuPPN's per-zone network integration. The reference's Fortran frames call
+ *   evaluate_all_rates(ye, nvar, nvrel, rho, t9, yps, nu)                 physics/source/evaluate_rates.F90:14
+ *   integrate_network(nvar, yps, t9_0, t9_1, rho_0, rho_1, ye, dtwant, nvrel, nu, ierr)
+ *                                                                          solver/source/solver.F90:53
+ * once per zone (ppn.F90:298-301, mppnp.F90:719-724, tppnp.F90:152-154). Those routines read the
+ * network from module globals (rates::v, k1..k8, nuc_data masks, /cnetw/ A and Z, the REACLIB and
+ * weak-rate tables, jac_rhs::dns2csr_map). Here the network is handed over once, as a descriptor of
+ * plain arrays in the reference's slot layout, and every entry point is batched over zones.
+ *
+ * Conventions
+ *   - Species and reaction slots keep the reference's order; indices are 0-based (Fortran index - 1).
+ *   - The library owns device memory; the caller owns every host buffer passed in.
+ *   - No entry point exits or stops: problems come back as a nuppn_status, per-zone solver outcomes as
+ *     the reference's error codes (utils/source/errors.F90:5-21) in ierr[].
+ *   - Abundance arrays are zone-major: X[z * ldx + i] is species i of zone z (ldx >= nsp).
+ *   - Entry points are not re-entrant on the same nuppn_net (one host thread per handle), like the
+ *     reference's module state.
+ */
+#ifndef NUPPN_H
+#define NUPPN_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NUPPN_ABI_VERSION 1
+
+typedef enum {
+  NUPPN_OK = 0,
+  NUPPN_ERR_ARG = -1,      /* bad argument or descriptor                                 */
+  NUPPN_ERR_CUDA = -2,     /* a CUDA runtime call failed                                 */
+  NUPPN_ERR_NOMEM = -3,    /* device or host allocation failed                           */
+  NUPPN_ERR_NET = -4,      /* network inconsistent (e.g. k index out of range)           */
+  NUPPN_ERR_LIMIT = -5,    /* size beyond a compiled limit                               */
+  NUPPN_ERR_NODEV = -6,    /* no usable sm_100 device                                    */
+  NUPPN_ERR_TIMEOUT = -7   /* a bounded device wait ran out                              */
+} nuppn_status;
+
+/* Per-zone solver outcome codes: utils/source/errors.F90:5-21 (0 = success). */
+#define NUPPN_SLV_CNVRG    1
+#define NUPPN_MAX_SUBSTEPS 2
+#define NUPPN_BAD_STEP     3
+#define NUPPN_NEG_ABUNDS   4
+#define NUPPN_HUGE_ABUNDS  5
+#define NUPPN_SUM_X        6
+#define NUPPN_GOT_NAN      7
+#define NUPPN_BAD_YE       8
+#define NUPPN_NSE_CNVRG    9
+#define NUPPN_NSE_WEAK     10
+#define NUPPN_SMALL_DT     11
+#define NUPPN_BAD_INPUT    20  /* T9/rho not finite or not positive (the reference would stop) */
+
+/* Rate sources of a reaction slot (the label lab(nre) of reaction_info.F90:53-56, reduced to what
+ * decides how the rate is computed; ppn_physics.F90:550-589 gathers by the same label). */
+enum {
+  NUPPN_SRC_NONE = 0,      /* rate 0 (slot unused)                                        */
+  NUPPN_SRC_VITAL = 1,     /* analytic template (vital.F90:239-2209)                      */
+  NUPPN_SRC_REACLIB = 2,   /* REACLIB rate (reaclib.F90:431-582)                          */
+  NUPPN_SRC_NETGEN = 3,    /* NETGEN table (netgen.F90:179-310)                           */
+  NUPPN_SRC_FULLER = 4,    /* FFN 2-D table (fuller.F90:92-122)                           */
+  NUPPN_SRC_KADONIS = 5,   /* KADoNiS (n,g) table, Akima in kT (kadonis.F90:150-187)      */
+  NUPPN_SRC_CONST = 6      /* constant rate (alpha decays, alpha_decays.F90)              */
+};
+
+/* Solver and physics knobs on the path: &ppn_solver defaults of solver_knobs.F90:43-57 and the
+ * physics_knobs.F90 switches that evaluate_all_rates reads. */
+typedef struct nuppn_knobs {
+  int32_t ittd;                /* max Newton iterations (6)                                   */
+  int32_t integration_method;  /* 0 = backward Euler + Newton, 1 = Bader-Deuflhard           */
+  int32_t max_sub_steps;       /* 4000                                                        */
+  int32_t interpolate_temp;    /* 1                                                           */
+  int32_t interpolate_dens;    /* 1                                                           */
+  int32_t screen_option;       /* 0 none, 2 Chugunov-DeWitt-Yakovlev 2007                     */
+  int32_t detailed_balance;    /* 1                                                           */
+  int32_t weak_rates;          /* 1                                                           */
+  int32_t strong_rates;        /* 1                                                           */
+  int32_t decay;               /* 0                                                           */
+  int32_t i_nse;               /* 0                                                           */
+  int32_t nse_weak_method;     /* 1 = Cash-Karp RK, 0 = Euler                                 */
+  double dgrd;                 /* 1e-3                                                        */
+  double grdthreshold;         /* 1e-15                                                       */
+  double cyminformal;          /* 1e-30                                                       */
+  double min_rate_ov_dt;       /* 1e-99                                                       */
+  double min_t9_for_slv;       /* 0.01                                                        */
+  double delta_state_max;      /* 1e99                                                        */
+  double nse_min_t9;           /* 6                                                           */
+  /* device-only choices (no reference counterpart) */
+  int32_t lu_precision;        /* 0 = FP64 factor, 1 = FP32 factor + FP64 iterative refinement */
+  int32_t ir_max_iters;        /* refinement sweeps per solve in mode 1 (default 3)           */
+  double ir_rtol;              /* refinement stops when |dx| <= ir_rtol*|x| (default 1e-14)   */
+  int32_t threads_per_zone;    /* CTA size (0 = library choice)                               */
+  int32_t reserved[7];
+} nuppn_knobs;
+
+/* Network description in the reference's slot layout (what rnetw2007, reaclib_init, netgen_init,
+ * fuller_init, kadonis_init and reverse_init leave in module state). Array extents in brackets. */
+typedef struct nuppn_net_desc {
+  int32_t nsp, nre;
+  int32_t igamma;                    /* slot of 'OOOOO' (jac_rhs.F90:52-58)                      */
+  const double *anetw, *znetw;       /* [nsp] A and Z, COMMON /cnetw/                            */
+  const uint8_t *considerisotope;    /* [nsp]                                                    */
+  const double *exmass;              /* [nsp] mass excess (MeV): masses/Q of nse_swj.F90:186-196 */
+  const double *gspin;               /* [nsp] 2J+1                                               */
+  const int32_t *spec_part;          /* [nsp] partition-function row or -1                       */
+  const int32_t *k;                  /* [nre][8] k1..k8 (rates.F90:15)                           */
+  const int32_t *ilabb;              /* [nre] reaction type 1..22 (reaction_info.F90:8-34)      */
+  const uint8_t *considerreaction;   /* [nre]                                                    */
+  const double *rfac;                /* [nre] rate factors (evaluate_rates.F90:195)              */
+  const int32_t *src, *src_idx;      /* [nre] rate source and index in that source              */
+  const int32_t *irev;               /* [nre] detailed-balance partner or -1 (reverse.F90:13)   */
+  /* REACLIB: contributions (a0..a6) summed into rates (reaclib.F90:478-498) */
+  int32_t rl_ncontrib, rl_nrate;
+  const double *rl_a;                /* [ncontrib][7]                                            */
+  const int32_t *rl_rate;            /* [ncontrib] rate index, non-decreasing                    */
+  const int32_t *rl_chapter;         /* [nrate] 1..11                                            */
+  const uint8_t *rl_vflag;           /* [nrate] rflag2 == 'v'                                    */
+  const uint8_t *rl_ecflag;          /* [nrate] rrlreac == '  ec'                                */
+  const int32_t *rl_nireac;          /* [nrate] reaction type used for the density factor       */
+  const int32_t *rl_part;            /* [nrate][6] partition-function rows (-1 -> 1.0)           */
+  int32_t npart;
+  const double *part_t9;             /* [24] temperature grid                                    */
+  const double *part_val;            /* [npart][24]                                              */
+  /* VITAL analytic templates: v = rho^dpow * xfac * sum c*T9^p*exp(d*T9^(-1/3) + f/T9 + g*T9) */
+  int32_t vt_nrate, vt_nterm;
+  const int32_t *vt_first;           /* [nrate+1]                                                */
+  const double *vt_terms;            /* [nterm][5] (c, p, d, f, g)                               */
+  const double *vt_dpow;             /* [nrate]                                                  */
+  const int32_t *vt_xfac;            /* [nrate] species for the 0.5*(1+X) factor, or -1          */
+  /* NETGEN beta table (netgen.F90:179-310) */
+  int32_t ng_kgrid, ng_nreac, ng_ndmax;
+  const double *ng_t8;               /* [kgrid]                                                  */
+  const double *ng_flag;             /* [nreac]                                                  */
+  const int32_t *ng_ndata;           /* [nreac]                                                  */
+  const double *ng_ane;              /* [nreac][ndmax]                                           */
+  const double *ng_l10v;             /* [kgrid][nreac][ndmax]                                    */
+  /* FFN table (fuller.F90:92-122) */
+  int32_t ff_nv, ff_nt, ff_nr;
+  const double *ff_t9coo, *ff_rhocoo;/* [nt], [nr] (log10 T9, log10 rho*Ye)                      */
+  const double *ff_l10v;             /* [nv][nt][nr]                                             */
+  /* KADoNiS (kadonis.F90:150-187) */
+  int32_t kd_n, kd_ne;
+  const double *kd_e;                /* [ne] keV                                                 */
+  const double *kd_rate;             /* [n][ne]                                                  */
+  /* constant rates */
+  int32_t nconst;
+  const double *const_rate;          /* [nconst]                                                 */
+} nuppn_net_desc;
+
+typedef struct nuppn_net nuppn_net;
+
+typedef struct nuppn_net_info {
+  int32_t nsp, nre;                  /* slots                                                    */
+  int32_t nspec_active, nreac_active;/* considered species / reactions                           */
+  int32_t nnz_jac;                   /* nonzeros of the static Jacobian (jac_rhs.F90:504)       */
+  int32_t nnz_lu;                    /* nonzeros of the filled pattern after symbolic analysis   */
+  int32_t n_solve;                   /* order of the device system (considered, non-gamma)       */
+  int32_t levels_lower, levels_upper;/* dependency levels of the triangular solves               */
+  int64_t lu_flops;                  /* multiply-adds of one numeric factorization              */
+  int64_t device_bytes;              /* device memory held by the handle                        */
+} nuppn_net_info;
+
+/* Per-zone counters of one nuppn_integrate call (solver_diagnostics.F90) */
+typedef struct nuppn_zone_stats {
+  int32_t nsucc;          /* accepted sub-steps                                                   */
+  int32_t nfail;          /* rejected sub-steps                                                   */
+  int32_t newton_iters;   /* total Newton iterations (BE) or sub-steps (BD)                       */
+  int32_t nfact;          /* numeric factorizations                                               */
+  int32_t nsolve;         /* triangular solve pairs                                               */
+  int32_t nvar1_last;     /* species in the last dynamic-network solve                            */
+  int32_t ir_sweeps;      /* refinement sweeps (mixed precision)                                  */
+  int32_t reserved;
+} nuppn_zone_stats;
+
+/* -- library --------------------------------------------------------------------------------- */
+int32_t nuppn_abi_version(void);
+void nuppn_default_knobs(nuppn_knobs *knobs);
+const char *nuppn_status_string(nuppn_status s);
+/* Device status of the last failing CUDA call (human-readable, static storage). */
+const char *nuppn_last_error(void);
+
+/* Network set-up: replaces the init chain of ppn.F90:80-209 that fills module state, plus makemap
+ * (jac_rhs.F90:461-540) and the one-time symbolic analysis that takes the place of SuperLU's
+ * per-call COLAMD/symbolic work (c_fortran_dgssv.c:110-119). */
+nuppn_status nuppn_net_create(const nuppn_net_desc *desc, const nuppn_knobs *knobs, int32_t device,
+                              nuppn_net **out);
+nuppn_status nuppn_net_destroy(nuppn_net *net);
+nuppn_status nuppn_net_info_get(const nuppn_net *net, nuppn_net_info *info);
+nuppn_status nuppn_set_knobs(nuppn_net *net, const nuppn_knobs *knobs);
+
+/* Static Jacobian pattern of makemap (jac_rhs.F90:461-540): row/col (0-based) of each COO entry in
+ * the reference's row-major numbering, and dns2csr_map[nre][8] (entry index per slot, -1 if the
+ * reaction is not considered). Sizes: row/col [nnz_jac]. */
+nuppn_status nuppn_jac_pattern(const nuppn_net *net, int32_t *row, int32_t *col, int32_t *dns2csr_map);
+
+/* evaluate_all_rates (evaluate_rates.F90:14-174) for nz zones: v[z*nre + r]. Host buffers. */
+nuppn_status nuppn_eval_rates(nuppn_net *net, int32_t nz, const double *t9, const double *rho,
+                              const double *ye, const double *X, int32_t ldx, double *v);
+
+/* calculate_dxdt (jac_rhs.F90:217-278) from given rates: dxdt[z*nsp + i]. */
+nuppn_status nuppn_dxdt(nuppn_net *net, int32_t nz, const double *v, const double *X, int32_t ldx,
+                        double *dxdt);
+
+/* calculate_jacobian (jac_rhs.F90:282-455) from given rates at step dt: jac values [z*nnz_jac + e]
+ * (before the -dt scaling), entry set flags (row(e) /= -1) and the dynamic-network mask [z*nsp+i]. */
+nuppn_status nuppn_jacobian(nuppn_net *net, int32_t nz, const double *v, const double *X, int32_t ldx,
+                            const double *dt, double *jac, uint8_t *entry_set, uint8_t *mask);
+
+/* One linear solve per zone of the reduced system that newton_iteration builds
+ * (backward_euler.F90:133-148): (I - dt*J) x = b restricted to the mask, with the entry set flags
+ * of nuppn_jacobian; x[z*nsp+i] = 0 for unmasked species. jac as returned by nuppn_jacobian. */
+nuppn_status nuppn_solve_reduced(nuppn_net *net, int32_t nz, const double *jac,
+                                 const uint8_t *entry_set, const uint8_t *mask, const double *dt,
+                                 const double *b, double *x);
+
+/* integrate_network (solver.F90:53-238), batched: every zone z advances X[z*ldx + :] over
+ * dtwant[z] with its own sub-steps; ye[z] is updated; ierr[z] gets the reference's code. Rates are
+ * evaluated at entry (the frames call evaluate_all_rates right before integrate_network) and again
+ * whenever the interval-mean T9 or rho changes (solver.F90:146-150). stats may be NULL.
+ * bd_state[z] carries what the reference keeps in saved module variables between calls of one
+ * process: the Bader-Deuflhard optimal column kopt (bader_deuflhard.F90:32) and the first-call flag
+ * frst (solver.F90:80). 0 = a fresh zone (frst true for its first sub-step, kopt from
+ * bader_deuflhard_init); the call writes back the value to pass next time. May be NULL (all fresh). */
+nuppn_status nuppn_integrate(nuppn_net *net, int32_t nz, double *X, int32_t ldx, const double *t9_0,
+                             const double *t9_1, const double *rho_0, const double *rho_1, double *ye,
+                             const double *dtwant, int32_t *ierr, nuppn_zone_stats *stats,
+                             int32_t *bd_state);
+
+/* Same on device-resident buffers (pointers from cudaMalloc in the caller's context) on the given
+ * cudaStream_t (passed as void*; NULL = legacy default stream). Asynchronous: returns after launch. */
+nuppn_status nuppn_integrate_device(nuppn_net *net, int32_t nz, double *d_X, int32_t ldx,
+                                    const double *d_t9_0, const double *d_t9_1, const double *d_rho_0,
+                                    const double *d_rho_1, double *d_ye, const double *d_dtwant,
+                                    int32_t *d_ierr, nuppn_zone_stats *d_stats, int32_t *d_bd_state,
+                                    void *stream);
+
+/* Number of kernel launches issued by the library since the handle was created. */
+int64_t nuppn_launch_count(const nuppn_net *net);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NUPPN_H */
