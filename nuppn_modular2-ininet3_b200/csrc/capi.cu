@@ -1,0 +1,483 @@
+// capi.cu -- implementation of the C ABI declared in include/nuppn.h.
+//
+// The handle owns: the host analysis (HostNet), one device arena with every zone-shared network
+// array (DevNet points into it), and a workspace of one slab per resident CTA. Host-buffer entry
+// points stage their arguments through device buffers owned by the handle.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "net_host.h"
+#include "nuppn_internal.h"
+
+namespace nuppn {
+cudaError_t launch_integrate(const DevNet &N, const WsLayout &L, char *ws, int grid, int block,
+                             const IntegrateArgs &A, cudaStream_t st);
+cudaError_t launch_phase(const DevNet &N, const WsLayout &L, char *ws, int grid, int block, const PhaseArgs &A,
+                         cudaStream_t st);
+cudaError_t occupancy_integrate(int block, int *per_sm);
+}  // namespace nuppn
+
+using namespace nuppn;
+
+namespace {
+std::mutex g_err_mu;
+std::string g_last_error;
+
+void set_error(const std::string &s) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  g_last_error = s;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct DevBuf {  // grow-only device buffer
+  void *p = nullptr;
+  size_t n = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= n) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaSuccess) n = bytes;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+}  // namespace
+
+struct nuppn_net {
+  HostNet H;
+  DevNet D;
+  void *arena = nullptr;
+  size_t arena_bytes = 0;
+  WsLayout L;
+  DevBuf ws, stage, counter;
+  int ws_slots = 0;
+  int block = 256;
+  int device = 0;
+  int nsm = 0;
+  int64_t launches = 0;
+};
+
+#define CK(call)                                                                                  \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess) {                                                                      \
+      set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                              \
+      return NUPPN_ERR_CUDA;                                                                      \
+    }                                                                                             \
+  } while (0)
+
+namespace {
+
+// ---- arena upload ------------------------------------------------------------------------------
+struct Arena {
+  std::vector<std::pair<const void *, size_t>> items;
+  std::vector<size_t> offs;
+  size_t total = 0;
+  template <class T>
+  size_t add(const std::vector<T> &v) {
+    size_t off = total;
+    items.push_back({v.data(), v.size() * sizeof(T)});
+    offs.push_back(off);
+    total = align256(total + std::max<size_t>(v.size() * sizeof(T), 1));
+    return off;
+  }
+};
+
+nuppn_status upload(nuppn_net *net) {
+  HostNet &H = net->H;
+  DevNet &D = net->D;
+  Arena A;
+  // record offsets in a fixed sequence, then resolve to pointers
+  std::vector<size_t> o;
+  auto P = [&](auto &vec) { o.push_back(A.add(vec)); };
+  P(H.an); P(H.zn); P(H.ciso); P(H.spart); P(H.gspin_nse);
+  P(H.src); P(H.sidx); P(H.rfac); P(H.crea); P(H.rev_target); P(H.ilabb); P(H.scr_mode); P(H.scr_z1); P(H.scr_z2);
+  P(H.irev); P(H.rev_sp); P(H.rev_kind); P(H.rev_mc); P(H.rev_Q);
+  P(H.act_slot); P(H.act_k); P(H.act_ice);
+  P(H.rl_first); P(H.rl_a); P(H.rl_info); P(H.rl_part); P(H.pt9); P(H.pval);
+  P(H.vfirst); P(H.vxfac); P(H.vterms); P(H.vdpow);
+  P(H.ngt8); P(H.ngl10t8); P(H.ngflag); P(H.ngane); P(H.ngl10v); P(H.ngndata);
+  P(H.fft9); P(H.ffrho); P(H.ffl10v); P(H.kdE); P(H.kdcoef); P(H.constr);
+  P(H.jrow); P(H.jcol); P(H.jdiag); P(H.jg_ptr); P(H.jg_item); P(H.dg_ptr); P(H.dg_item); P(H.dg_coef);
+  P(H.jg_long); P(H.dg_long);
+  P(H.sys_of_sp); P(H.sp_of_sys); P(H.pos_of_entry); P(H.lu_rowptr); P(H.lu_diag); P(H.lu_col); P(H.upd_start);
+  P(H.upd_off); P(H.lvL_ptr); P(H.lvL_rows); P(H.lvL_grp); P(H.lvU_ptr); P(H.lvU_rows); P(H.lvU_grp);
+  CK(cudaMalloc(&net->arena, A.total));
+  net->arena_bytes = A.total;
+  std::vector<char> host(A.total, 0);
+  for (size_t i = 0; i < A.items.size(); ++i)
+    if (A.items[i].second) memcpy(host.data() + A.offs[i], A.items[i].first, A.items[i].second);
+  CK(cudaMemcpy(net->arena, host.data(), A.total, cudaMemcpyHostToDevice));
+  char *b = (char *)net->arena;
+  size_t q = 0;
+  auto nx = [&]() { return (void *)(b + o[q++]); };
+  memset(&D, 0, sizeof(D));
+  D.an = (const double *)nx(); D.zn = (const double *)nx(); D.ciso = (const uint8_t *)nx(); D.spart = (const int *)nx();
+  D.gspin_nse = (const double *)nx();
+  D.src = (const int *)nx(); D.sidx = (const int *)nx(); D.rfac = (const double *)nx(); D.crea = (const uint8_t *)nx();
+  D.rev_target = (const uint8_t *)nx(); D.ilabb = (const int *)nx(); D.scr_mode = (const int *)nx();
+  D.scr_z1 = (const double *)nx(); D.scr_z2 = (const double *)nx();
+  D.irev = (const int *)nx(); D.rev_sp = (const int *)nx(); D.rev_kind = (const int *)nx();
+  D.rev_mc = (const double *)nx(); D.rev_Q = (const double *)nx();
+  D.act_slot = (const int *)nx(); D.act_k = (const int *)nx(); D.act_ice = (const int *)nx();
+  D.rl_first = (const int *)nx(); D.rl_a = (const double *)nx(); D.rl_info = (const int *)nx();
+  D.rl_part = (const int *)nx(); D.pt9 = (const double *)nx(); D.pval = (const double *)nx();
+  D.vfirst = (const int *)nx(); D.vxfac = (const int *)nx(); D.vterms = (const double *)nx(); D.vdpow = (const double *)nx();
+  D.ngt8 = (const double *)nx(); D.ngl10t8 = (const double *)nx(); D.ngflag = (const double *)nx();
+  D.ngane = (const double *)nx(); D.ngl10v = (const double *)nx(); D.ngndata = (const int *)nx();
+  D.fft9 = (const double *)nx(); D.ffrho = (const double *)nx(); D.ffl10v = (const double *)nx();
+  D.kdE = (const double *)nx(); D.kdcoef = (const double *)nx(); D.constr = (const double *)nx();
+  D.jrow = (const int *)nx(); D.jcol = (const int *)nx(); D.jdiag = (const int *)nx();
+  D.jg_ptr = (const int *)nx(); D.jg_item = (const int *)nx(); D.dg_ptr = (const int *)nx();
+  D.dg_item = (const int *)nx(); D.dg_coef = (const double *)nx();
+  D.jg_long = (const int *)nx(); D.dg_long = (const int *)nx();
+  D.sys_of_sp = (const int *)nx(); D.sp_of_sys = (const int *)nx(); D.pos_of_entry = (const int *)nx();
+  D.lu_rowptr = (const int *)nx(); D.lu_diag = (const int *)nx(); D.lu_col = (const int *)nx();
+  D.upd_start = (const int *)nx(); D.upd_off = (const uint16_t *)nx();
+  D.lvL_ptr = (const int *)nx(); D.lvL_rows = (const int *)nx(); D.lvL_grp = (const int *)nx();
+  D.lvU_ptr = (const int *)nx(); D.lvU_rows = (const int *)nx(); D.lvU_grp = (const int *)nx();
+  // scalars
+  D.nsp = H.nsp; D.nre = H.nre; D.nact = H.nact; D.ig = H.ig; D.nsys = H.nsys; D.nnzJ = H.nnzJ; D.nnzLU = H.nnzLU;
+  D.ihe4 = H.ihe4; D.ibe8 = H.ibe8;
+  D.nc = H.nc; D.nr = H.nr; D.npart = H.npart; D.nv = H.nv;
+  D.ngk = H.ngk; D.ngn = H.ngn; D.ngd = H.ngd; D.ffv = H.ffv; D.fft = H.fft; D.ffr = H.ffr;
+  D.kdn = H.kdn; D.kde = H.kde;
+  D.njg_long = (int)H.jg_long.size(); D.ndg_long = (int)H.dg_long.size();
+  D.nlvL = (int)H.lvL_ptr.size() - 1; D.nlvU = (int)H.lvU_ptr.size() - 1;
+  memcpy(D.nseq, H.nseq, sizeof(D.nseq));
+  memcpy(D.bd_a, H.bd_a, sizeof(D.bd_a));
+  memcpy(D.alf, H.alf, sizeof(D.alf));
+  D.kmax = H.kmax; D.kopt0 = H.kopt0;
+  D.kn = H.kn;
+  D.nvar = H.nvar;
+  return NUPPN_OK;
+}
+
+WsLayout layout(const HostNet &H) {
+  WsLayout L;
+  size_t t = 0;
+  auto take = [&](size_t bytes) { size_t o = t; t = align256(t + std::max<size_t>(bytes, 8)); return o; };
+  const size_t d = sizeof(double);
+  L.v = take(H.nre * d); L.rv = take(H.nr * d); L.ngv = take(H.ngn * d); L.ffv = take(H.ffv * d);
+  L.kdv = take(H.kdn * d); L.partinter = take(H.npart * d); L.G = take(H.nsp * d); L.flux = take(H.nact * d);
+  L.contrib = take(std::max<size_t>((size_t)H.nact * 8, H.nre) * d); L.first_l = take(H.nsp * sizeof(int));
+  L.eset = take(H.nnzJ); L.jac = take(H.nnzJ * d); L.mask = take(H.nsp); L.xn = take(H.nsp * d);
+  L.dxdt = take(H.nsp * d); L.y = take(H.nsp * d); L.y_old = take(H.nsp * d); L.y_cur = take(H.nsp * d);
+  L.y_new = take(H.nsp * d); L.y_k = take(H.nsp * d); L.delta_k = take(H.nsp * d); L.y_ext = take(H.nsp * d);
+  L.yscal = take(H.nsp * d); L.qcol = take((size_t)(kMaxLevels + 1) * H.nsp * d);
+  L.yerr = take((size_t)(kMaxLevels + 1) * H.nsp * d); L.lu = take((size_t)H.nnzLU * d);
+  L.bsys = take(H.nsys * d); L.xsys = take(H.nsys * d); L.rhs = take(H.nsp * d);
+  L.bytes = t;
+  return L;
+}
+
+nuppn_status ensure_ws(nuppn_net *net, int slots) {
+  if (slots <= net->ws_slots) return NUPPN_OK;
+  CK(net->ws.ensure((size_t)slots * net->L.bytes));
+  net->ws_slots = slots;
+  return NUPPN_OK;
+}
+
+int resident_slots(nuppn_net *net) {
+  int per = 0;
+  if (occupancy_integrate(net->block, &per) != cudaSuccess || per <= 0) per = 1;
+  return per * net->nsm;
+}
+
+nuppn_status check_zone_args(nuppn_net *net, int nz, int ldx) {
+  if (!net) { set_error("null handle"); return NUPPN_ERR_ARG; }
+  if (nz < 0) { set_error("nz < 0"); return NUPPN_ERR_ARG; }
+  if (ldx < net->H.nsp) { set_error("ldx < nsp"); return NUPPN_ERR_ARG; }
+  return NUPPN_OK;
+}
+
+// stage host arrays into the handle's device staging buffer
+struct Stager {
+  std::vector<std::pair<size_t, size_t>> parts;  // (offset, bytes)
+  size_t total = 0;
+  size_t add(size_t bytes) {
+    size_t o = total;
+    total = align256(total + std::max<size_t>(bytes, 8));
+    return o;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+int32_t nuppn_abi_version(void) { return NUPPN_ABI_VERSION; }
+
+void nuppn_default_knobs(nuppn_knobs *k) {
+  if (!k) return;
+  memset(k, 0, sizeof(*k));
+  k->ittd = 6; k->integration_method = 0; k->max_sub_steps = 4000;
+  k->interpolate_temp = 1; k->interpolate_dens = 1; k->screen_option = 2; k->detailed_balance = 1;
+  k->weak_rates = 1; k->strong_rates = 1; k->decay = 0; k->i_nse = 0; k->nse_weak_method = 1;
+  k->dgrd = 1.e-3; k->grdthreshold = 1.e-15; k->cyminformal = 1.0e-30; k->min_rate_ov_dt = 1.e-99;
+  k->min_t9_for_slv = 0.01; k->delta_state_max = 1.e99; k->nse_min_t9 = 6.0;
+  k->lu_precision = 0; k->ir_max_iters = 3; k->ir_rtol = 1e-14; k->threads_per_zone = 0;
+}
+
+const char *nuppn_status_string(nuppn_status s) {
+  switch (s) {
+    case NUPPN_OK: return "ok";
+    case NUPPN_ERR_ARG: return "bad argument";
+    case NUPPN_ERR_CUDA: return "CUDA error";
+    case NUPPN_ERR_NOMEM: return "out of memory";
+    case NUPPN_ERR_NET: return "inconsistent network";
+    case NUPPN_ERR_LIMIT: return "size limit";
+    case NUPPN_ERR_NODEV: return "no sm_100 device";
+    case NUPPN_ERR_TIMEOUT: return "device wait timed out";
+  }
+  return "unknown";
+}
+
+const char *nuppn_last_error(void) {
+  static thread_local std::string copy;
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  copy = g_last_error;
+  return copy.c_str();
+}
+
+nuppn_status nuppn_net_create(const nuppn_net_desc *desc, const nuppn_knobs *knobs, int32_t device, nuppn_net **out) {
+  if (!desc || !out) { set_error("null argument"); return NUPPN_ERR_ARG; }
+  *out = nullptr;
+  nuppn_knobs kn;
+  if (knobs) kn = *knobs; else nuppn_default_knobs(&kn);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0) {
+    set_error("no CUDA device");
+    return NUPPN_ERR_NODEV;
+  }
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10) { set_error("device is not sm_100 or newer"); return NUPPN_ERR_NODEV; }
+  CK(cudaSetDevice(device));
+  nuppn_net *net = new (std::nothrow) nuppn_net();
+  if (!net) return NUPPN_ERR_NOMEM;
+  std::string msg = build_host_net(*desc, kn, net->H);
+  if (!msg.empty()) {
+    set_error(msg);
+    delete net;
+    return NUPPN_ERR_NET;
+  }
+  net->device = device;
+  net->nsm = prop.multiProcessorCount;
+  net->block = kn.threads_per_zone > 0 ? kn.threads_per_zone : 256;
+  if (net->block % 32 || net->block > 256) { delete net; set_error("threads_per_zone must be a multiple of 32, <= 256"); return NUPPN_ERR_ARG; }
+  nuppn_status st = upload(net);
+  if (st != NUPPN_OK) { delete net; return st; }
+  net->L = layout(net->H);
+  if (net->counter.ensure(256) != cudaSuccess) { delete net; set_error("counter alloc"); return NUPPN_ERR_NOMEM; }
+  *out = net;
+  return NUPPN_OK;
+}
+
+nuppn_status nuppn_net_destroy(nuppn_net *net) {
+  if (!net) return NUPPN_OK;
+  cudaSetDevice(net->device);
+  if (net->arena) cudaFree(net->arena);
+  net->ws.release();
+  net->stage.release();
+  net->counter.release();
+  delete net;
+  return NUPPN_OK;
+}
+
+nuppn_status nuppn_net_info_get(const nuppn_net *net, nuppn_net_info *info) {
+  if (!net || !info) return NUPPN_ERR_ARG;
+  const HostNet &H = net->H;
+  info->nsp = H.nsp; info->nre = H.nre; info->nspec_active = H.nvar; info->nreac_active = H.nact;
+  info->nnz_jac = H.nnzJ; info->nnz_lu = H.nnzLU; info->n_solve = H.nsys;
+  info->levels_lower = (int)H.lvL_ptr.size() - 1; info->levels_upper = (int)H.lvU_ptr.size() - 1;
+  info->lu_flops = H.lu_flops;
+  info->device_bytes = (int64_t)(net->arena_bytes + net->ws.n + net->stage.n + net->counter.n);
+  return NUPPN_OK;
+}
+
+nuppn_status nuppn_set_knobs(nuppn_net *net, const nuppn_knobs *knobs) {
+  if (!net || !knobs) return NUPPN_ERR_ARG;
+  double old_dgrd = net->H.kn.dgrd;
+  net->H.kn = *knobs;
+  if (knobs->dgrd != old_dgrd) bd_constants(net->H);
+  memcpy(net->D.nseq, net->H.nseq, sizeof(net->D.nseq));
+  memcpy(net->D.bd_a, net->H.bd_a, sizeof(net->D.bd_a));
+  memcpy(net->D.alf, net->H.alf, sizeof(net->D.alf));
+  net->D.kmax = net->H.kmax; net->D.kopt0 = net->H.kopt0;
+  net->D.kn = *knobs;
+  return NUPPN_OK;
+}
+
+nuppn_status nuppn_jac_pattern(const nuppn_net *net, int32_t *row, int32_t *col, int32_t *map) {
+  if (!net) return NUPPN_ERR_ARG;
+  const HostNet &H = net->H;
+  if (row) memcpy(row, H.jrow.data(), H.jrow.size() * sizeof(int));
+  if (col) memcpy(col, H.jcol.data(), H.jcol.size() * sizeof(int));
+  if (map) memcpy(map, H.dmap_all.data(), H.dmap_all.size() * sizeof(int));
+  return NUPPN_OK;
+}
+
+int64_t nuppn_launch_count(const nuppn_net *net) { return net ? net->launches : 0; }
+
+// ---- phase entry points (host buffers) ----------------------------------------------------------
+static nuppn_status run_phase(nuppn_net *net, int nz, int op, const double *X, int ldx, const double *t9,
+                              const double *rho, const double *ye, const double *v, const double *dt,
+                              const double *jac, const uint8_t *eset, const uint8_t *mask, const double *b,
+                              double *out_v, double *out_dxdt, double *out_jac, uint8_t *out_eset, uint8_t *out_mask,
+                              double *out_x) {
+  nuppn_status st = check_zone_args(net, nz, X ? ldx : net ? net->H.nsp : 0);
+  if (st != NUPPN_OK) return st;
+  if (nz == 0) return NUPPN_OK;
+  CK(cudaSetDevice(net->device));
+  const HostNet &H = net->H;
+  Stager S;
+  size_t oX = X ? S.add((size_t)nz * ldx * 8) : 0, ot9 = t9 ? S.add(nz * 8) : 0, orho = rho ? S.add(nz * 8) : 0;
+  size_t oye = ye ? S.add(nz * 8) : 0, ov = v ? S.add((size_t)nz * H.nre * 8) : 0, odt = dt ? S.add(nz * 8) : 0;
+  size_t ojac = jac ? S.add((size_t)nz * H.nnzJ * 8) : 0, oes = eset ? S.add((size_t)nz * H.nnzJ) : 0;
+  size_t omk = mask ? S.add((size_t)nz * H.nsp) : 0, ob = b ? S.add((size_t)nz * H.nsp * 8) : 0;
+  size_t oov = out_v ? S.add((size_t)nz * H.nre * 8) : 0, ood = out_dxdt ? S.add((size_t)nz * H.nsp * 8) : 0;
+  size_t ooj = out_jac ? S.add((size_t)nz * H.nnzJ * 8) : 0, ooe = out_eset ? S.add((size_t)nz * H.nnzJ) : 0;
+  size_t oom = out_mask ? S.add((size_t)nz * H.nsp) : 0, oox = out_x ? S.add((size_t)nz * H.nsp * 8) : 0;
+  CK(net->stage.ensure(S.total));
+  char *sb = (char *)net->stage.p;
+  auto up = [&](size_t off, const void *src, size_t bytes) -> cudaError_t {
+    return src ? cudaMemcpy(sb + off, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
+  };
+  CK(up(oX, X, (size_t)nz * ldx * 8)); CK(up(ot9, t9, nz * 8)); CK(up(orho, rho, nz * 8)); CK(up(oye, ye, nz * 8));
+  CK(up(ov, v, (size_t)nz * H.nre * 8)); CK(up(odt, dt, nz * 8)); CK(up(ojac, jac, (size_t)nz * H.nnzJ * 8));
+  CK(up(oes, eset, (size_t)nz * H.nnzJ)); CK(up(omk, mask, (size_t)nz * H.nsp)); CK(up(ob, b, (size_t)nz * H.nsp * 8));
+  int grid = std::min(nz, resident_slots(net));
+  st = ensure_ws(net, grid);
+  if (st != NUPPN_OK) return st;
+  PhaseArgs A;
+  memset(&A, 0, sizeof(A));
+  A.nz = nz; A.ldx = ldx; A.op = op;
+  A.X = X ? (const double *)(sb + oX) : nullptr; A.t9 = t9 ? (const double *)(sb + ot9) : nullptr;
+  A.rho = rho ? (const double *)(sb + orho) : nullptr; A.ye = ye ? (const double *)(sb + oye) : nullptr;
+  A.v_in = v ? (const double *)(sb + ov) : nullptr; A.dt = dt ? (const double *)(sb + odt) : nullptr;
+  A.jac_in = jac ? (const double *)(sb + ojac) : nullptr; A.eset_in = eset ? (const uint8_t *)(sb + oes) : nullptr;
+  A.mask_in = mask ? (const uint8_t *)(sb + omk) : nullptr; A.b = b ? (const double *)(sb + ob) : nullptr;
+  A.out_v = out_v ? (double *)(sb + oov) : nullptr; A.out_dxdt = out_dxdt ? (double *)(sb + ood) : nullptr;
+  A.out_jac = out_jac ? (double *)(sb + ooj) : nullptr; A.out_eset = out_eset ? (uint8_t *)(sb + ooe) : nullptr;
+  A.out_mask = out_mask ? (uint8_t *)(sb + oom) : nullptr; A.out_x = out_x ? (double *)(sb + oox) : nullptr;
+  CK(launch_phase(net->D, net->L, (char *)net->ws.p, grid, net->block, A, 0));
+  net->launches++;
+  CK(cudaDeviceSynchronize());
+  auto down = [&](void *dst, size_t off, size_t bytes) -> cudaError_t {
+    return dst ? cudaMemcpy(dst, sb + off, bytes, cudaMemcpyDeviceToHost) : cudaSuccess;
+  };
+  CK(down(out_v, oov, (size_t)nz * H.nre * 8)); CK(down(out_dxdt, ood, (size_t)nz * H.nsp * 8));
+  CK(down(out_jac, ooj, (size_t)nz * H.nnzJ * 8)); CK(down(out_eset, ooe, (size_t)nz * H.nnzJ));
+  CK(down(out_mask, oom, (size_t)nz * H.nsp)); CK(down(out_x, oox, (size_t)nz * H.nsp * 8));
+  return NUPPN_OK;
+}
+
+nuppn_status nuppn_eval_rates(nuppn_net *net, int32_t nz, const double *t9, const double *rho, const double *ye,
+                              const double *X, int32_t ldx, double *v) {
+  if (!t9 || !rho || !ye || !X || !v) { set_error("null argument"); return NUPPN_ERR_ARG; }
+  return run_phase(net, nz, 0, X, ldx, t9, rho, ye, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, v, nullptr,
+                   nullptr, nullptr, nullptr, nullptr);
+}
+
+nuppn_status nuppn_dxdt(nuppn_net *net, int32_t nz, const double *v, const double *X, int32_t ldx, double *dxdt) {
+  if (!v || !X || !dxdt) { set_error("null argument"); return NUPPN_ERR_ARG; }
+  return run_phase(net, nz, 1, X, ldx, nullptr, nullptr, nullptr, v, nullptr, nullptr, nullptr, nullptr, nullptr,
+                   nullptr, dxdt, nullptr, nullptr, nullptr, nullptr);
+}
+
+nuppn_status nuppn_jacobian(nuppn_net *net, int32_t nz, const double *v, const double *X, int32_t ldx, const double *dt,
+                            double *jac, uint8_t *entry_set, uint8_t *mask) {
+  if (!v || !X || !dt || !jac || !entry_set || !mask) { set_error("null argument"); return NUPPN_ERR_ARG; }
+  return run_phase(net, nz, 2, X, ldx, nullptr, nullptr, nullptr, v, dt, nullptr, nullptr, nullptr, nullptr, nullptr,
+                   nullptr, jac, entry_set, mask, nullptr);
+}
+
+nuppn_status nuppn_solve_reduced(nuppn_net *net, int32_t nz, const double *jac, const uint8_t *entry_set,
+                                 const uint8_t *mask, const double *dt, const double *b, double *x) {
+  if (!jac || !entry_set || !mask || !dt || !b || !x) { set_error("null argument"); return NUPPN_ERR_ARG; }
+  return run_phase(net, nz, 3, nullptr, net ? net->H.nsp : 0, nullptr, nullptr, nullptr, nullptr, dt, jac, entry_set,
+                   mask, b, nullptr, nullptr, nullptr, nullptr, nullptr, x);
+}
+
+// ---- integration -------------------------------------------------------------------------------
+nuppn_status nuppn_integrate_device(nuppn_net *net, int32_t nz, double *d_X, int32_t ldx, const double *d_t9_0,
+                                    const double *d_t9_1, const double *d_rho_0, const double *d_rho_1, double *d_ye,
+                                    const double *d_dtwant, int32_t *d_ierr, nuppn_zone_stats *d_stats,
+                                    int32_t *d_bd_state, void *stream) {
+  nuppn_status st = check_zone_args(net, nz, ldx);
+  if (st != NUPPN_OK) return st;
+  if (nz == 0) return NUPPN_OK;
+  if (!d_X || !d_t9_0 || !d_t9_1 || !d_rho_0 || !d_rho_1 || !d_ye || !d_dtwant || !d_ierr) {
+    set_error("null device argument");
+    return NUPPN_ERR_ARG;
+  }
+  CK(cudaSetDevice(net->device));
+  int grid = std::min(nz, resident_slots(net));
+  st = ensure_ws(net, grid);
+  if (st != NUPPN_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  CK(cudaMemsetAsync(net->counter.p, 0, sizeof(int), s));
+  IntegrateArgs A;
+  A.nz = nz; A.ldx = ldx; A.X = d_X; A.t9_0 = d_t9_0; A.t9_1 = d_t9_1; A.rho_0 = d_rho_0; A.rho_1 = d_rho_1;
+  A.dtwant = d_dtwant; A.ye = d_ye; A.ierr = d_ierr; A.stats = d_stats; A.bd_state = d_bd_state;
+  A.counter = (int *)net->counter.p;
+  CK(launch_integrate(net->D, net->L, (char *)net->ws.p, grid, net->block, A, s));
+  net->launches++;
+  return NUPPN_OK;
+}
+
+nuppn_status nuppn_integrate(nuppn_net *net, int32_t nz, double *X, int32_t ldx, const double *t9_0,
+                             const double *t9_1, const double *rho_0, const double *rho_1, double *ye,
+                             const double *dtwant, int32_t *ierr, nuppn_zone_stats *stats, int32_t *bd_state) {
+  nuppn_status st = check_zone_args(net, nz, ldx);
+  if (st != NUPPN_OK) return st;
+  if (nz == 0) return NUPPN_OK;
+  if (!X || !t9_0 || !t9_1 || !rho_0 || !rho_1 || !ye || !dtwant || !ierr) {
+    set_error("null argument");
+    return NUPPN_ERR_ARG;
+  }
+  CK(cudaSetDevice(net->device));
+  Stager S;
+  size_t oX = S.add((size_t)nz * ldx * 8), o1 = S.add(nz * 8), o2 = S.add(nz * 8), o3 = S.add(nz * 8);
+  size_t o4 = S.add(nz * 8), o5 = S.add(nz * 8), o6 = S.add(nz * 8), oi = S.add(nz * 4);
+  size_t os = S.add((size_t)nz * sizeof(nuppn_zone_stats)), ob = S.add(nz * 4);
+  CK(net->stage.ensure(S.total));
+  char *sb = (char *)net->stage.p;
+  CK(cudaMemcpy(sb + oX, X, (size_t)nz * ldx * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + o1, t9_0, nz * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + o2, t9_1, nz * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + o3, rho_0, nz * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + o4, rho_1, nz * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + o5, ye, nz * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + o6, dtwant, nz * 8, cudaMemcpyHostToDevice));
+  if (bd_state) CK(cudaMemcpy(sb + ob, bd_state, nz * 4, cudaMemcpyHostToDevice));
+  else CK(cudaMemset(sb + ob, 0, nz * 4));
+  st = nuppn_integrate_device(net, nz, (double *)(sb + oX), ldx, (double *)(sb + o1), (double *)(sb + o2),
+                              (double *)(sb + o3), (double *)(sb + o4), (double *)(sb + o5), (double *)(sb + o6),
+                              (int *)(sb + oi), (nuppn_zone_stats *)(sb + os), (int *)(sb + ob), nullptr);
+  if (st != NUPPN_OK) return st;
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(X, sb + oX, (size_t)nz * ldx * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ye, sb + o5, nz * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ierr, sb + oi, nz * 4, cudaMemcpyDeviceToHost));
+  if (stats) CK(cudaMemcpy(stats, sb + os, (size_t)nz * sizeof(nuppn_zone_stats), cudaMemcpyDeviceToHost));
+  if (bd_state) CK(cudaMemcpy(bd_state, sb + ob, nz * 4, cudaMemcpyDeviceToHost));
+  return NUPPN_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,341 @@
+// integrator.cuh -- step control on the device (included by solver.cu after the phase kernels).
+//
+// backward_euler_newton / newton_iteration   solver/source/backward_euler.F90:29-176
+// bader_deuflhard_integration and helpers   solver/source/bader_deuflhard.F90:139-488
+// integrate_network / do_one_time_step      solver/source/solver.F90:53-274
+//
+// All threads of the CTA run this control flow with identical scalars.
+#pragma once
+
+namespace nuppn {
+
+struct ZoneCtl {
+  nuppn_zone_stats st;
+  int kopt;
+  bool reduce;
+  double sumerr;  // kept between levels like the reference's module variable
+  double err[kMaxLevels + 1];
+  double xhist[kMaxLevels + 1];
+};
+
+__device__ void vcopy(double *dst, const double *src, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+}
+
+__device__ double vsum(const double *a, int n, double *sred) {
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += a[i];
+  return block_sum(s, sred);
+}
+
+__device__ double vmaxneg(const double *a, int n, double *sred) {
+  double m = -DBL_MAX;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, -a[i]);
+  return block_max(m, sred);
+}
+
+// ypsplus (utils.F90:726-740)
+__device__ void ypsplus(double *y, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double v = y[i];
+    if (v < -1.e-27) v = 1.e-99;
+    if (v < 1.e-27) v = 1.e-99;
+    y[i] = v;
+  }
+  __syncthreads();
+}
+
+// calculate_ye (utils.F90:537-553)
+__device__ double dev_ye(const DevNet &N, const double *x, double *sred) {
+  double s = 0.0;
+  for (int i = threadIdx.x; i < N.nsp; i += blockDim.x)
+    if (N.ciso[i]) s += (N.an[i] - 2.0 * N.zn[i]) * x[i] / N.an[i];
+  s = block_sum(s, sred);
+  return (1.0 - s) * 0.5;
+}
+
+// ---------------------------------------------------------------------------------------------
+__device__ int dev_backward_euler(const DevNet &N, const Ws &W, ZoneCtl &C, double *yps, double dt, double &dtrcmd,
+                                  double *sred) {
+  const int nsp = N.nsp, tid = threadIdx.x, nt = blockDim.x;
+  const double rmin = 0.2, rmax = 2.0, dgrd = N.kn.dgrd;
+  const double sum_check = N.kn.grdthreshold * N.nvar * dgrd;
+  for (int i = tid; i < nsp; i += nt) { W.y_new[i] = yps[i]; W.y_old[i] = yps[i]; W.y_cur[i] = yps[i]; }
+  __syncthreads();
+  int iter = 0;
+  double grd = 0.0;
+  for (;;) {
+    if (iter > N.kn.ittd) {
+      double mneg = vmaxneg(W.y_new, nsp, sred), err, tol;
+      double sumy = vsum(W.y_new, nsp, sred);
+      int ierr;
+      if (mneg >= sum_check) { err = mneg; tol = sum_check; ierr = NEG_ABUNDS; }
+      else if (fabs(1.0 - sumy) > K_SUM_TOL) { err = fabs(1.0 - sumy); tol = K_SUM_TOL; ierr = SUM_X; }
+      else { err = grd; tol = dgrd; ierr = SLV_CNVRG; }
+      dtrcmd = fmax(fmin(pow(tol / fmax(err, K_SMALL), 0.5), rmax), rmin) * dt;
+      return ierr;
+    }
+    // newton_iteration (backward_euler.F90:120-176)
+    dev_jacobian(N, W, dt, W.y_cur);
+    dev_assemble_factor(N, W, dt);
+    dev_dxdt(N, W, W.y_cur, W.dxdt);
+    for (int i = tid; i < nsp; i += nt) W.rhs[i] = W.y_old[i] - W.y_cur[i] + dt * W.dxdt[i];
+    __syncthreads();
+    dev_solve(N, W, W.rhs, W.delta_k);  // delta_k doubles as the correction buffer here
+    C.st.nfact++; C.st.nsolve++;
+    double g = 0.0;
+    for (int i = tid; i < nsp; i += nt) {
+      double yn = W.mask[i] ? W.y_cur[i] + W.delta_k[i] : W.y_new[i];
+      W.y_new[i] = yn;
+      if (W.y_cur[i] > N.kn.grdthreshold) g = fmax(g, fabs((yn - W.y_cur[i]) / W.y_cur[i]));
+    }
+    grd = block_max(g, sred);
+    iter++;
+    C.st.newton_iters++;
+    double mneg = vmaxneg(W.y_new, nsp, sred);
+    double sumy = vsum(W.y_new, nsp, sred);
+    if (grd <= dgrd && mneg < sum_check && fabs(1.0 - sumy) <= K_SUM_TOL) {
+      vcopy(yps, W.y_new, nsp);
+      dtrcmd = 2.0 * fmax(fmin(pow(dgrd / fmax(grd, K_SMALL), 0.5), rmax), rmin) * dt;
+      ypsplus(yps, nsp);
+      return 0;
+    }
+    vcopy(W.y_cur, W.y_new, nsp);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// one semi-implicit midpoint sub-step, bader_deuflhard_step (bader_deuflhard.F90:410-488)
+__device__ int dev_bd_substep(const DevNet &N, const Ws &W, ZoneCtl &C, double h, int stage, double *sred) {
+  const int nsp = N.nsp, tid = threadIdx.x, nt = blockDim.x;
+  dev_dxdt(N, W, W.y_k, W.dxdt);
+  if (stage == 1) for (int i = tid; i < nsp; i += nt) W.rhs[i] = h * W.dxdt[i];
+  else for (int i = tid; i < nsp; i += nt) W.rhs[i] = h * W.dxdt[i] - W.delta_k[i];
+  __syncthreads();
+  dev_solve(N, W, W.rhs, W.y_ext);  // y_ext doubles as the solution buffer here
+  C.st.nsolve++;
+  bool huge = false;
+  for (int i = tid; i < nsp; i += nt) {
+    double d = stage == 2 ? W.delta_k[i] + 2.0 * W.y_ext[i] : W.y_ext[i];
+    W.delta_k[i] = d;
+    double yk = W.y_k[i] + d;
+    W.y_k[i] = yk;
+    if (yk > 2.0) huge = true;
+  }
+  return block_any(huge) ? HUGE_ABUNDS : 0;
+}
+
+// extrapolate (bader_deuflhard.F90:371-407): Neville tableau, column k
+__device__ void dev_extrapolate(const DevNet &N, const Ws &W, ZoneCtl &C, int k, double xest) {
+  const int n = N.nsp, tid = threadIdx.x, nt = blockDim.x;
+  C.xhist[k] = xest;
+  double *Q = W.qcol, *E = W.yerr;
+  for (int j = tid; j < n; j += nt) {
+    double yest = W.y_k[j];
+    E[(size_t)k * n + j] = yest;
+    if (k == 1) {
+      Q[(size_t)k * n + j] = yest;
+      W.y_ext[j] = yest;
+      continue;
+    }
+    double yz = yest, d = yest, e = yest;
+    for (int k1 = 1; k1 <= k - 1; ++k1) {
+      double delta = 1.0 / (C.xhist[k - k1] - xest);
+      double f1 = xest * delta, f2 = C.xhist[k - k1] * delta;
+      double q = Q[(size_t)k1 * n + j];
+      Q[(size_t)k1 * n + j] = e;
+      double dl = d - q;
+      e = f1 * dl;
+      d = f2 * dl;
+      yz = yz + e;
+    }
+    E[(size_t)k * n + j] = e;
+    Q[(size_t)k * n + j] = e;
+    W.y_ext[j] = yz;
+  }
+  __syncthreads();
+}
+
+__device__ int dev_bader_deuflhard(const DevNet &N, const Ws &W, ZoneCtl &C, double *yps, double dt, double &dtrcmd,
+                                   bool frst, double *sred) {
+  const int nsp = N.nsp, tid = threadIdx.x, nt = blockDim.x;
+  const double safe1 = 0.25, safe2 = 0.7, redmin = 0.7, redmax = 1.e-5, scalmx = 0.25;
+  int km = -1, k;
+  double scal = 1.0, red = -1.0, errmax = 0.0, abuerr = 0.0, negerr = 0.0;
+  dev_jacobian(N, W, dt, yps);
+  for (k = 1; k <= N.kmax; ++k) {
+    vcopy(W.y_k, yps, nsp);
+    // semi_implicit_extrapolation (bader_deuflhard.F90:276-316)
+    double h = dt / (double)N.nseq[k];
+    double xest = powi(h / N.nseq[k], 2);
+    dev_assemble_factor(N, W, h);
+    C.st.nfact++;
+    int ierr = dev_bd_substep(N, W, C, h, 1, sred);
+    for (int i = 1; ierr == 0 && i <= N.nseq[k] - 1; ++i) ierr = dev_bd_substep(N, W, C, h, 2, sred);
+    if (ierr == 0) ierr = dev_bd_substep(N, W, C, h, 3, sred);
+    if (ierr != 0) {
+      dtrcmd = dt * 0.2;
+      vcopy(yps, W.y_k, nsp);
+      return ierr;
+    }
+    C.st.newton_iters += N.nseq[k];
+    dev_extrapolate(N, W, C, k, xest);
+    bool nan = false;
+    for (int i = tid; i < nsp; i += nt) {
+      double y = W.y_ext[i];
+      W.y_k[i] = y;
+      if (y != y) nan = true;
+      W.yscal[i] = fmax(fabs(y), N.kn.grdthreshold);
+    }
+    if (block_any(nan)) {
+      dtrcmd = dt * 0.2;
+      vcopy(yps, W.y_k, nsp);
+      return GOT_NAN;
+    }
+    if (k != 1) {
+      // compute_error (bader_deuflhard.F90:325-366)
+      double am = -DBL_MAX, nm = -DBL_MAX;
+      for (int i = tid; i < nsp; i += nt) {
+        double y = W.y_k[i];
+        if (y > 1e-27) am = fmax(am, fabs(W.yerr[(size_t)k * nsp + i] / W.yscal[i]));
+        if (y < N.kn.grdthreshold) nm = fmax(nm, -y);
+      }
+      abuerr = block_max(am, sred) / N.kn.dgrd;
+      negerr = block_max(nm, sred) / N.kn.grdthreshold;
+      if (abuerr < 1e-3) {
+        errmax = abuerr;
+      } else {
+        C.sumerr = fabs(1.0 - vsum(W.y_k, nsp, sred)) / K_SUM_TOL;
+        errmax = fmax(abuerr, C.sumerr);
+      }
+      errmax = fmax(errmax, negerr);
+      km = k - 1;
+      C.err[km] = pow(errmax / safe1, 1.0 / (2.0 * km + 1.0));
+    }
+    if (k != 1 && (k >= C.kopt - 1 || frst)) {
+      if (errmax <= 1.0) {
+        C.reduce = false;
+        break;
+      } else {
+        if (k == N.kmax || k == C.kopt + 1) {
+          C.reduce = true; red = safe2 / C.err[km];
+        } else if (k == C.kopt) {
+          if (N.alf[C.kopt - 1][C.kopt] < C.err[km]) { C.reduce = true; red = safe2 / C.err[km]; }
+        } else if (C.kopt == N.kmax) {
+          if (N.alf[km][N.kmax - 1] < C.err[km]) { C.reduce = true; red = N.alf[km][N.kmax - 1] * safe2 / C.err[km]; }
+        } else if (N.alf[km][C.kopt] < C.err[km]) {
+          C.reduce = true; red = N.alf[km][C.kopt - 1] / C.err[km];
+        }
+      }
+    }
+  }
+  int ierr = 0;
+  if (k > N.kmax) k = N.kmax + 1;
+  if (C.reduce) {
+    red = fmax(redmax, fmin(red, redmin));
+    dtrcmd = dt * red;
+    if (negerr > C.sumerr && negerr > abuerr) ierr = NEG_ABUNDS;
+    else if (C.sumerr > abuerr) ierr = SUM_X;
+    else ierr = SLV_CNVRG;
+  } else {
+    double workmin = 1.e35;
+    for (int kk = 1; kk <= km; ++kk) {
+      double f = fmax(C.err[kk], scalmx), work = f * N.bd_a[kk + 1];
+      if (work < workmin) { scal = f; workmin = work; C.kopt = kk + 1; }
+    }
+    dtrcmd = 2.0 * dt / scal;
+    if (C.kopt >= k && C.kopt != N.kmax) {
+      double f = fmax(scal / N.alf[C.kopt - 1][C.kopt], scalmx);
+      if (N.bd_a[C.kopt + 1] * f <= workmin) {
+        dtrcmd = dtrcmd * scal / f;
+        C.kopt = C.kopt + 1;
+      }
+    }
+  }
+  vcopy(yps, W.y_k, nsp);
+  return ierr;
+}
+
+__device__ __forceinline__ double interp2(double x1, double y0, double y1, double xw) {  // interp.F90:29-50
+  double xwant = fmin(fmax(xw, 0.0), x1);
+  return y0 + (y1 - y0) * (xwant - 0.0) / (x1 - 0.0);
+}
+
+// integrate_network (solver.F90:53-238) for the CTA's zone; W.y holds yps on entry and exit
+__device__ int dev_integrate_zone(const DevNet &N, const Ws &W, ZoneCtl &C, double t9_0, double t9_1, double rho_0,
+                                  double rho_1, double &ye, double dtwant, bool frst, double *sred) {
+  const int nsp = N.nsp;
+  const nuppn_knobs &kn = N.kn;
+  double *yps = W.y;
+  if (!(t9_0 > 0.0) || !(t9_1 > 0.0) || !(rho_0 > 0.0) || !(rho_1 > 0.0) || !isfinite(t9_0 + t9_1 + rho_0 + rho_1) ||
+      !(dtwant > 0.0) || !isfinite(dtwant))
+    return NUPPN_BAD_INPUT;
+  vcopy(W.y_old, yps, nsp);
+  double ye_old = ye, dtdone = 0.0, dtrcmd = 0.0, dttry = dtwant;
+  double t9_last = 0.5 * (t9_0 + t9_1), rho_last = 0.5 * (rho_0 + rho_1);
+  dev_eval_rates(N, W, t9_last, rho_last, ye, yps, sred);  // the frame's evaluate_all_rates
+  for (int i = 1; i <= kn.max_sub_steps; ++i) {
+    if (i > 1) frst = false;
+    double t_0 = dtdone, t_1 = fmin(dtdone + dttry, dtwant);
+    double my_t9_0 = 0, my_t9_1 = 0, my_rho_0 = 0, my_rho_1 = 0, my_t9, my_rho;
+    if (kn.interpolate_temp) {
+      my_t9_0 = interp2(dtwant, t9_0, t9_1, t_0);
+      my_t9_1 = interp2(dtwant, t9_0, t9_1, t_1);
+      my_t9 = 0.5 * (my_t9_0 + my_t9_1);
+    } else {
+      my_t9 = 0.5 * (t9_0 + t9_1);
+    }
+    if (kn.interpolate_dens) {
+      my_rho_0 = interp2(dtwant, rho_0, rho_1, t_0);
+      my_rho_1 = interp2(dtwant, rho_0, rho_1, t_1);
+      my_rho = 0.5 * (my_rho_0 + my_rho_1);
+    } else {
+      my_rho = 0.5 * (rho_0 + rho_1);
+    }
+    double diff = fmax(fabs(my_t9_0 - my_t9_1) / my_t9_0, fabs(my_rho_0 - my_rho_1) / my_rho_0);
+    if (diff > kn.delta_state_max && t9_0 > kn.min_t9_for_slv && t9_1 > kn.min_t9_for_slv) {
+      dttry = 0.5 * dttry;
+      continue;
+    }
+    if (my_t9 != t9_last || my_rho != rho_last) {
+      dev_eval_rates(N, W, my_t9, my_rho, ye, yps, sred);
+      t9_last = my_t9; rho_last = my_rho;
+    }
+    int ierr = 0;
+    if (my_t9 >= kn.min_t9_for_slv) {
+      if (kn.integration_method == 0) ierr = dev_backward_euler(N, W, C, yps, dttry, dtrcmd, sred);
+      else ierr = dev_bader_deuflhard(N, W, C, yps, dttry, dtrcmd, frst, sred);
+      ye = dev_ye(N, yps, sred);
+      if (dttry < K_SMALL) return SMALL_DT;
+    }
+    if (ierr == 0) {
+      dtdone = dtdone + dttry;
+      for (int s = threadIdx.x; s < nsp; s += blockDim.x) {
+        double y = fmax(yps[s], 1.e-99);
+        yps[s] = y;
+        W.y_old[s] = y;
+      }
+      __syncthreads();
+      ye_old = ye;
+      C.st.nsucc++;
+      if (dtdone >= dtwant) break;
+    } else {
+      vcopy(yps, W.y_old, nsp);
+      ye = ye_old;
+      C.st.nfail++;
+    }
+    dttry = fmin(dtrcmd, dtwant - dtdone);
+    if (i == kn.max_sub_steps) return MAX_SUBSTEPS;
+  }
+  if (kn.integration_method == 1) {
+    double s = vsum(yps, nsp, sred);
+    for (int q = threadIdx.x; q < nsp; q += blockDim.x) yps[q] = yps[q] / s;
+    __syncthreads();
+  }
+  for (int q = threadIdx.x; q < nsp; q += blockDim.x) yps[q] = fmax(yps[q], 1.e-99);
+  __syncthreads();
+  return 0;
+}
+
+}  // namespace nuppn

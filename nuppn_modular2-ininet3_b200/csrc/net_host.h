@@ -1,0 +1,68 @@
+// net_host.h -- one-time host analysis of a network description.
+//
+// Everything the reference recomputes per call or keeps in module state is prepared here once:
+// the static Jacobian pattern of makemap (jac_rhs.F90:461-540), the accumulation orders of
+// calculate_dxdt / calculate_jacobian (jac_rhs.F90:243-262, 363-392) turned into per-target gather
+// lists, and a static-pivot sparse LU (fill-reducing order, filled pattern, update map and level
+// schedules) that takes the place of SuperLU's per-call COLAMD + symbolic analysis
+// (c_fortran_dgssv.c:110-119).
+#pragma once
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "nuppn_internal.h"
+
+namespace nuppn {
+
+struct HostNet {
+  nuppn_knobs kn;
+  int nsp = 0, nre = 0, ig = 0, nact = 0, nsys = 0, nnzJ = 0, nnzLU = 0, ihe4 = -1, ibe8 = -1;
+  int nvar = 0;
+  std::vector<double> an, zn, gspin_nse;
+  std::vector<uint8_t> ciso, crea, rev_target;
+  std::vector<int> spart, src, sidx, ilabb, scr_mode, irev, rev_sp, rev_kind;
+  std::vector<double> rfac, scr_z1, scr_z2, rev_mc, rev_Q;
+  std::vector<int> act_slot, act_k, act_ice;
+  // raw k of all slots (for the pattern query)
+  std::vector<int> k_all;
+  // REACLIB
+  int nc = 0, nr = 0;
+  std::vector<int> rl_first, rl_info, rl_part;
+  std::vector<double> rl_a;
+  int npart = 0;
+  std::vector<double> pt9, pval;
+  int nv = 0;
+  std::vector<int> vfirst, vxfac;
+  std::vector<double> vterms, vdpow;
+  int ngk = 0, ngn = 0, ngd = 1;
+  std::vector<double> ngt8, ngl10t8, ngflag, ngane, ngl10v;
+  std::vector<int> ngndata;
+  int ffv = 0, fft = 0, ffr = 0;
+  std::vector<double> fft9, ffrho, ffl10v;
+  int kdn = 0, kde = 0;
+  std::vector<double> kdE, kdcoef;
+  std::vector<double> constr;
+  // pattern
+  std::vector<int> jrow, jcol, jdiag, dmap_all;  // dmap_all[nre*8] (-1 for unconsidered)
+  std::vector<int> jg_ptr, jg_item, dg_ptr, dg_item, jg_long, dg_long;
+  std::vector<double> dg_coef;
+  // system / LU
+  std::vector<int> sys_of_sp, sp_of_sys, pos_of_entry;
+  std::vector<int> lu_rowptr, lu_diag, lu_col, upd_start;
+  std::vector<uint16_t> upd_off;
+  std::vector<int> lvL_ptr, lvL_rows, lvL_grp, lvU_ptr, lvU_rows, lvU_grp;
+  int64_t lu_flops = 0;
+  // BD constants
+  int nseq[kMaxLevels + 2];
+  double bd_a[kMaxLevels + 2];
+  double alf[kMaxLevels + 1][kMaxLevels + 1];
+  int kmax = 0, kopt0 = 0;
+};
+
+// Builds the analysis; returns an empty string on success or a message describing the problem.
+std::string build_host_net(const nuppn_net_desc &d, const nuppn_knobs &kn, HostNet &H);
+void bd_constants(HostNet &H);
+
+}  // namespace nuppn

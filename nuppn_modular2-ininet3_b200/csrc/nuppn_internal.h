@@ -1,0 +1,117 @@
+// nuppn_internal.h -- shared host/device structures of the B200 solver library.
+#pragma once
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/nuppn.h"
+
+namespace nuppn {
+
+constexpr int kMaxLevels = 8;       // Bader-Deuflhard tableau columns (bader_deuflhard.F90:24)
+constexpr int kPartDim = 24;        // partition-function temperature points (array_sizes.F90:15)
+
+// Network as the device sees it: every pointer is device memory, read-only during solves.
+struct DevNet {
+  int nsp, nre, nact, ig, nsys, nnzJ, nnzLU;
+  int ihe4, ibe8;
+  // species
+  const double *an, *zn;
+  const uint8_t *ciso;
+  const int *spart;          // partition row or -1
+  const double *gspin_nse;   // ppn_g where the species is in the NSE set, 0 otherwise
+  // all reaction slots (rates)
+  const int *src, *sidx;
+  const double *rfac;
+  const uint8_t *crea, *rev_target;
+  const int *ilabb;
+  const int *scr_mode;       // 0 pair (z1,z2), 1 triple-alpha, 2 n(2a,g), 3 unscreened-slot
+  const double *scr_z1, *scr_z2;
+  const int *irev;           // slot of the reverse or -1 (considered forwards only)
+  const int *rev_sp;         // [nre*4] species for G: a1, a2 (or a1 if na1==2), b1 (-1 -> G=0), b2
+  const int *rev_kind;       // 1 capture (ng,pg,ag), 2 other, 0 unusable
+  const double *rev_mc;      // capture: m_a1 m_a2/m_b2 *2pi/h^2 ; other: (m_a1 m_a2/m_b1/m_b2)^1.5
+  const double *rev_Q;       // Q (MeV) as reverse.F90:279/296
+  // active (considered) reactions
+  const int *act_slot;       // [nact] slot index
+  const int *act_k;          // [nact*8] k1..k8
+  const int *act_ice;        // [nact*8] dns2csr_map in reference slot order
+  // REACLIB
+  int nc, nr;
+  const int *rl_first;       // [nr+1]
+  const double *rl_a;        // [nc*7]
+  const int *rl_info;        // [nr] chapter | vflag<<8 | ecflag<<9 | nireac<<16
+  const int *rl_part;        // [nr*6]
+  int npart;
+  const double *pt9, *pval;  // [24], [npart*24]
+  // VITAL templates
+  int nv;
+  const int *vfirst, *vxfac;
+  const double *vterms, *vdpow;
+  // NETGEN
+  int ngk, ngn, ngd;
+  const double *ngt8, *ngl10t8, *ngflag, *ngane, *ngl10v;
+  const int *ngndata;
+  // FFN
+  int ffv, fft, ffr;
+  const double *fft9, *ffrho, *ffl10v;
+  // KADoNiS (Akima coefficients [n][ne-1][4])
+  int kdn, kde;
+  const double *kdE, *kdcoef;
+  const double *constr;
+  // Jacobian pattern and gathers
+  const int *jrow, *jcol, *jdiag;          // jdiag[nsp]: entry of (i,i) or -1
+  const int *jg_ptr, *jg_item;             // entry -> (a*8 + s) in reference accumulation order
+  const int *dg_ptr, *dg_item;             // species -> (a*4 + slot) in scatter order
+  const double *dg_coef;                   // coefficient of each dg item: -k2, -1, k6, k8
+  int njg_long, ndg_long;
+  const int *jg_long, *dg_long;            // entries / species whose gather lists are long
+  // system and LU
+  const int *sys_of_sp, *sp_of_sys;        // [nsp], [nsys]
+  const int *pos_of_entry;                 // [nnzJ] LU position or -1
+  const int *lu_rowptr, *lu_diag, *lu_col; // [nsys+1], [nsys], [nnzLU]
+  const int *upd_start;                    // [nnzLU+1] for L entries: start in upd_off
+  const uint16_t *upd_off;                 // offsets into the target row
+  int nlvL, nlvU;
+  const int *lvL_ptr, *lvL_rows, *lvL_grp; // factorization / forward levels
+  const int *lvU_ptr, *lvU_rows, *lvU_grp; // backward levels
+  // Bader-Deuflhard constants
+  int nseq[kMaxLevels + 2];
+  double bd_a[kMaxLevels + 2];
+  double alf[kMaxLevels + 1][kMaxLevels + 1];
+  int kmax, kopt0;
+  nuppn_knobs kn;
+  // derived constants
+  int nvar;                                // count(considerisotope)
+};
+
+// Per-CTA workspace layout (byte offsets into one slab).
+struct WsLayout {
+  size_t v, rv, ngv, ffv, kdv, partinter, G, flux, contrib, first_l, eset, jac, mask, xn, dxdt;
+  size_t y, y_old, y_cur, y_new, y_k, delta_k, y_ext, yscal, qcol, yerr, lu, bsys, xsys, rhs;
+  size_t bytes;
+};
+
+// arguments of the persistent integration kernel
+struct IntegrateArgs {
+  int nz, ldx;
+  double *X;
+  const double *t9_0, *t9_1, *rho_0, *rho_1, *dtwant;
+  double *ye;
+  int *ierr;
+  nuppn_zone_stats *stats;
+  int *bd_state;
+  int *counter;
+};
+
+// arguments of the single-phase parity kernel
+struct PhaseArgs {
+  int nz, ldx, op;  // op: 0 rates, 1 dxdt, 2 jacobian, 3 reduced solve
+  const double *X, *t9, *rho, *ye, *v_in, *dt, *jac_in, *b;
+  const uint8_t *eset_in, *mask_in;
+  double *out_v, *out_dxdt, *out_jac, *out_x;
+  uint8_t *out_eset, *out_mask;
+};
+
+}  // namespace nuppn

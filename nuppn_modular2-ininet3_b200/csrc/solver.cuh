@@ -1,0 +1,47 @@
+// solver.cuh -- device side of the B200 solver: one CTA advances one zone at a time.
+//
+// Data layout: the network (DevNet) is zone-shared and read-only; every CTA owns a workspace slab
+// (WsLayout) holding its zone's rates, Jacobian values, LU values and integrator vectors, so each
+// per-zone sweep is a contiguous, coalesced stream. Every phase below is a block-wide loop followed
+// by a barrier; scalar control flow (step-size logic of solver.F90, backward_euler.F90 and
+// bader_deuflhard.F90) is evaluated redundantly by all threads from block-reduced values, so it
+// is uniform across the CTA.
+#pragma once
+#include <cuda_runtime.h>
+#include <float.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "nuppn_internal.h"
+
+namespace nuppn {
+
+#define NUPPN_FULL 0xffffffffu
+
+constexpr int kLongList = 48;   // gather lists longer than this are summed by a whole warp
+
+struct Ws {
+  double *v, *rv, *ngv, *ffv, *kdv, *partinter, *G, *flux, *contrib, *jac, *xn, *dxdt;
+  double *y, *y_old, *y_cur, *y_new, *y_k, *delta_k, *y_ext, *yscal, *qcol, *yerr, *lu, *bsys, *xsys, *rhs;
+  int *first_l;
+  uint8_t *eset, *mask;
+};
+
+__device__ __forceinline__ Ws ws_bind(char *base, const WsLayout &L) {
+  Ws w;
+  w.v = (double *)(base + L.v); w.rv = (double *)(base + L.rv); w.ngv = (double *)(base + L.ngv);
+  w.ffv = (double *)(base + L.ffv); w.kdv = (double *)(base + L.kdv);
+  w.partinter = (double *)(base + L.partinter); w.G = (double *)(base + L.G);
+  w.flux = (double *)(base + L.flux); w.contrib = (double *)(base + L.contrib);
+  w.first_l = (int *)(base + L.first_l); w.eset = (uint8_t *)(base + L.eset);
+  w.jac = (double *)(base + L.jac); w.mask = (uint8_t *)(base + L.mask); w.xn = (double *)(base + L.xn);
+  w.dxdt = (double *)(base + L.dxdt); w.y = (double *)(base + L.y); w.y_old = (double *)(base + L.y_old);
+  w.y_cur = (double *)(base + L.y_cur); w.y_new = (double *)(base + L.y_new); w.y_k = (double *)(base + L.y_k);
+  w.delta_k = (double *)(base + L.delta_k); w.y_ext = (double *)(base + L.y_ext);
+  w.yscal = (double *)(base + L.yscal); w.qcol = (double *)(base + L.qcol); w.yerr = (double *)(base + L.yerr);
+  w.lu = (double *)(base + L.lu); w.bsys = (double *)(base + L.bsys); w.xsys = (double *)(base + L.xsys);
+  w.rhs = (double *)(base + L.rhs);
+  return w;
+}
+
+}  // namespace nuppn

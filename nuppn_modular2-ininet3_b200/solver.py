@@ -1,0 +1,186 @@
+"""Host-side mirror of the reference's solver interface, over the C ABI (include/nuppn.h).
+
+``Network`` arrays go in once (``NetworkSolver(net)``); afterwards the calls mirror the reference's
+entry points, batched over zones:
+
+* ``evaluate_all_rates(t9, rho, ye, X)``          physics/source/evaluate_rates.F90:14
+* ``integrate_network(X, t9_0, t9_1, rho_0, rho_1, ye, dtwant)``   solver/source/solver.F90:53
+* ``calculate_dxdt`` / ``calculate_jacobian``       solver/source/jac_rhs.F90:217, 282
+
+Per-zone outcomes use the reference's error codes (``abi.ERROR_CODE``); library failures raise
+``NuppnError``. The CUDA library is required: there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from . import synthnet as sn
+
+_LIB = None
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libnuppn_b200.so")
+
+
+class NuppnError(RuntimeError):
+    pass
+
+
+def load_library():
+    """Load libnuppn_b200.so (built in-tree); raise if it is missing."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise NuppnError(f"CUDA library not built: {LIB_PATH} (run __graft_entry__.build())")
+    L = C.CDLL(LIB_PATH)
+    vp, i32, i64 = C.c_void_p, C.c_int32, C.c_int64
+    L.nuppn_abi_version.restype = i32
+    L.nuppn_status_string.restype = C.c_char_p
+    L.nuppn_status_string.argtypes = [i32]
+    L.nuppn_last_error.restype = C.c_char_p
+    L.nuppn_default_knobs.argtypes = [vp]
+    L.nuppn_net_create.argtypes = [vp, vp, i32, C.POINTER(vp)]
+    L.nuppn_net_destroy.argtypes = [vp]
+    L.nuppn_net_info_get.argtypes = [vp, vp]
+    L.nuppn_set_knobs.argtypes = [vp, vp]
+    L.nuppn_jac_pattern.argtypes = [vp, vp, vp, vp]
+    L.nuppn_eval_rates.argtypes = [vp, i32, vp, vp, vp, vp, i32, vp]
+    L.nuppn_dxdt.argtypes = [vp, i32, vp, vp, i32, vp]
+    L.nuppn_jacobian.argtypes = [vp, i32, vp, vp, i32, vp, vp, vp, vp]
+    L.nuppn_solve_reduced.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp]
+    L.nuppn_integrate.argtypes = [vp, i32, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.nuppn_integrate_device.argtypes = [vp, i32, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.nuppn_launch_count.argtypes = [vp]
+    L.nuppn_launch_count.restype = i64
+    for name in ("nuppn_net_create", "nuppn_net_destroy", "nuppn_net_info_get", "nuppn_set_knobs",
+                 "nuppn_jac_pattern", "nuppn_eval_rates", "nuppn_dxdt", "nuppn_jacobian",
+                 "nuppn_solve_reduced", "nuppn_integrate", "nuppn_integrate_device"):
+        getattr(L, name).restype = i32
+    _LIB = L
+    return L
+
+
+def _p(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def _f64(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if n is not None and a.shape == ():
+        a = np.full(n, float(a))
+    return a
+
+
+class NetworkSolver:
+    """One network on one device (the module state of the reference, as a handle)."""
+
+    def __init__(self, net: sn.Network, knobs: abi.Knobs | None = None, device: int = 0):
+        self.L = load_library()
+        self.net = net
+        self.knobs = knobs or abi.default_knobs()
+        self._desc = abi.make_desc(net)
+        h = C.c_void_p()
+        self._check(self.L.nuppn_net_create(C.byref(self._desc), C.byref(self.knobs), device, C.byref(h)))
+        self.h = h
+        info = abi.NetInfo()
+        self._check(self.L.nuppn_net_info_get(self.h, C.byref(info)))
+        self.info = info
+
+    def _check(self, st):
+        if st != 0:
+            msg = self.L.nuppn_last_error().decode()
+            raise NuppnError(f"{self.L.nuppn_status_string(st).decode()}: {msg}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.nuppn_net_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_knobs(self, knobs: abi.Knobs):
+        self.knobs = knobs
+        self._check(self.L.nuppn_set_knobs(self.h, C.byref(knobs)))
+
+    @property
+    def nsp(self):
+        return self.net.nsp
+
+    @property
+    def nre(self):
+        return self.net.nre
+
+    def launches(self) -> int:
+        return int(self.L.nuppn_launch_count(self.h))
+
+    def jac_pattern(self):
+        nnz = self.info.nnz_jac
+        row = np.zeros(nnz, np.int32); col = np.zeros(nnz, np.int32)
+        dmap = np.zeros(self.nre * 8, np.int32)
+        self._check(self.L.nuppn_jac_pattern(self.h, _p(row), _p(col), _p(dmap)))
+        return row, col, dmap.reshape(self.nre, 8)
+
+    def evaluate_all_rates(self, t9, rho, ye, X):
+        X = np.ascontiguousarray(np.atleast_2d(X), dtype=np.float64)
+        nz = X.shape[0]
+        t9, rho, ye = _f64(t9, nz), _f64(rho, nz), _f64(ye, nz)
+        v = np.zeros((nz, self.nre))
+        self._check(self.L.nuppn_eval_rates(self.h, nz, _p(t9), _p(rho), _p(ye), _p(X), X.shape[1], _p(v)))
+        return v
+
+    def calculate_dxdt(self, v, X):
+        X = np.ascontiguousarray(np.atleast_2d(X), dtype=np.float64)
+        v = np.ascontiguousarray(np.atleast_2d(v), dtype=np.float64)
+        out = np.zeros((X.shape[0], self.nsp))
+        self._check(self.L.nuppn_dxdt(self.h, X.shape[0], _p(v), _p(X), X.shape[1], _p(out)))
+        return out
+
+    def calculate_jacobian(self, v, X, dt):
+        X = np.ascontiguousarray(np.atleast_2d(X), dtype=np.float64)
+        v = np.ascontiguousarray(np.atleast_2d(v), dtype=np.float64)
+        nz = X.shape[0]
+        dt = _f64(dt, nz)
+        nnz = self.info.nnz_jac
+        jac = np.zeros((nz, nnz)); es = np.zeros((nz, nnz), np.uint8); mask = np.zeros((nz, self.nsp), np.uint8)
+        self._check(self.L.nuppn_jacobian(self.h, nz, _p(v), _p(X), X.shape[1], _p(dt), _p(jac), _p(es), _p(mask)))
+        return jac, es, mask
+
+    def solve_reduced(self, jac, entry_set, mask, dt, b):
+        jac = np.ascontiguousarray(np.atleast_2d(jac), dtype=np.float64)
+        nz = jac.shape[0]
+        es = np.ascontiguousarray(np.atleast_2d(entry_set), dtype=np.uint8)
+        mk = np.ascontiguousarray(np.atleast_2d(mask), dtype=np.uint8)
+        b = np.ascontiguousarray(np.atleast_2d(b), dtype=np.float64)
+        dt = _f64(dt, nz)
+        x = np.zeros((nz, self.nsp))
+        self._check(self.L.nuppn_solve_reduced(self.h, nz, _p(jac), _p(es), _p(mk), _p(dt), _p(b), _p(x)))
+        return x
+
+    def integrate_network(self, X, t9_0, t9_1, rho_0, rho_1, ye, dtwant, bd_state=None):
+        """Advance every zone; returns (X, ye, ierr, stats, bd_state). X is not modified."""
+        X = np.array(np.atleast_2d(X), dtype=np.float64, order="C", copy=True)
+        nz = X.shape[0]
+        t9_0, t9_1, rho_0, rho_1 = _f64(t9_0, nz), _f64(t9_1, nz), _f64(rho_0, nz), _f64(rho_1, nz)
+        ye = np.array(_f64(ye, nz), copy=True)
+        dtwant = _f64(dtwant, nz)
+        ierr = np.zeros(nz, np.int32)
+        stats = (abi.ZoneStats * nz)()
+        bd = np.zeros(nz, np.int32) if bd_state is None else np.array(bd_state, dtype=np.int32, copy=True)
+        self._check(self.L.nuppn_integrate(self.h, nz, _p(X), X.shape[1], _p(t9_0), _p(t9_1), _p(rho_0),
+                                           _p(rho_1), _p(ye), _p(dtwant), _p(ierr), stats, _p(bd)))
+        return X, ye, ierr, stats, bd
+
+    def integrate_device(self, X, t9_0, t9_1, rho_0, rho_1, ye, dtwant, ierr, stats=None, bd_state=None,
+                         stream=0):
+        """Device-resident form: arguments are torch CUDA tensors (or objects with data_ptr())."""
+        ptr = lambda t: None if t is None else C.c_void_p(t.data_ptr())
+        self._check(self.L.nuppn_integrate_device(
+            self.h, X.shape[0], ptr(X), X.shape[1], ptr(t9_0), ptr(t9_1), ptr(rho_0), ptr(rho_1), ptr(ye),
+            ptr(dtwant), ptr(ierr), ptr(stats), ptr(bd_state), C.c_void_p(stream)))

@@ -1,0 +1,89 @@
+"""Seeded zone batches for the benchmark and parity cases (numpy default_rng, PCG64).
+
+* ``hburn_zone``    ppn-style single H-burning zone, ~300-species network, backward Euler,
+                    T9 = 0.020, rho = 100, X(H1) = 0.70, X(He4) = 0.28, Z = 0.02 over stable species,
+                    200 frame steps with dt log-spaced 1e3 .. 1e13 s.
+* ``heshell_batch`` He-burning shell zones on the ~1100-species network, Bader-Deuflhard:
+                    T9 ~ U[0.10, 0.30], rho log-U[1e2, 1e4], X(He4) = 0.97, X(C12) = 0.01,
+                    X(Ne22) = 0.02, trace Fe56 = 1e-3 (renormalised), each species x lognormal(0.05),
+                    one integrate_network call of 1e10 s per zone.
+"""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+
+from . import synthnet as sn
+
+
+@dataclasses.dataclass
+class ZoneBatch:
+    X: np.ndarray
+    t9_0: np.ndarray
+    t9_1: np.ndarray
+    rho_0: np.ndarray
+    rho_1: np.ndarray
+    ye: np.ndarray
+    dtwant: np.ndarray
+
+    @property
+    def nz(self):
+        return self.X.shape[0]
+
+    def take(self, idx):
+        return ZoneBatch(*(getattr(self, f.name)[idx] for f in dataclasses.fields(self)))
+
+
+def _ye_of(net: sn.Network, X: np.ndarray) -> np.ndarray:
+    """calculate_ye (utils.F90:537-553) on a batch, for the initial Ye of a composition."""
+    a = net.anetw.copy()
+    a[a == 0] = 1.0
+    eta = np.where(net.considerisotope.astype(bool), (net.anetw - 2.0 * net.znetw) * X / a, 0.0)
+    return (1.0 - eta.sum(axis=1)) * 0.5
+
+
+_NETS: dict = {}
+
+
+def network(nnn: int, seed: int = 20240611) -> sn.Network:
+    key = (nnn, seed)
+    if key not in _NETS:
+        _NETS[key] = sn.build_network(nnn, seed)
+    return _NETS[key]
+
+
+def heshell_batch(nz: int, net: sn.Network | None = None, seed: int = 2, dtwant: float = 1.0e10) -> ZoneBatch:
+    net = net or network(1107)
+    rng = np.random.default_rng(seed)
+    X = np.full((nz, net.nsp), 1.0e-99)
+    base = {"HE  4": 0.97, "C  12": 0.01, "NE 22": 0.02, "FE 56": 1.0e-3}
+    for name, x in base.items():
+        if name in net.zis:  # small networks may stop below Fe
+            X[:, net.species_index(name)] = x
+    X /= X.sum(axis=1, keepdims=True)
+    nonz = X > 1e-90
+    X = np.where(nonz, X * np.exp(rng.normal(0.0, 0.05, size=X.shape)), X)
+    X /= np.where(nonz, X, 0.0).sum(axis=1, keepdims=True) + np.where(~nonz, X, 0.0).sum(axis=1, keepdims=True)
+    t9 = rng.uniform(0.10, 0.30, nz)
+    rho = 10.0 ** rng.uniform(2.0, 4.0, nz)
+    return ZoneBatch(X=X, t9_0=t9.copy(), t9_1=t9.copy(), rho_0=rho.copy(), rho_1=rho.copy(),
+                     ye=_ye_of(net, X), dtwant=np.full(nz, dtwant))
+
+
+def hburn_zone(net: sn.Network | None = None) -> tuple[ZoneBatch, np.ndarray]:
+    """One H-burning zone and its 200 frame time steps (dt log-spaced 1e3 .. 1e13 s)."""
+    net = net or network(300)
+    X = np.full((1, net.nsp), 1.0e-99)
+    X[0, net.species_index("PROT ")] = 0.70
+    X[0, net.species_index("HE  4")] = 0.28
+    # metals: stable (near-valley) species, abundance falling with A (solar-scaled shape)
+    stable = [i for i in range(net.nsp) if net.considerisotope[i] and net.anetw[i] > 4
+              and abs((net.anetw[i] - net.znetw[i]) - sn.n_center(int(net.znetw[i]))) <= 1.0]
+    w = np.array([10.0 ** (-0.045 * net.anetw[i]) for i in stable])
+    X[0, stable] = 0.02 * w / w.sum()
+    X /= X.sum()
+    dts = 10.0 ** np.linspace(3.0, 13.0, 200)
+    zb = ZoneBatch(X=X, t9_0=np.array([0.020]), t9_1=np.array([0.020]), rho_0=np.array([100.0]),
+                   rho_1=np.array([100.0]), ye=_ye_of(net, X), dtwant=np.array([dts[0]]))
+    return zb, dts

@@ -1,0 +1,149 @@
+"""ctypes front end of the CPU checker (oracle/liboracle.so + the reference SuperLU in oracle/_ref).
+
+TEST INFRASTRUCTURE ONLY: tests/, __graft_entry__.smoke() and bench.py's CPU-baseline and reference
+arms load it as the checker. The product (the CUDA library) never uses it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+SLU = os.path.join(HERE, "_ref", "libslu_ref.so")
+
+_L = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB) and os.path.exists(SLU)
+
+
+def load():
+    global _L
+    if _L is not None:
+        return _L
+    if not available():
+        raise RuntimeError("oracle not built (make -C oracle oracle ref)")
+    L = C.CDLL(LIB)
+    vp, i32, d = C.c_void_p, C.c_int32, C.c_double
+    L.oracle_load_superlu.argtypes = [C.c_char_p]
+    if L.oracle_load_superlu(SLU.encode()) != 0:
+        raise RuntimeError("cannot load the reference SuperLU from " + SLU)
+    L.oracle_net_create.restype = vp
+    L.oracle_net_create.argtypes = [vp, vp]
+    L.oracle_net_destroy.argtypes = [vp]
+    L.oracle_nnz.argtypes = [vp]
+    L.oracle_jac_pattern.argtypes = [vp, vp, vp, vp]
+    L.oracle_eval_rates.argtypes = [vp, d, d, d, vp, vp]
+    L.oracle_dxdt.argtypes = [vp, vp, vp, vp]
+    L.oracle_jacobian.argtypes = [vp, vp, vp, d, vp, vp, vp]
+    L.oracle_solve_reduced.argtypes = [vp, vp, vp, vp, d, vp, vp]
+    L.oracle_integrate.argtypes = [vp, i32, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, i32]
+    L.oracle_calculate_ye.argtypes = [vp, vp]
+    L.oracle_calculate_ye.restype = d
+    L.oracle_sortedsum.argtypes = [vp, i32]
+    L.oracle_sortedsum.restype = d
+    _L = L
+    return L
+
+
+def _p(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+class Oracle:
+    def __init__(self, net, knobs):
+        from importlib import import_module
+        abi = import_module("nuppn_modular2-ininet3_b200.abi")
+        self.L = load()
+        self.net = net
+        self.knobs = knobs
+        self._desc = abi.make_desc(net)
+        self._abi = abi
+        self.h = self.L.oracle_net_create(C.byref(self._desc), C.byref(knobs))
+
+    def __del__(self):
+        try:
+            self.L.oracle_net_destroy(self.h)
+        except Exception:
+            pass
+
+    def nnz(self):
+        return self.L.oracle_nnz(self.h)
+
+    def jac_pattern(self):
+        n = self.nnz()
+        row = np.zeros(n, np.int32); col = np.zeros(n, np.int32)
+        dmap = np.zeros(self.net.nre * 8, np.int32)
+        self.L.oracle_jac_pattern(self.h, _p(row), _p(col), _p(dmap))
+        return row, col, dmap.reshape(-1, 8)
+
+    def evaluate_all_rates(self, t9, rho, ye, X):
+        X = np.ascontiguousarray(np.atleast_2d(X), dtype=np.float64)
+        out = np.zeros((X.shape[0], self.net.nre))
+        t9, rho, ye = (np.broadcast_to(np.asarray(a, float), (X.shape[0],)) for a in (t9, rho, ye))
+        for z in range(X.shape[0]):
+            row = np.ascontiguousarray(X[z]); o = np.zeros(self.net.nre)
+            self.L.oracle_eval_rates(self.h, float(t9[z]), float(rho[z]), float(ye[z]), _p(row), _p(o))
+            out[z] = o
+        return out
+
+    def calculate_dxdt(self, v, X):
+        X = np.atleast_2d(X); v = np.atleast_2d(v)
+        out = np.zeros((X.shape[0], self.net.nsp))
+        for z in range(X.shape[0]):
+            vr = np.ascontiguousarray(v[z], dtype=np.float64); xr = np.ascontiguousarray(X[z], dtype=np.float64)
+            o = np.zeros(self.net.nsp)
+            self.L.oracle_dxdt(self.h, _p(vr), _p(xr), _p(o))
+            out[z] = o
+        return out
+
+    def calculate_jacobian(self, v, X, dt):
+        X = np.atleast_2d(X); v = np.atleast_2d(v)
+        nz, n = X.shape[0], self.nnz()
+        dt = np.broadcast_to(np.asarray(dt, float), (nz,))
+        jac = np.zeros((nz, n)); es = np.zeros((nz, n), np.uint8); mk = np.zeros((nz, self.net.nsp), np.uint8)
+        for z in range(nz):
+            vr = np.ascontiguousarray(v[z], dtype=np.float64); xr = np.ascontiguousarray(X[z], dtype=np.float64)
+            j = np.zeros(n); e = np.zeros(n, np.uint8); m = np.zeros(self.net.nsp, np.uint8)
+            self.L.oracle_jacobian(self.h, _p(vr), _p(xr), float(dt[z]), _p(j), _p(e), _p(m))
+            jac[z], es[z], mk[z] = j, e, m
+        return jac, es, mk
+
+    def solve_reduced(self, jac, es, mask, dt, b):
+        jac = np.atleast_2d(jac); nz = jac.shape[0]
+        dt = np.broadcast_to(np.asarray(dt, float), (nz,))
+        x = np.zeros((nz, self.net.nsp)); ierr = np.zeros(nz, np.int32)
+        for z in range(nz):
+            xo = np.zeros(self.net.nsp)
+            ierr[z] = self.L.oracle_solve_reduced(
+                self.h, _p(np.ascontiguousarray(jac[z])), _p(np.ascontiguousarray(np.atleast_2d(es)[z])),
+                _p(np.ascontiguousarray(np.atleast_2d(mask)[z])), float(dt[z]),
+                _p(np.ascontiguousarray(np.atleast_2d(b)[z], dtype=np.float64)), _p(xo))
+            x[z] = xo
+        return x, ierr
+
+    def integrate_network(self, X, t9_0, t9_1, rho_0, rho_1, ye, dtwant, bd_state=None, nthreads=1):
+        X = np.array(np.atleast_2d(X), dtype=np.float64, order="C", copy=True)
+        nz = X.shape[0]
+        f = lambda a: np.ascontiguousarray(np.broadcast_to(np.asarray(a, float), (nz,)))
+        t9_0, t9_1, rho_0, rho_1, dtwant = f(t9_0), f(t9_1), f(rho_0), f(rho_1), f(dtwant)
+        ye = np.array(f(ye), copy=True)
+        ierr = np.zeros(nz, np.int32)
+        stats = (self._abi.ZoneStats * nz)()
+        bd = np.zeros(nz, np.int32) if bd_state is None else np.array(bd_state, dtype=np.int32, copy=True)
+        self.L.oracle_integrate(self.h, nz, _p(X), X.shape[1], _p(t9_0), _p(t9_1), _p(rho_0), _p(rho_1), _p(ye),
+                                _p(dtwant), _p(ierr), stats, _p(bd), int(nthreads))
+        return X, ye, ierr, stats, bd
+
+    def calculate_ye(self, X):
+        x = np.ascontiguousarray(X, dtype=np.float64)
+        return self.L.oracle_calculate_ye(self.h, _p(x))
+
+
+def sortedsum(a) -> float:
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return load().oracle_sortedsum(_p(a), len(a))

@@ -1,0 +1,178 @@
+"""CPU tests: the checker against its pins and invariants, the synthetic networks, and the C ABI
+library's exports (no device calls)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_superlu_matrixtest_pin(orc):
+    """slu_f90/matrixtest.f90: the reference's own 20x20 smoke system through slu_solve; x(1) =
+    0.38737081 is the value the reference prints."""
+    L = C.CDLL(orc.SLU)
+    n, nnz = 20, 24
+    val = np.array([1., 0.66004251, 1., 1., 0.16580944, 1., 1., 1., 1., 1., 0.48754192, 1., 1., 1., 1., 1.,
+                    1., 0.39321144, 1., 1., 1., 1., 1., 1.])
+    colind = (np.array([0, 2, 1, 2, 15, 3, 4, 5, 6, 7, 1, 8, 9, 10, 11, 12, 13, 10, 14, 15, 16, 17, 18, 19]) + 1).astype(np.int32)
+    rowptr = (np.array([0, 2, 3, 5, 6, 7, 8, 9, 10, 12, 13, 14, 15, 16, 17, 19, 20, 21, 22, 23, 24]) + 1).astype(np.int32)
+    rhs = np.array([0.36505416, 0.87209716, 0.11306562, 0.15746164, 0.36074325, 0.95214683, 0.97631797,
+                    0.26061262, 0.25675798, 0.75232693, 0.07135243, 0.07346062, 0.41943103, 0.48905309,
+                    0.12271773, 0.88581534, 0.99626864, 0.6568508, 0.63238463, 0.65226356])
+    b = rhs.copy()
+    ierr = C.c_int(0)
+    P = lambda a: C.c_void_p(a.ctypes.data)
+    L.slu_solve(n, nnz, 1, 1, P(val), P(colind), P(rowptr), P(b), C.byref(ierr))
+    assert ierr.value == 0
+    assert abs(b[0] - 0.38737081) < 5e-9
+    # residual of the unscaled system
+    A = np.zeros((n, n))
+    ci, rp = colind - 1 + 1, rowptr  # slu_solve shifted the index arrays to 0-based in place
+    for i in range(n):
+        for k in range(rp[i], rp[i + 1]):
+            A[i, ci[k]] = val[k]
+    assert np.abs(A @ b - rhs).max() < 1e-12
+
+
+def test_sortedsum_heapsort_order(orc):
+    rng = np.random.default_rng(0)
+    a = np.concatenate([10.0 ** rng.uniform(-30, 0, 500), -10.0 ** rng.uniform(-30, -5, 50)])
+    s = orc.sortedsum(a)
+    ref = 0.0
+    for x in np.sort(a):
+        ref = ref + x
+    assert s == ref
+
+
+@pytest.fixture(scope="module")
+def small(wl):
+    return wl.network(120)
+
+
+def test_network_layout(small, sn):
+    net = small
+    assert net.zis[net.igamma] == "OOOOO" and not net.considerisotope[net.igamma]
+    k = net.k[net.considerreaction == 1]
+    assert (k[:, [0, 2, 4, 6]] >= 0).all() and (k[:, [0, 2, 4, 6]] < net.nsp).all()
+    assert (k[:, 0] != net.igamma).all() and (k[:, 6] != net.igamma).all()
+    # triple alpha in the reference's slot 43 (1-based)
+    assert net.k[42, 0] == net.species_index("HE  4") and net.k[42, 1] == 3
+    # baryon number conserved by every considered reaction
+    A = net.anetw
+    lhs = A[k[:, 0]] * k[:, 1] + A[k[:, 2]] * k[:, 3]
+    rhs = A[k[:, 4]] * k[:, 5] + A[k[:, 6]] * k[:, 7]
+    assert np.allclose(lhs, rhs)
+    Z = net.znetw
+    lz = Z[k[:, 0]] * k[:, 1] + Z[k[:, 2]] * k[:, 3]
+    rz = Z[k[:, 4]] * k[:, 5] + Z[k[:, 6]] * k[:, 7]
+    # charge: network reactions other than weak ones (the VITAL block labels p(p,e+nu)d as (p,g))
+    idx = np.nonzero(net.considerreaction == 1)[0]
+    strong = ~np.isin(net.ilabb[idx], [13, 14, 15, 16]) & (idx >= net.nrcp)
+    assert np.allclose(lz[strong], rz[strong])
+
+
+def test_network_deterministic(sn):
+    a, b = sn.build_network(150, seed=3), sn.build_network(150, seed=3)
+    assert (a.k == b.k).all() and np.array_equal(a.rl_a, b.rl_a)
+
+
+def test_oracle_rhs_conserves_mass(orc, abi, small, wl):
+    """sum_i dX_i/dt = 0 for mass-conserving reactions (calculate_dxdt, jac_rhs.F90:217-278)."""
+    ref = orc.Oracle(small, abi.default_knobs())
+    zb = wl.heshell_batch(3, net=small, seed=4)
+    v = ref.evaluate_all_rates(zb.t9_0, zb.rho_0, zb.ye, zb.X)
+    d = ref.calculate_dxdt(v, zb.X)
+    scale = np.abs(d).max(axis=1)
+    assert (np.abs(d.sum(axis=1)) <= 1e-10 * scale).all()
+
+
+def test_oracle_detailed_balance_ratio(orc, abi, small, wl):
+    """v_rev / v_fwd equals the reverse.F90 factor before screening: checked with screening off."""
+    kn = abi.default_knobs(screen_option=0)
+    ref = orc.Oracle(small, kn)
+    zb = wl.heshell_batch(1, net=small, seed=4)
+    v = ref.evaluate_all_rates(zb.t9_0, zb.rho_0, zb.ye, zb.X)[0]
+    pairs = [(i, j) for i, j in enumerate(small.irev) if j >= 0 and small.considerreaction[i]]
+    assert pairs
+    kn0 = abi.default_knobs(screen_option=0, detailed_balance=0)
+    v0 = orc.Oracle(small, kn0).evaluate_all_rates(zb.t9_0, zb.rho_0, zb.ye, zb.X)[0]
+    # without detailed balance the 'RVRSE' slots are not gathered (clipped to 1e-99)
+    assert all(v0[j] == 1e-99 for _, j in pairs)
+    changed = [j for i, j in pairs if v[i] > 1e-97]
+    assert any(v[j] > 1e-99 for j in changed)
+
+
+def test_oracle_jacobian_is_dfdx(orc, abi, small, wl):
+    """calculate_jacobian values are the derivative of dxdt (finite differences on a few columns)."""
+    ref = orc.Oracle(small, abi.default_knobs())
+    zb = wl.heshell_batch(1, net=small, seed=9)
+    X = zb.X[0].copy()
+    X[X < 1e-20] = 1e-6  # move every species off the floor so derivatives are well defined
+    X /= X.sum()
+    v = ref.evaluate_all_rates(zb.t9_0, zb.rho_0, zb.ye, X)
+    jac, es, mk = ref.calculate_jacobian(v, X, 1.0)
+    row, col, _ = ref.jac_pattern()
+    J = {}
+    for e in range(len(row)):
+        J[(row[e], col[e])] = jac[0, e] - 1e-99
+    d0 = ref.calculate_dxdt(v, X)[0]
+    for j in [small.species_index(s) for s in ("HE  4", "C  12", "NE 22")]:
+        h = X[j] * 1e-6
+        Xp = X.copy(); Xp[j] += h
+        fd = (ref.calculate_dxdt(v, Xp)[0] - d0) / h
+        for i in range(small.nsp):
+            if i == small.igamma:
+                continue
+            ana = J.get((i, j), 0.0)
+            # finite-difference round-off: a few ulps of dxdt_i divided by the step
+            fd_noise = 64 * np.finfo(float).eps * abs(d0[i]) / h
+            assert abs(fd[i] - ana) <= 1e-4 * max(abs(ana), abs(fd[i])) + fd_noise
+
+
+def test_oracle_bd_conserves_mass(orc, abi, wl):
+    net = wl.network(200)
+    ref = orc.Oracle(net, abi.default_knobs(integration_method=1))
+    zb = wl.heshell_batch(2, net=net, seed=5)
+    X, ye, ierr, st, _ = ref.integrate_network(zb.X, zb.t9_0, zb.t9_1, zb.rho_0, zb.rho_1, zb.ye, zb.dtwant)
+    assert (ierr == 0).all()
+    assert np.abs(X.sum(axis=1) - 1).max() < 1e-12
+    assert all(s.nsucc >= 1 for s in st)
+    # Ye from composition (calculate_ye) of the last sub-step, before the final renormalisation
+    # of solver.F90:234, so equal to the Ye of the returned X only to the size of that correction
+    for z in range(2):
+        assert abs(ye[z] - ref.calculate_ye(X[z])) < 1e-8
+
+
+def test_oracle_bd_order_on_linear_decay(orc, abi, sn, wl):
+    """Bader-Deuflhard on a chain whose solution is analytic: the He-shell batch with strong rates
+    switched off leaves pure beta decays; conservation and positivity must hold."""
+    net = wl.network(120)
+    kn = abi.default_knobs(integration_method=1, strong_rates=0)
+    ref = orc.Oracle(net, kn)
+    zb = wl.heshell_batch(1, net=net, seed=6)
+    X, ye, ierr, st, _ = ref.integrate_network(zb.X, zb.t9_0, zb.t9_1, zb.rho_0, zb.rho_1, zb.ye, zb.dtwant)
+    assert ierr[0] == 0
+    assert (X >= 1e-99).all()
+
+
+def test_library_exports_header_symbols(solver_mod):
+    """Every function declared in include/nuppn.h is exported by the built library."""
+    hdr = open(os.path.join(ROOT, "include", "nuppn.h")).read()
+    names = sorted(set(re.findall(r"\b(nuppn_[a-z_]+)\s*\(", hdr)))
+    assert len(names) >= 14
+    L = solver_mod.load_library()
+    for n in names:
+        assert hasattr(L, n), n
+    assert L.nuppn_abi_version() == 1
+
+
+def test_no_cpu_fallback_in_product(solver_mod):
+    """The product package never loads the checker."""
+    pkgdir = os.path.join(ROOT, "nuppn_modular2-ininet3_b200")
+    for f in os.listdir(pkgdir):
+        if f.endswith(".py"):
+            src = open(os.path.join(pkgdir, f)).read()
+            assert "oracle" not in src.replace("reference", ""), f
