@@ -161,7 +161,8 @@ def test_oracle_bd_order_on_linear_decay(orc, abi, sn, wl):
 def test_library_exports_header_symbols(solver_mod):
     """Every function declared in include/nuppn.h is exported by the built library."""
     hdr = open(os.path.join(ROOT, "include", "nuppn.h")).read()
-    names = sorted(set(re.findall(r"\b(nuppn_[a-z_]+)\s*\(", hdr)))
+    names = sorted(set(re.findall(
+        r"^(?:nuppn_status|int32_t|int64_t|void|const char \*)\s*(nuppn_[a-z_]+)\(", hdr, re.M)))
     assert len(names) >= 14
     L = solver_mod.load_library()
     for n in names:
