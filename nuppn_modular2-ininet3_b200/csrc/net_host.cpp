@@ -58,9 +58,12 @@ std::vector<int> min_degree(int n, const std::vector<std::vector<int>> &adj0, co
   for (int i = 0; i < n; ++i) adj[i] = std::set<int>(adj0[i].begin(), adj0[i].end());
   std::vector<char> alive(n, 1), islast(n, 0);
   for (int v : last) islast[v] = 1;
-  std::set<std::pair<int, int>> pq;  // (degree, node)
-  for (int i = 0; i < n; ++i)
-    if (!islast[i]) pq.insert({(int)adj[i].size(), i});
+  std::set<std::pair<int, int>> pq;  // (degree, node); deg[] holds the key stored for each node
+  std::vector<int> deg(n);
+  for (int i = 0; i < n; ++i) {
+    deg[i] = (int)adj[i].size();
+    if (!islast[i]) pq.insert({deg[i], i});
+  }
   std::vector<int> order;
   order.reserve(n);
   while (!pq.empty()) {
@@ -70,15 +73,14 @@ std::vector<int> min_degree(int n, const std::vector<std::vector<int>> &adj0, co
     alive[v] = 0;
     std::vector<int> nb(adj[v].begin(), adj[v].end());
     for (int a : nb) adj[a].erase(v);
-    for (size_t x = 0; x < nb.size(); ++x) {
-      int a = nb[x];
-      int before = (int)adj[a].size();
+    for (size_t x = 0; x < nb.size(); ++x)
       for (size_t y = 0; y < nb.size(); ++y)
-        if (x != y) adj[a].insert(nb[y]);
-      if (!islast[a] && (int)adj[a].size() != before) {
-        pq.erase({before, a});
-        pq.insert({(int)adj[a].size(), a});
-      }
+        if (x != y) adj[nb[x]].insert(nb[y]);
+    for (int a : nb) {
+      if (islast[a] || (int)adj[a].size() == deg[a]) continue;
+      pq.erase({deg[a], a});
+      deg[a] = (int)adj[a].size();
+      pq.insert({deg[a], a});
     }
     adj[v].clear();
   }

@@ -68,10 +68,14 @@ def _p(a):
 
 
 def _f64(a, n=None):
-    a = np.ascontiguousarray(a, dtype=np.float64)
-    if n is not None and a.shape == ():
-        a = np.full(n, float(a))
-    return a
+    """Per-zone float64 array; a scalar (or a length-1 array) is broadcast to n zones."""
+    a = np.asarray(a, dtype=np.float64)
+    if n is not None:
+        if a.size == 1:
+            a = np.full(n, float(a.reshape(-1)[0]))
+        elif a.shape != (n,):
+            raise ValueError(f"expected {n} per-zone values, got shape {a.shape}")
+    return np.ascontiguousarray(a)
 
 
 class NetworkSolver:
