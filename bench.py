@@ -1,0 +1,293 @@
+"""Benchmark: zone-timesteps/s of batched Bader-Deuflhard integration on the ~1100-species network.
+
+Workload (one GPU): 1024 independent He-burning shell zones on the 1109-slot synthetic network
+(NNN = 1107), T9 ~ U[0.10, 0.30], rho log-U[1e2, 1e4], X(He4)=0.97, X(C12)=0.01, X(Ne22)=0.02,
+Fe56=1e-3 (renormalised) x lognormal(0.05) per species, one integrate_network call of 1e10 s per zone
+with adaptive Bader-Deuflhard steps, FP64. A "step" is one call over the whole batch, restarted from
+the same initial state. The metric counts accepted sub-steps (zone-timesteps) per second.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--nz Z] [--lu fp64|mixed]
+
+--impl reference times the reference's own algorithm on the host cores (the CPU restatement of
+NuPPN's FP64 path, calling the reference's SuperLU) on a bounded sample of the same workload.
+For N > 1 (torchrun) the zones are sharded across ranks; there is no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import importlib
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+PKG = "nuppn_modular2-ininet3_b200"
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[3 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def algorithmic_bytes(info, stats_np, nre_active, nsp):
+    """Bytes a zone-step must move at minimum (per-zone arrays, each read/written once per use):
+    8 * [ rates (R+3) + per Jacobian nnzJ + per factorization (nnzJ + nnzLU)
+          + per RHS+solve (R + 3N + nnzLU) ]."""
+    R, N, nnzJ, nnzLU = nre_active, nsp, info.nnz_jac, info.nnz_lu
+    nsucc, nfail, nfact, nsolve = (stats_np[:, i].astype(np.int64) for i in (0, 1, 3, 4))
+    per_zone = (R + 3) + (nsucc + nfail) * nnzJ + nfact * (nnzJ + nnzLU) + nsolve * (R + 3 * N + nnzLU)
+    return 8 * int(per_zone.sum())
+
+
+def run_reference(args, rank, world):
+    """CPU reference arm: the checker (restated FP64 path + reference SuperLU), all host threads."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    wl = importlib.import_module(PKG + ".workloads")
+    abi = importlib.import_module(PKG + ".abi")
+    net = wl.network(1107)
+    zb = wl.heshell_batch(args.nz, net=net, seed=2)
+    cores = os.cpu_count() or 1
+    sample = min(args.nz, max(cores, args.ref_zones))
+    sub = zb.take(np.arange(sample))
+    ref = orc.Oracle(net, abi.default_knobs(integration_method=1))
+    times, steps = [], []
+    for it in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        X, ye, ierr, st, _ = ref.integrate_network(sub.X, sub.t9_0, sub.t9_1, sub.rho_0, sub.rho_1, sub.ye,
+                                                   sub.dtwant, nthreads=cores)
+        dt = time.perf_counter() - t0
+        if it >= args.warmup:
+            times.append(dt)
+            steps.append(sum(s.nsucc for s in st))
+    v = sum(steps) / sum(times)
+    line = {"impl": "reference", "metric": "zone-timesteps/s", "value": v, "unit": "zone-timesteps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "heshell-1107 BD 1e10 s", "zones": args.nz, "sample_zones": sample,
+                       "network_species": net.nsp, "integrator": "bader-deuflhard"},
+            "cpu_baseline": {"value": v, "unit": "zone-timesteps/s", "cores": cores, "kind": "port",
+                             "sample": f"{sample} of {args.nz} zones per step, restated FP64 path + "
+                                       f"reference SuperLU 5.0"},
+            "e2e": {"value": v, "unit": "zone-timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nz", type=int, default=1024)
+    ap.add_argument("--lu", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--ref-zones", type=int, default=32)
+    ap.add_argument("--cpu-zones", type=int, default=16)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dev_id = torch.cuda.current_device()
+
+    abi = importlib.import_module(PKG + ".abi")
+    wl = importlib.import_module(PKG + ".workloads")
+    solver = importlib.import_module(PKG + ".solver")
+    net = wl.network(1107)
+    zb_all = wl.heshell_batch(args.nz * world, net=net, seed=2)
+    zb = zb_all.take(np.arange(rank * args.nz, (rank + 1) * args.nz))  # weak scaling: shard of zones
+    knobs = abi.default_knobs(integration_method=1, lu_precision=1 if args.lu == "mixed" else 0)
+    S = solver.NetworkSolver(net, knobs, device=dev_id)
+    nz = zb.nz
+
+    cu = lambda a, dt=torch.float64: torch.tensor(np.ascontiguousarray(a), dtype=dt, device="cuda")
+    X0, ye0 = cu(zb.X), cu(zb.ye)
+    t9a, t9b, rha, rhb, dtw = cu(zb.t9_0), cu(zb.t9_1), cu(zb.rho_0), cu(zb.rho_1), cu(zb.dtwant)
+    X, ye = X0.clone(), ye0.clone()
+    ierr = torch.zeros(nz, dtype=torch.int32, device="cuda")
+    stats = torch.zeros((nz, 8), dtype=torch.int32, device="cuda")
+    bd = torch.zeros(nz, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def one_step():
+        X.copy_(X0); ye.copy_(ye0); bd.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        S.integrate_device(X, t9a, t9b, rha, rhb, ye, dtw, ierr, stats, bd, stream=stream)
+        e1.record()
+        return e0, e1
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = S.launches()
+    ev = []
+    steps_done = 0
+    with ClockSampler(dev_id) as clk:
+        for _ in range(args.steps):
+            ev.append(one_step())
+        torch.cuda.synchronize()
+    st_np = stats.cpu().numpy()
+    steps_done = int(st_np[:, 0].sum()) * args.steps  # identical work every step (same inputs)
+    kernel_ms = [a.elapsed_time(b) for a, b in ev]
+    t_ms = float(sum(kernel_ms))
+    gpu_launches = S.launches() - launches0
+    if world > 1:
+        t = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms = float(t.item())
+        s = torch.tensor([steps_done], device="cuda", dtype=torch.float64)
+        dist.all_reduce(s, op=dist.ReduceOp.SUM)
+        steps_done = int(s.item())
+    value = steps_done / (t_ms * 1e-3)
+
+    # end to end through the host-buffer entry point (host <-> device copies inside)
+    Xh = np.ascontiguousarray(zb.X)
+    e2e_t, e2e_steps = 0.0, 0
+    for it in range(2 + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        Xo, yeo, ie, st, _ = S.integrate_network(Xh, zb.t9_0, zb.t9_1, zb.rho_0, zb.rho_1, zb.ye, zb.dtwant)
+        dt = time.perf_counter() - t0
+        if it >= 2:
+            e2e_t += dt
+            e2e_steps += sum(s.nsucc for s in st)
+    h2d = Xh.nbytes + 6 * 8 * nz + 4 * nz
+    d2h = Xh.nbytes + 8 * nz + 4 * nz + 32 * nz + 4 * nz
+    if world > 1:
+        t = torch.tensor([e2e_t], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+        s = torch.tensor([e2e_steps], device="cuda", dtype=torch.float64)
+        dist.all_reduce(s, op=dist.ReduceOp.SUM)
+        e2e_steps = int(s.item())
+    e2e = e2e_steps / e2e_t
+
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        nre_active = int(net.considerreaction.sum())
+        bytes_per_launch = algorithmic_bytes(S.info, st_np, nre_active, net.nsp)
+        per_launch_s = (sum(kernel_ms) / len(kernel_ms)) * 1e-3
+        achieved = bytes_per_launch / per_launch_s / 1e9
+        line = {
+            "metric": "zone-timesteps/s", "value": value, "unit": "zone-timesteps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.lu == "fp64" else "f64+f32-lu", "data": "synthetic",
+            "config": {"workload": "heshell-1107 BD 1e10 s", "zones": nz * world, "zones_per_gpu": nz,
+                       "network_species": net.nsp, "nnz_jac": S.info.nnz_jac, "nnz_lu": S.info.nnz_lu,
+                       "integrator": "bader-deuflhard", "lu": args.lu,
+                       "l2": "per-zone workspace (>1 GB) exceeds L2; no flush needed",
+                       "accepted_steps_per_call": int(st_np[:, 0].sum()),
+                       "rejected_steps_per_call": int(st_np[:, 1].sum())},
+            "gpu_launches": int(gpu_launches),
+            "e2e": {"value": e2e, "unit": "zone-timesteps/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": peak_kind, "kernel": "k_integrate",
+                         "algorithmic_bytes_per_launch": bytes_per_launch},
+            "clocks": clk.summary(),
+        }
+        if not args.no_cpu:
+            line["cpu_baseline"] = cpu_baseline(net, zb, args.cpu_zones)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline(net, zb, nzones):
+    """The checker on the host cores, a bounded sample of the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    abi = importlib.import_module(PKG + ".abi")
+    if not orc.available():
+        return {"value": None, "unit": "zone-timesteps/s", "cores": 0, "kind": "port", "sample": "unavailable"}
+    cores = os.cpu_count() or 1
+    n = min(zb.nz, max(nzones, cores))
+    sub = zb.take(np.arange(n))
+    ref = orc.Oracle(net, abi.default_knobs(integration_method=1))
+    t0 = time.perf_counter()
+    X, ye, ierr, st, _ = ref.integrate_network(sub.X, sub.t9_0, sub.t9_1, sub.rho_0, sub.rho_1, sub.ye,
+                                               sub.dtwant, nthreads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": sum(s.nsucc for s in st) / dt, "unit": "zone-timesteps/s", "cores": cores, "kind": "port",
+            "sample": f"{n} zones of the same batch (restated FP64 path + reference SuperLU), {dt:.1f} s"}
+
+
+if __name__ == "__main__":
+    main()

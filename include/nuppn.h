@@ -94,7 +94,9 @@ typedef struct nuppn_knobs {
   int32_t ir_max_iters;        /* refinement sweeps per solve in mode 1 (default 3)           */
   double ir_rtol;              /* refinement stops when |dx| <= ir_rtol*|x| (default 1e-14)   */
   int32_t threads_per_zone;    /* CTA size (0 = library choice)                               */
-  int32_t reserved[7];
+  int32_t lu_onewarp_max;      /* active systems up to this size are factored/solved by one warp
+                                  (0 = library default; larger ones use sync-free multi-warp)    */
+  int32_t reserved[6];
 } nuppn_knobs;
 
 /* Network description in the reference's slot layout (what rnetw2007, reaclib_init, netgen_init,
@@ -173,7 +175,7 @@ typedef struct nuppn_zone_stats {
   int32_t nsolve;         /* triangular solve pairs                                               */
   int32_t nvar1_last;     /* species in the last dynamic-network solve                            */
   int32_t ir_sweeps;      /* refinement sweeps (mixed precision)                                  */
-  int32_t reserved;
+  int32_t nvar1_max;      /* largest dynamic-network solve of the call                            */
 } nuppn_zone_stats;
 
 /* -- library --------------------------------------------------------------------------------- */

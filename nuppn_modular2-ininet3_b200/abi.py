@@ -36,7 +36,7 @@ class Knobs(C.Structure):
                 ("delta_state_max", C.c_double), ("nse_min_t9", C.c_double),
                 ("lu_precision", C.c_int32), ("ir_max_iters", C.c_int32),
                 ("ir_rtol", C.c_double), ("threads_per_zone", C.c_int32),
-                ("reserved", C.c_int32 * 7)]
+                ("lu_onewarp_max", C.c_int32), ("reserved", C.c_int32 * 6)]
 
 
 def default_knobs(**over) -> Knobs:
@@ -94,7 +94,7 @@ class NetDesc(C.Structure):
 class ZoneStats(C.Structure):
     _fields_ = [("nsucc", C.c_int32), ("nfail", C.c_int32), ("newton_iters", C.c_int32),
                 ("nfact", C.c_int32), ("nsolve", C.c_int32), ("nvar1_last", C.c_int32),
-                ("ir_sweeps", C.c_int32), ("reserved", C.c_int32)]
+                ("ir_sweeps", C.c_int32), ("nvar1_max", C.c_int32)]
 
 
 class NetInfo(C.Structure):

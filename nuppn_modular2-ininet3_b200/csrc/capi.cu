@@ -17,11 +17,12 @@
 #include "nuppn_internal.h"
 
 namespace nuppn {
-cudaError_t launch_integrate(const DevNet &N, const WsLayout &L, char *ws, int grid, int block,
+cudaError_t launch_integrate(const DevNet &N, const WsLayout &L, char *ws, int grid, int block, int act_smem,
                              const IntegrateArgs &A, cudaStream_t st);
-cudaError_t launch_phase(const DevNet &N, const WsLayout &L, char *ws, int grid, int block, const PhaseArgs &A,
-                         cudaStream_t st);
-cudaError_t occupancy_integrate(int block, int *per_sm);
+cudaError_t launch_phase(const DevNet &N, const WsLayout &L, char *ws, int grid, int block, int act_smem,
+                         const PhaseArgs &A, cudaStream_t st);
+cudaError_t configure_kernels(int act_smem);
+cudaError_t occupancy_integrate(int block, int act_smem, int *per_sm);
 }  // namespace nuppn
 
 using namespace nuppn;
@@ -66,6 +67,7 @@ struct nuppn_net {
   DevBuf ws, stage, counter;
   int ws_slots = 0;
   int block = 256;
+  int act_smem = 64 * 1024;  // shared-memory budget per CTA for the active-subsystem LU
   int device = 0;
   int nsm = 0;
   int64_t launches = 0;
@@ -114,7 +116,7 @@ nuppn_status upload(nuppn_net *net) {
   P(H.fft9); P(H.ffrho); P(H.ffl10v); P(H.kdE); P(H.kdcoef); P(H.constr);
   P(H.jrow); P(H.jcol); P(H.jdiag); P(H.jg_ptr); P(H.jg_item); P(H.dg_ptr); P(H.dg_item); P(H.dg_coef);
   P(H.jg_long); P(H.dg_long);
-  P(H.sys_of_sp); P(H.sp_of_sys); P(H.pos_of_entry); P(H.lu_rowptr); P(H.lu_diag); P(H.lu_col); P(H.upd_start);
+  P(H.sys_of_sp); P(H.sp_of_sys); P(H.pos_of_entry); P(H.lu_src); P(H.lu_rowptr); P(H.lu_diag); P(H.lu_col); P(H.upd_start);
   P(H.upd_off); P(H.lvL_ptr); P(H.lvL_rows); P(H.lvL_grp); P(H.lvU_ptr); P(H.lvU_rows); P(H.lvU_grp);
   CK(cudaMalloc(&net->arena, A.total));
   net->arena_bytes = A.total;
@@ -146,6 +148,7 @@ nuppn_status upload(nuppn_net *net) {
   D.dg_item = (const int *)nx(); D.dg_coef = (const double *)nx();
   D.jg_long = (const int *)nx(); D.dg_long = (const int *)nx();
   D.sys_of_sp = (const int *)nx(); D.sp_of_sys = (const int *)nx(); D.pos_of_entry = (const int *)nx();
+  D.lu_src = (const int *)nx();
   D.lu_rowptr = (const int *)nx(); D.lu_diag = (const int *)nx(); D.lu_col = (const int *)nx();
   D.upd_start = (const int *)nx(); D.upd_off = (const uint16_t *)nx();
   D.lvL_ptr = (const int *)nx(); D.lvL_rows = (const int *)nx(); D.lvL_grp = (const int *)nx();
@@ -181,6 +184,20 @@ WsLayout layout(const HostNet &H) {
   L.yscal = take(H.nsp * d); L.qcol = take((size_t)(kMaxLevels + 1) * H.nsp * d);
   L.yerr = take((size_t)(kMaxLevels + 1) * H.nsp * d); L.lu = take((size_t)H.nnzLU * d);
   L.bsys = take(H.nsys * d); L.xsys = take(H.nsys * d); L.rhs = take(H.nsp * d);
+  L.act_tmp = take((size_t)4 * (H.nsys + 1) * sizeof(int));
+  L.act = take(act_bytes(H.nsys, H.nnzLU, 8));
+  L.act_rtmp = take((size_t)(H.nact + 1) * sizeof(int));
+  {
+    auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };
+    size_t ngi = H.dg_item.size(), nar = H.nact, na = H.nsys;
+    L.act_r = take(a16(nar * 4) + a16((na + 1) * 4) + a16(ngi * 4) + a16(ngi * 4) + a16(nar * 8));
+    size_t njg = H.jg_item.size();
+    L.act_itmp = take((std::max(ngi, njg) + 1) * sizeof(int));
+    L.act_otmp = take(((size_t)H.nnzLU + 1) * sizeof(int));
+    L.act_dtmp = take(njg * sizeof(double));
+    L.act_btmp = take(njg);
+    L.bd = take((size_t)(2 * kMaxLevels + 8) * H.nsys * sizeof(double));
+  }
   L.bytes = t;
   return L;
 }
@@ -194,7 +211,7 @@ nuppn_status ensure_ws(nuppn_net *net, int slots) {
 
 int resident_slots(nuppn_net *net) {
   int per = 0;
-  if (occupancy_integrate(net->block, &per) != cudaSuccess || per <= 0) per = 1;
+  if (occupancy_integrate(net->block, net->act_smem, &per) != cudaSuccess || per <= 0) per = 1;
   return per * net->nsm;
 }
 
@@ -282,6 +299,11 @@ nuppn_status nuppn_net_create(const nuppn_net_desc *desc, const nuppn_knobs *kno
   if (net->block % 32 || net->block > 256) { delete net; set_error("threads_per_zone must be a multiple of 32, <= 256"); return NUPPN_ERR_ARG; }
   nuppn_status st = upload(net);
   if (st != NUPPN_OK) { delete net; return st; }
+  if (configure_kernels(net->act_smem) != cudaSuccess) {
+    set_error("cannot configure dynamic shared memory");
+    nuppn_net_destroy(net);
+    return NUPPN_ERR_CUDA;
+  }
   net->L = layout(net->H);
   if (net->counter.ensure(256) != cudaSuccess) { delete net; set_error("counter alloc"); return NUPPN_ERR_NOMEM; }
   *out = net;
@@ -375,7 +397,7 @@ static nuppn_status run_phase(nuppn_net *net, int nz, int op, const double *X, i
   A.out_v = out_v ? (double *)(sb + oov) : nullptr; A.out_dxdt = out_dxdt ? (double *)(sb + ood) : nullptr;
   A.out_jac = out_jac ? (double *)(sb + ooj) : nullptr; A.out_eset = out_eset ? (uint8_t *)(sb + ooe) : nullptr;
   A.out_mask = out_mask ? (uint8_t *)(sb + oom) : nullptr; A.out_x = out_x ? (double *)(sb + oox) : nullptr;
-  CK(launch_phase(net->D, net->L, (char *)net->ws.p, grid, net->block, A, 0));
+  CK(launch_phase(net->D, net->L, (char *)net->ws.p, grid, net->block, net->act_smem, A, 0));
   net->launches++;
   CK(cudaDeviceSynchronize());
   auto down = [&](void *dst, size_t off, size_t bytes) -> cudaError_t {
@@ -436,7 +458,7 @@ nuppn_status nuppn_integrate_device(nuppn_net *net, int32_t nz, double *d_X, int
   A.nz = nz; A.ldx = ldx; A.X = d_X; A.t9_0 = d_t9_0; A.t9_1 = d_t9_1; A.rho_0 = d_rho_0; A.rho_1 = d_rho_1;
   A.dtwant = d_dtwant; A.ye = d_ye; A.ierr = d_ierr; A.stats = d_stats; A.bd_state = d_bd_state;
   A.counter = (int *)net->counter.p;
-  CK(launch_integrate(net->D, net->L, (char *)net->ws.p, grid, net->block, A, s));
+  CK(launch_integrate(net->D, net->L, (char *)net->ws.p, grid, net->block, net->act_smem, A, s));
   net->launches++;
   return NUPPN_OK;
 }

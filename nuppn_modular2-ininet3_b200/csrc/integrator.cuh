@@ -4,7 +4,11 @@
 // bader_deuflhard_integration and helpers   solver/source/bader_deuflhard.F90:139-488
 // integrate_network / do_one_time_step      solver/source/solver.F90:53-274
 //
-// All threads of the CTA run this control flow with identical scalars.
+// All threads of the CTA run this control flow with identical scalars. Within one step only the
+// species of the dynamic network change (the reference's correction is zero elsewhere,
+// ddecompac, jac_rhs.F90:584-608), so the Bader-Deuflhard vectors are kept on the active rows only;
+// for frozen species the extrapolation tableau is exact (a constant column), their error terms are
+// zero, and their share of the mass sum and of the negative-abundance test is a per-step constant.
 #pragma once
 
 namespace nuppn {
@@ -16,6 +20,10 @@ struct ZoneCtl {
   double sumerr;  // kept between levels like the reference's module variable
   double err[kMaxLevels + 1];
   double xhist[kMaxLevels + 1];
+  char *smem;     // dynamic shared memory for the active subsystem
+  int smem_bytes;
+  int *sint;      // shared scan scratch (>= 32 ints)
+  Act act;        // active subsystem of the current Jacobian
 };
 
 __device__ void vcopy(double *dst, const double *src, int n) {
@@ -55,12 +63,23 @@ __device__ double dev_ye(const DevNet &N, const double *x, double *sred) {
   return (1.0 - s) * 0.5;
 }
 
+// Jacobian pass, compaction, active Jacobian and restricted right-hand side for abundances y
+__device__ void dev_new_jacobian(const DevNet &N, const Ws &W, ZoneCtl &C, double dt, const double *y) {
+  dev_jacobian_mask(N, W, dt, y);
+  dev_compact(N, W, C.act, C.smem, C.smem_bytes, C.sint);
+  dev_jacobian_active(N, W, C.act, C.sint);
+  dev_compact_rhs(N, W, C.act, C.smem, C.smem_bytes, C.sint);
+  C.st.nvar1_last = C.act.na;
+  C.st.nvar1_max = max(C.st.nvar1_max, C.act.na);
+}
+
 // ---------------------------------------------------------------------------------------------
 __device__ int dev_backward_euler(const DevNet &N, const Ws &W, ZoneCtl &C, double *yps, double dt, double &dtrcmd,
                                   double *sred) {
   const int nsp = N.nsp, tid = threadIdx.x, nt = blockDim.x;
   const double rmin = 0.2, rmax = 2.0, dgrd = N.kn.dgrd;
   const double sum_check = N.kn.grdthreshold * N.nvar * dgrd;
+  double *yc = W.bd, *dxc = W.bd + N.nsys;
   for (int i = tid; i < nsp; i += nt) { W.y_new[i] = yps[i]; W.y_old[i] = yps[i]; W.y_cur[i] = yps[i]; }
   __syncthreads();
   int iter = 0;
@@ -76,19 +95,27 @@ __device__ int dev_backward_euler(const DevNet &N, const Ws &W, ZoneCtl &C, doub
       dtrcmd = fmax(fmin(pow(tol / fmax(err, K_SMALL), 0.5), rmax), rmin) * dt;
       return ierr;
     }
-    // newton_iteration (backward_euler.F90:120-176)
-    dev_jacobian(N, W, dt, W.y_cur);
-    dev_assemble_factor(N, W, dt);
-    dev_dxdt(N, W, W.y_cur, W.dxdt);
-    for (int i = tid; i < nsp; i += nt) W.rhs[i] = W.y_old[i] - W.y_cur[i] + dt * W.dxdt[i];
+    // newton_iteration (backward_euler.F90:120-176) on the dynamic network
+    dev_new_jacobian(N, W, C, dt, W.y_cur);
+    Act &A = C.act;
+    bool ok = dev_factor_active(N, W, A, dt);
+    for (int c = tid; c < A.na; c += nt) yc[c] = W.y_cur[N.sp_of_sys[A.arow[c]]];
     __syncthreads();
-    dev_solve(N, W, W.rhs, W.delta_k);  // delta_k doubles as the correction buffer here
+    dev_dxdt_active(N, W, A, yc, dxc);
+    for (int c = tid; c < A.na; c += nt) {
+      const int s = N.sp_of_sys[A.arow[c]];
+      A.xs[c] = W.y_old[s] - W.y_cur[s] + dt * dxc[c];
+    }
+    __syncthreads();
+    ok = dev_solve_active(A) && ok;
+    if (!ok) return BAD_STEP;
     C.st.nfact++; C.st.nsolve++;
     double g = 0.0;
-    for (int i = tid; i < nsp; i += nt) {
-      double yn = W.mask[i] ? W.y_cur[i] + W.delta_k[i] : W.y_new[i];
-      W.y_new[i] = yn;
-      if (W.y_cur[i] > N.kn.grdthreshold) g = fmax(g, fabs((yn - W.y_cur[i]) / W.y_cur[i]));
+    for (int c = tid; c < A.na; c += nt) {  // unmasked species keep y_new = y_cur (zero correction)
+      const int s = N.sp_of_sys[A.arow[c]];
+      const double yn = W.y_cur[s] + A.xs[c];
+      W.y_new[s] = yn;
+      if (W.y_cur[s] > N.kn.grdthreshold) g = fmax(g, fabs((yn - W.y_cur[s]) / W.y_cur[s]));
     }
     grd = block_max(g, sred);
     iter++;
@@ -106,107 +133,143 @@ __device__ int dev_backward_euler(const DevNet &N, const Ws &W, ZoneCtl &C, doub
 }
 
 // ---------------------------------------------------------------------------------------------
-// one semi-implicit midpoint sub-step, bader_deuflhard_step (bader_deuflhard.F90:410-488)
-__device__ int dev_bd_substep(const DevNet &N, const Ws &W, ZoneCtl &C, double h, int stage, double *sred) {
-  const int nsp = N.nsp, tid = threadIdx.x, nt = blockDim.x;
-  dev_dxdt(N, W, W.y_k, W.dxdt);
-  if (stage == 1) for (int i = tid; i < nsp; i += nt) W.rhs[i] = h * W.dxdt[i];
-  else for (int i = tid; i < nsp; i += nt) W.rhs[i] = h * W.dxdt[i] - W.delta_k[i];
-  __syncthreads();
-  dev_solve(N, W, W.rhs, W.y_ext);  // y_ext doubles as the solution buffer here
-  C.st.nsolve++;
-  bool huge = false;
-  for (int i = tid; i < nsp; i += nt) {
-    double d = stage == 2 ? W.delta_k[i] + 2.0 * W.y_ext[i] : W.y_ext[i];
-    W.delta_k[i] = d;
-    double yk = W.y_k[i] + d;
-    W.y_k[i] = yk;
-    if (yk > 2.0) huge = true;
-  }
-  return block_any(huge) ? HUGE_ABUNDS : 0;
+// Compact Bader-Deuflhard vectors (indexed by active row c)
+struct BdVec {
+  double *yk, *dk, *yext, *ysc, *dxc, *Q, *E;
+};
+
+__device__ __forceinline__ BdVec bd_bind(const Ws &W, int nsys) {
+  BdVec B;
+  B.yk = W.bd; B.dk = W.bd + nsys; B.yext = W.bd + 2 * nsys; B.ysc = W.bd + 3 * nsys; B.dxc = W.bd + 4 * nsys;
+  B.Q = W.bd + 6 * nsys;
+  B.E = W.bd + (6 + kMaxLevels + 1) * (size_t)nsys;
+  return B;
 }
 
-// extrapolate (bader_deuflhard.F90:371-407): Neville tableau, column k
-__device__ void dev_extrapolate(const DevNet &N, const Ws &W, ZoneCtl &C, int k, double xest) {
-  const int n = N.nsp, tid = threadIdx.x, nt = blockDim.x;
+// one semi-implicit midpoint sub-step, bader_deuflhard_step (bader_deuflhard.F90:410-488)
+__device__ int dev_bd_substep(const DevNet &N, const Ws &W, ZoneCtl &C, const BdVec &B, double h, int stage,
+                              bool huge_frozen) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  Act &A = C.act;
+  dev_dxdt_active(N, W, A, B.yk, B.dxc);
+  if (stage == 1) for (int c = tid; c < A.na; c += nt) A.xs[c] = h * B.dxc[c];
+  else for (int c = tid; c < A.na; c += nt) A.xs[c] = h * B.dxc[c] - B.dk[c];
+  __syncthreads();
+  if (!dev_solve_active(A)) return BAD_STEP;
+  C.st.nsolve++;
+  bool huge = false;
+  for (int c = tid; c < A.na; c += nt) {
+    const double d = stage == 2 ? B.dk[c] + 2.0 * A.xs[c] : A.xs[c];
+    B.dk[c] = d;
+    const double yk = B.yk[c] + d;
+    B.yk[c] = yk;
+    if (yk > 2.0) huge = true;
+  }
+  return (block_any(huge) || huge_frozen) ? HUGE_ABUNDS : 0;
+}
+
+// extrapolate (bader_deuflhard.F90:371-407): Neville tableau, column k, on the active rows
+__device__ void dev_extrapolate(ZoneCtl &C, const BdVec &B, int na, int k, double xest) {
   C.xhist[k] = xest;
-  double *Q = W.qcol, *E = W.yerr;
-  for (int j = tid; j < n; j += nt) {
-    double yest = W.y_k[j];
-    E[(size_t)k * n + j] = yest;
+  for (int j = threadIdx.x; j < na; j += blockDim.x) {
+    const double yest = B.yk[j];
     if (k == 1) {
-      Q[(size_t)k * n + j] = yest;
-      W.y_ext[j] = yest;
+      B.Q[(size_t)k * na + j] = yest;
+      B.E[(size_t)k * na + j] = yest;
+      B.yext[j] = yest;
       continue;
     }
     double yz = yest, d = yest, e = yest;
     for (int k1 = 1; k1 <= k - 1; ++k1) {
-      double delta = 1.0 / (C.xhist[k - k1] - xest);
-      double f1 = xest * delta, f2 = C.xhist[k - k1] * delta;
-      double q = Q[(size_t)k1 * n + j];
-      Q[(size_t)k1 * n + j] = e;
-      double dl = d - q;
+      const double delta = 1.0 / (C.xhist[k - k1] - xest);
+      const double f1 = xest * delta, f2 = C.xhist[k - k1] * delta;
+      const double q = B.Q[(size_t)k1 * na + j];
+      B.Q[(size_t)k1 * na + j] = e;
+      const double dl = d - q;
       e = f1 * dl;
       d = f2 * dl;
       yz = yz + e;
     }
-    E[(size_t)k * n + j] = e;
-    Q[(size_t)k * n + j] = e;
-    W.y_ext[j] = yz;
+    B.E[(size_t)k * na + j] = e;
+    B.Q[(size_t)k * na + j] = e;
+    B.yext[j] = yz;
   }
   __syncthreads();
 }
 
 __device__ int dev_bader_deuflhard(const DevNet &N, const Ws &W, ZoneCtl &C, double *yps, double dt, double &dtrcmd,
                                    bool frst, double *sred) {
-  const int nsp = N.nsp, tid = threadIdx.x, nt = blockDim.x;
+  const int tid = threadIdx.x, nt = blockDim.x;
   const double safe1 = 0.25, safe2 = 0.7, redmin = 0.7, redmax = 1.e-5, scalmx = 0.25;
+  const double thr = N.kn.grdthreshold;
   int km = -1, k;
   double scal = 1.0, red = -1.0, errmax = 0.0, abuerr = 0.0, negerr = 0.0;
-  dev_jacobian(N, W, dt, yps);
+  dev_new_jacobian(N, W, C, dt, yps);
+  Act &A = C.act;
+  const int na = A.na;
+  const BdVec B = bd_bind(W, N.nsys);
+  // frozen species: constant share of the mass sum, of the negative test and of the error mask
+  double sum_fz = 0.0, neg_fz = -DBL_MAX;
+  bool big_fz = false, huge_fz = false;
+  for (int s = tid; s < N.nsp; s += nt) {
+    if (W.mask[s]) continue;
+    const double y = yps[s];
+    sum_fz += y;
+    if (y < thr) neg_fz = fmax(neg_fz, -y);
+    if (y > 1e-27) big_fz = true;
+    if (y > 2.0) huge_fz = true;
+  }
+  sum_fz = block_sum(sum_fz, sred);
+  neg_fz = block_max(neg_fz, sred);
+  big_fz = block_any(big_fz);
+  huge_fz = block_any(huge_fz);
   for (k = 1; k <= N.kmax; ++k) {
-    vcopy(W.y_k, yps, nsp);
+    for (int c = tid; c < na; c += nt) B.yk[c] = yps[N.sp_of_sys[A.arow[c]]];
+    __syncthreads();
     // semi_implicit_extrapolation (bader_deuflhard.F90:276-316)
-    double h = dt / (double)N.nseq[k];
-    double xest = powi(h / N.nseq[k], 2);
-    dev_assemble_factor(N, W, h);
+    const double h = dt / (double)N.nseq[k];
+    const double xest = powi(h / N.nseq[k], 2);
+    if (!dev_factor_active(N, W, A, h)) {
+      dtrcmd = dt * 0.2;
+      return BAD_STEP;
+    }
     C.st.nfact++;
-    int ierr = dev_bd_substep(N, W, C, h, 1, sred);
-    for (int i = 1; ierr == 0 && i <= N.nseq[k] - 1; ++i) ierr = dev_bd_substep(N, W, C, h, 2, sred);
-    if (ierr == 0) ierr = dev_bd_substep(N, W, C, h, 3, sred);
+    int ierr = dev_bd_substep(N, W, C, B, h, 1, huge_fz);
+    for (int i = 1; ierr == 0 && i <= N.nseq[k] - 1; ++i) ierr = dev_bd_substep(N, W, C, B, h, 2, huge_fz);
+    if (ierr == 0) ierr = dev_bd_substep(N, W, C, B, h, 3, huge_fz);
     if (ierr != 0) {
       dtrcmd = dt * 0.2;
-      vcopy(yps, W.y_k, nsp);
       return ierr;
     }
     C.st.newton_iters += N.nseq[k];
-    dev_extrapolate(N, W, C, k, xest);
+    dev_extrapolate(C, B, na, k, xest);
     bool nan = false;
-    for (int i = tid; i < nsp; i += nt) {
-      double y = W.y_ext[i];
-      W.y_k[i] = y;
+    for (int c = tid; c < na; c += nt) {
+      const double y = B.yext[c];
+      B.yk[c] = y;
       if (y != y) nan = true;
-      W.yscal[i] = fmax(fabs(y), N.kn.grdthreshold);
+      B.ysc[c] = fmax(fabs(y), thr);
     }
     if (block_any(nan)) {
       dtrcmd = dt * 0.2;
-      vcopy(yps, W.y_k, nsp);
       return GOT_NAN;
     }
     if (k != 1) {
       // compute_error (bader_deuflhard.F90:325-366)
-      double am = -DBL_MAX, nm = -DBL_MAX;
-      for (int i = tid; i < nsp; i += nt) {
-        double y = W.y_k[i];
-        if (y > 1e-27) am = fmax(am, fabs(W.yerr[(size_t)k * nsp + i] / W.yscal[i]));
-        if (y < N.kn.grdthreshold) nm = fmax(nm, -y);
+      double am = big_fz ? 0.0 : -DBL_MAX, nm = -DBL_MAX, sy = 0.0;
+      for (int c = tid; c < na; c += nt) {
+        const double y = B.yk[c];
+        if (y > 1e-27) am = fmax(am, fabs(B.E[(size_t)k * na + c] / B.ysc[c]));
+        if (y < thr) nm = fmax(nm, -y);
+        sy += y;
       }
       abuerr = block_max(am, sred) / N.kn.dgrd;
-      negerr = block_max(nm, sred) / N.kn.grdthreshold;
+      negerr = fmax(block_max(nm, sred), neg_fz) / thr;
+      sy = block_sum(sy, sred);
       if (abuerr < 1e-3) {
         errmax = abuerr;
       } else {
-        C.sumerr = fabs(1.0 - vsum(W.y_k, nsp, sred)) / K_SUM_TOL;
+        C.sumerr = fabs(1.0 - (sy + sum_fz)) / K_SUM_TOL;
         errmax = fmax(abuerr, C.sumerr);
       }
       errmax = fmax(errmax, negerr);
@@ -253,7 +316,8 @@ __device__ int dev_bader_deuflhard(const DevNet &N, const Ws &W, ZoneCtl &C, dou
       }
     }
   }
-  vcopy(yps, W.y_k, nsp);
+  for (int c = tid; c < na; c += nt) yps[N.sp_of_sys[A.arow[c]]] = B.yk[c];  // yps(:) = y_k(:)
+  __syncthreads();
   return ierr;
 }
 

@@ -454,6 +454,9 @@ std::string build_host_net(const nuppn_net_desc &d, const nuppn_knobs &kn, HostN
     auto it = std::lower_bound(b, en, c);
     H.pos_of_entry[e] = (int)(it - H.lu_col.begin());
   }
+  H.lu_src.assign(H.nnzLU, -1);
+  for (int e = 0; e < H.nnzJ; ++e)
+    if (H.pos_of_entry[e] >= 0) H.lu_src[H.pos_of_entry[e]] = e;
   bd_constants(H);
   return "";
 }

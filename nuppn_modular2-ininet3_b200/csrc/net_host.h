@@ -49,7 +49,7 @@ struct HostNet {
   std::vector<int> jg_ptr, jg_item, dg_ptr, dg_item, jg_long, dg_long;
   std::vector<double> dg_coef;
   // system / LU
-  std::vector<int> sys_of_sp, sp_of_sys, pos_of_entry;
+  std::vector<int> sys_of_sp, sp_of_sys, pos_of_entry, lu_src;
   std::vector<int> lu_rowptr, lu_diag, lu_col, upd_start;
   std::vector<uint16_t> upd_off;
   std::vector<int> lvL_ptr, lvL_rows, lvL_grp, lvU_ptr, lvU_rows, lvU_grp;

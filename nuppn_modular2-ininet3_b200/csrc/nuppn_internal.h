@@ -70,6 +70,7 @@ struct DevNet {
   // system and LU
   const int *sys_of_sp, *sp_of_sys;        // [nsp], [nsys]
   const int *pos_of_entry;                 // [nnzJ] LU position or -1
+  const int *lu_src;                       // [nnzLU] Jacobian entry of an LU position or -1 (fill)
   const int *lu_rowptr, *lu_diag, *lu_col; // [nsys+1], [nsys], [nnzLU]
   const int *upd_start;                    // [nnzLU+1] for L entries: start in upd_off
   const uint16_t *upd_off;                 // offsets into the target row
@@ -90,8 +91,25 @@ struct DevNet {
 struct WsLayout {
   size_t v, rv, ngv, ffv, kdv, partinter, G, flux, contrib, first_l, eset, jac, mask, xn, dxdt;
   size_t y, y_old, y_cur, y_new, y_k, delta_k, y_ext, yscal, qcol, yerr, lu, bsys, xsys, rhs;
+  size_t act_tmp, act;           // compaction scratch (ints) and the global fallback of the active LU
+  size_t act_rtmp, act_r;        // reaction keep-map scratch and the restricted right-hand side
+  size_t act_itmp, act_otmp, act_dtmp, act_btmp, bd;  // flattened-gather scratch, compact BD vectors
   size_t bytes;
 };
+
+// Bytes of the active-subsystem LU for na rows, nnz entries and nwarps warps (see active_lu.cuh):
+// int crp[na+1], cdiag[na], arow[na], flagF[na], flagS[na], ccol[nnz], csrc[nnz];
+// double cval[nnz], xs[na], wbuf[nwarps*na]; every array 16-byte aligned.
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+inline size_t act_bytes(int na, int nnz, int nwarps) {
+  auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };
+  size_t b = 0;
+  b += a16((size_t)(na + 1) * 4) + 4 * a16((size_t)na * 4) + 2 * a16((size_t)nnz * 4);
+  b += a16((size_t)nnz * 8) + a16((size_t)na * 8) + a16((size_t)nwarps * na * 8);
+  return b;
+}
 
 // arguments of the persistent integration kernel
 struct IntegrateArgs {

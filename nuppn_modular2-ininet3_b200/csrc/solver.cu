@@ -515,110 +515,50 @@ __device__ void dev_jacobian(const DevNet &N, const Ws &W, double dzeit, const d
   __syncthreads();
 }
 
-// ---------------------------------------------------------------------------------------------
-// I - h J on the filled pattern (reduce_jacobian semantics, jac_rhs.F90:134-197), then the numeric
-// factorization with static diagonal pivots, up-looking by rows in level order.
-__device__ void dev_assemble_factor(const DevNet &N, const Ws &W, double h) {
-  const int tid = threadIdx.x, nt = blockDim.x;
-  for (int p = tid; p < N.nnzLU; p += nt) W.lu[p] = 0.0;
-  __syncthreads();
-  for (int e = tid; e < N.nnzJ; e += nt) {
-    int pos = N.pos_of_entry[e];
-    if (pos < 0) continue;
-    double val = W.jac[e] * (-h);
-    bool set = W.eset[e] != 0;
-    if (set && (fabs(val) == 0.0 || val == -1.0)) { set = false; W.eset[e] = 0; }
-    int r = N.jrow[e];
-    if (N.jdiag[r] == e) {
-      if (W.mask[r]) { set = true; W.eset[e] = 1; val = val + 1.0; }
-      else { set = true; val = 1.0; }
-    }
-    if (set) W.lu[pos] = val;
-  }
-  __syncthreads();
-  const int lane = tid & 31, w = tid >> 5, nw = nt >> 5;
-  for (int lv = 0; lv < N.nlvL; ++lv) {
-    for (int q = N.lvL_ptr[lv] + w; q < N.lvL_ptr[lv + 1]; q += nw) {
-      int i = N.lvL_rows[q];
-      if (!W.mask[N.sp_of_sys[i]]) continue;  // identity row of a species outside the dynamic network
-      int rs = N.lu_rowptr[i], dg = N.lu_diag[i];
-      for (int p = rs; p < dg; ++p) {
-        double a = W.lu[p];
-        __syncwarp();
-        if (a == 0.0) continue;
-        int j = N.lu_col[p];
-        double l = a / W.lu[N.lu_diag[j]];
-        if (lane == 0) W.lu[p] = l;
-        int us = N.lu_diag[j] + 1, ue = N.lu_rowptr[j + 1], os = N.upd_start[p];
-        for (int qq = us + lane; qq < ue; qq += 32) W.lu[rs + N.upd_off[os + qq - us]] -= l * W.lu[qq];
-        __syncwarp();
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// Solve (I - hJ) x = rhs restricted to the mask: rhs and x species-indexed; x = 0 off the mask.
-__device__ void dev_solve(const DevNet &N, const Ws &W, const double *rhs, double *x) {
-  const int tid = threadIdx.x, nt = blockDim.x;
-  for (int i = tid; i < N.nsys; i += nt) {
-    int s = N.sp_of_sys[i];
-    W.bsys[i] = W.mask[s] ? rhs[s] : 0.0;
-  }
-  __syncthreads();
-  // Rows of a level are spread over groups of G lanes; the loop bound is uniform per warp so the
-  // group shuffles always run with the whole warp.
-  for (int lv = 0; lv < N.nlvL; ++lv) {
-    const int G = N.lvL_grp[lv], grp = tid / G, gl = tid % G, ng = nt / G;
-    const int q0 = N.lvL_ptr[lv], q1 = N.lvL_ptr[lv + 1];
-    for (int base = q0; base < q1; base += ng) {
-      int q = base + grp;
-      double s = 0.0;
-      int i = -1;
-      if (q < q1) {
-        i = N.lvL_rows[q];
-        for (int p = N.lu_rowptr[i] + gl; p < N.lu_diag[i]; p += G) s += W.lu[p] * W.bsys[N.lu_col[p]];
-      }
-      for (int o = G >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(NUPPN_FULL, s, o, G);
-      if (i >= 0 && gl == 0) W.bsys[i] = W.bsys[i] - s;
-    }
-    __syncthreads();
-  }
-  for (int lv = 0; lv < N.nlvU; ++lv) {
-    const int G = N.lvU_grp[lv], grp = tid / G, gl = tid % G, ng = nt / G;
-    const int q0 = N.lvU_ptr[lv], q1 = N.lvU_ptr[lv + 1];
-    for (int base = q0; base < q1; base += ng) {
-      int q = base + grp;
-      double s = 0.0;
-      int i = -1;
-      if (q < q1) {
-        i = N.lvU_rows[q];
-        for (int p = N.lu_diag[i] + 1 + gl; p < N.lu_rowptr[i + 1]; p += G) s += W.lu[p] * W.bsys[N.lu_col[p]];
-      }
-      for (int o = G >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(NUPPN_FULL, s, o, G);
-      if (i >= 0 && gl == 0) W.bsys[i] = (W.bsys[i] - s) / W.lu[N.lu_diag[i]];
-    }
-    __syncthreads();
-  }
+// First pass of calculate_jacobian for the integrator: only the dynamic-network mask (first_l, mask)
+// and each reaction's rate test (flux[a] = 1 if |v|/dt > min_rate_ov_dt). The values and entry flags
+// are then built for the active subsystem only (dev_jacobian_active, active_lu.cuh).
+__device__ void dev_jacobian_mask(const DevNet &N, const Ws &W, double dzeit, const double *x) {
+  const int tid = threadIdx.x, nt = blockDim.x, g = N.ig;
+  const double dfdNmin = N.kn.cyminformal / dzeit;
   for (int s = tid; s < N.nsp; s += nt) {
-    int i = N.sys_of_sp[s];
-    x[s] = (i >= 0 && W.mask[s]) ? W.bsys[i] : 0.0;
+    W.xn[s] = s == g ? 1.0 : ((N.ciso[s] && N.an[s] > 0.0) ? x[s] / N.an[s] : 0.0);
+    W.first_l[s] = 0x7fffffff;
   }
   __syncthreads();
+  for (int a = tid; a < N.nact; a += nt) {
+    const int *k = N.act_k + (size_t)a * 8;
+    const double v = W.v[N.act_slot[a]];
+    if (!(fabs(v) / dzeit > N.kn.min_rate_ov_dt)) {
+      W.flux[a] = 0.0;
+      continue;
+    }
+    W.flux[a] = 1.0;
+    const double dfdN = c_fact[k[1]] * c_fact[k[3]] * v * powi(W.xn[k[0]], k[1]) * W.xn[k[2]];
+    if (fabs(dfdN) > dfdNmin) {
+      atomicMin(&W.first_l[k[0]], a); atomicMin(&W.first_l[k[2]], a);
+      atomicMin(&W.first_l[k[4]], a); atomicMin(&W.first_l[k[6]], a);
+    }
+  }
+  __syncthreads();
+  for (int s = tid; s < N.nsp; s += nt) W.mask[s] = (W.first_l[s] != 0x7fffffff && s != g) ? 1 : 0;
+  __syncthreads();
 }
-
 }  // namespace nuppn
 
+#include "active_lu.cuh"
 #include "integrator.cuh"
 
 namespace nuppn {
 
 // ---------------------------------------------------------------------------------------------
-// kernels: persistent CTAs, one zone at a time, workspace slab per CTA
-
+// kernels: persistent CTAs, one zone at a time, workspace slab per CTA; dynamic shared memory holds
+// the active-subsystem LU when it fits (act_smem bytes).
 __global__ void __launch_bounds__(256) k_integrate(const __grid_constant__ DevNet N, const __grid_constant__ WsLayout L,
-                                                   char *ws, const __grid_constant__ IntegrateArgs A) {
+                                                   char *ws, const __grid_constant__ IntegrateArgs A, int act_smem) {
+  extern __shared__ __align__(16) char smem_dyn[];
   __shared__ double sred[32];
+  __shared__ int sint[32];
   __shared__ int zsh;
   const Ws W = ws_bind(ws + (size_t)blockIdx.x * L.bytes, L);
   for (;;) {
@@ -635,6 +575,9 @@ __global__ void __launch_bounds__(256) k_integrate(const __grid_constant__ DevNe
     C.kopt = (st >= 2 && st <= N.kmax) ? st : N.kopt0;
     C.reduce = false;
     C.sumerr = 0.0;
+    C.smem = smem_dyn;
+    C.smem_bytes = act_smem;
+    C.sint = sint;
     double ye = A.ye[z];
     int ierr = dev_integrate_zone(N, W, C, A.t9_0[z], A.t9_1[z], A.rho_0[z], A.rho_1[z], ye, A.dtwant[z], st <= 0, sred);
     for (int s = threadIdx.x; s < N.nsp; s += blockDim.x) A.X[(size_t)z * A.ldx + s] = W.y[s];
@@ -647,10 +590,11 @@ __global__ void __launch_bounds__(256) k_integrate(const __grid_constant__ DevNe
   }
 }
 
-
 __global__ void __launch_bounds__(256) k_phase(const __grid_constant__ DevNet N, const __grid_constant__ WsLayout L,
-                                               char *ws, const __grid_constant__ PhaseArgs A) {
+                                               char *ws, const __grid_constant__ PhaseArgs A, int act_smem) {
+  extern __shared__ __align__(16) char smem_dyn[];
   __shared__ double sred[32];
+  __shared__ int sint[32];
   const Ws W = ws_bind(ws + (size_t)blockIdx.x * L.bytes, L);
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int z = blockIdx.x; z < A.nz; z += gridDim.x) {
@@ -682,28 +626,36 @@ __global__ void __launch_bounds__(256) k_phase(const __grid_constant__ DevNet N,
         W.rhs[s] = A.b[(size_t)z * N.nsp + s];
       }
       __syncthreads();
-      dev_assemble_factor(N, W, A.dt[z]);
-      dev_solve(N, W, W.rhs, W.dxdt);
-      for (int s = tid; s < N.nsp; s += nt) A.out_x[(size_t)z * N.nsp + s] = W.dxdt[s];
+      Act act;
+      dev_compact(N, W, act, smem_dyn, act_smem, sint);
+      bool ok = dev_factor_active(N, W, act, A.dt[z]);
+      ok = dev_solve_species(N, act, W.rhs, W.dxdt) && ok;
+      for (int s = tid; s < N.nsp; s += nt) A.out_x[(size_t)z * N.nsp + s] = ok ? W.dxdt[s] : NAN;
     }
     __syncthreads();
   }
 }
 
-cudaError_t launch_integrate(const DevNet &N, const WsLayout &L, char *ws, int grid, int block,
+cudaError_t launch_integrate(const DevNet &N, const WsLayout &L, char *ws, int grid, int block, int act_smem,
                              const IntegrateArgs &A, cudaStream_t st) {
-  k_integrate<<<grid, block, 0, st>>>(N, L, ws, A);
+  k_integrate<<<grid, block, act_smem, st>>>(N, L, ws, A, act_smem);
   return cudaGetLastError();
 }
 
-cudaError_t launch_phase(const DevNet &N, const WsLayout &L, char *ws, int grid, int block, const PhaseArgs &A,
-                         cudaStream_t st) {
-  k_phase<<<grid, block, 0, st>>>(N, L, ws, A);
+cudaError_t launch_phase(const DevNet &N, const WsLayout &L, char *ws, int grid, int block, int act_smem,
+                         const PhaseArgs &A, cudaStream_t st) {
+  k_phase<<<grid, block, act_smem, st>>>(N, L, ws, A, act_smem);
   return cudaGetLastError();
 }
 
-cudaError_t occupancy_integrate(int block, int *per_sm) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_integrate, block, 0);
+cudaError_t configure_kernels(int act_smem) {
+  cudaError_t e = cudaFuncSetAttribute(k_integrate, cudaFuncAttributeMaxDynamicSharedMemorySize, act_smem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_phase, cudaFuncAttributeMaxDynamicSharedMemorySize, act_smem);
+}
+
+cudaError_t occupancy_integrate(int block, int act_smem, int *per_sm) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_integrate, block, act_smem);
 }
 
 }  // namespace nuppn

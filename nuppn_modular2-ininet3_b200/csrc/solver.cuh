@@ -25,6 +25,15 @@ struct Ws {
   double *y, *y_old, *y_cur, *y_new, *y_k, *delta_k, *y_ext, *yscal, *qcol, *yerr, *lu, *bsys, *xsys, *rhs;
   int *first_l;
   uint8_t *eset, *mask;
+  int *act_tmp;  // compaction scratch: sys2c, arow, counts
+  char *act;     // global fallback of the active-subsystem LU
+  int *act_rtmp; // reaction keep-map scratch [nact]
+  char *act_r;   // global fallback of the restricted right-hand side
+  int *act_itmp; // flattened-list flags / positions [max(list items) + 1]
+  int *act_otmp; // segment offsets of the active Jacobian entries [nnzLU + 1]
+  double *act_dtmp;   // flattened Jacobian contributions [jg items]
+  uint8_t *act_btmp;  // flattened entry-set flags [jg items]
+  double *bd;         // compact Bader-Deuflhard vectors [(2*kMaxLevels + 8) * nsys]
 };
 
 __device__ __forceinline__ Ws ws_bind(char *base, const WsLayout &L) {
@@ -41,6 +50,15 @@ __device__ __forceinline__ Ws ws_bind(char *base, const WsLayout &L) {
   w.yscal = (double *)(base + L.yscal); w.qcol = (double *)(base + L.qcol); w.yerr = (double *)(base + L.yerr);
   w.lu = (double *)(base + L.lu); w.bsys = (double *)(base + L.bsys); w.xsys = (double *)(base + L.xsys);
   w.rhs = (double *)(base + L.rhs);
+  w.act_tmp = (int *)(base + L.act_tmp);
+  w.act = base + L.act;
+  w.act_rtmp = (int *)(base + L.act_rtmp);
+  w.act_r = base + L.act_r;
+  w.act_itmp = (int *)(base + L.act_itmp);
+  w.act_otmp = (int *)(base + L.act_otmp);
+  w.act_dtmp = (double *)(base + L.act_dtmp);
+  w.act_btmp = (uint8_t *)(base + L.act_btmp);
+  w.bd = (double *)(base + L.bd);
   return w;
 }
 
