@@ -6,7 +6,7 @@ Fe56=1e-3 (renormalised) x lognormal(0.05) per species, one integrate_network ca
 with adaptive Bader-Deuflhard steps, FP64. A "step" is one call over the whole batch, restarted from
 the same initial state. The metric counts accepted sub-steps (zone-timesteps) per second.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--nz Z] [--lu fp64|mixed]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--nz Z]
 
 --impl reference times the reference's own algorithm on the host cores (the CPU restatement of
 NuPPN's FP64 path, calling the reference's SuperLU) on a bounded sample of the same workload.
@@ -86,6 +86,18 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def measured_traffic_per_zone():
+    """DRAM bytes per zone of k_integrate from the committed ncu summary (None if absent)."""
+    p = os.path.join(ROOT, "profiles", "k_integrate_heshell1107_256_memory.md")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_zone"):
+                return int(line.split("=")[1])
+    except OSError:
+        pass
+    return None
+
+
 def algorithmic_bytes(info, stats_np, nre_active, nsp):
     """Bytes a zone-step must move at minimum (per-zone arrays, each read/written once per use):
     8 * [ rates (R+3) + per Jacobian nnzJ + per factorization (nnzJ + nnzLU)
@@ -140,7 +152,6 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nz", type=int, default=1024)
-    ap.add_argument("--lu", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--ref-zones", type=int, default=32)
     ap.add_argument("--cpu-zones", type=int, default=16)
     ap.add_argument("--no-cpu", action="store_true")
@@ -166,7 +177,7 @@ def main():
     net = wl.network(1107)
     zb_all = wl.heshell_batch(args.nz * world, net=net, seed=2)
     zb = zb_all.take(np.arange(rank * args.nz, (rank + 1) * args.nz))  # weak scaling: shard of zones
-    knobs = abi.default_knobs(integration_method=1, lu_precision=1 if args.lu == "mixed" else 0)
+    knobs = abi.default_knobs(integration_method=1)
     S = solver.NetworkSolver(net, knobs, device=dev_id)
     nz = zb.nz
 
@@ -178,9 +189,11 @@ def main():
     stats = torch.zeros((nz, 8), dtype=torch.int32, device="cuda")
     bd = torch.zeros(nz, dtype=torch.int32, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # 2x the 126 MB L2
 
     def one_step():
         X.copy_(X0); ye.copy_(ye0); bd.zero_()
+        flush.fill_(1)  # evict the previous call's lines from L2 before the timed region
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         S.integrate_device(X, t9a, t9b, rha, rhb, ye, dtw, ierr, stats, bd, stream=stream)
@@ -242,24 +255,32 @@ def main():
         bytes_per_launch = algorithmic_bytes(S.info, st_np, nre_active, net.nsp)
         per_launch_s = (sum(kernel_ms) / len(kernel_ms)) * 1e-3
         achieved = bytes_per_launch / per_launch_s / 1e9
+        tpz = measured_traffic_per_zone()
+        traffic = tpz * nz if tpz else None
         line = {
             "metric": "zone-timesteps/s", "value": value, "unit": "zone-timesteps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.lu == "fp64" else "f64+f32-lu", "data": "synthetic",
+            "dtype": "f64", "data": "synthetic",
             "config": {"workload": "heshell-1107 BD 1e10 s", "zones": nz * world, "zones_per_gpu": nz,
                        "network_species": net.nsp, "nnz_jac": S.info.nnz_jac, "nnz_lu": S.info.nnz_lu,
-                       "integrator": "bader-deuflhard", "lu": args.lu,
-                       "l2": "per-zone workspace (>1 GB) exceeds L2; no flush needed",
+                       "integrator": "bader-deuflhard", "lu": "fp64",
+                       "l2": "flushed: 256 MiB written before each timed call",
                        "accepted_steps_per_call": int(st_np[:, 0].sum()),
                        "rejected_steps_per_call": int(st_np[:, 1].sum())},
             "gpu_launches": int(gpu_launches),
             "e2e": {"value": e2e, "unit": "zone-timesteps/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind, "kernel": "k_integrate",
-                         "algorithmic_bytes_per_launch": bytes_per_launch},
+                         "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "dram_achieved_gbs": (traffic / per_launch_s / 1e9) if traffic else None,
+                         "traffic_source": "ncu dram__bytes_read+write per zone at 256 zones, x zones",
+                         "note": "algorithmic bytes count the full-network sweeps (R + 3N + nnzLU per "
+                                 "substep) of the reference formulation; the kernel keeps each zone's "
+                                 "active subsystem on chip, so traffic is far below them and the "
+                                 "kernel is latency-bound"},
             "clocks": clk.summary(),
         }
         if not args.no_cpu:

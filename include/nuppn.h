@@ -96,7 +96,9 @@ typedef struct nuppn_knobs {
   int32_t threads_per_zone;    /* CTA size (0 = library choice)                               */
   int32_t lu_onewarp_max;      /* active systems up to this size are factored/solved by one warp
                                   (0 = library default; larger ones use sync-free multi-warp)    */
-  int32_t reserved[6];
+  int32_t lu_tile_max;         /* active systems up to this size (at most 64) are factored in a
+                                  dense tile and solved in registers (0 = 64, negative = never)  */
+  int32_t reserved[5];
 } nuppn_knobs;
 
 /* Network description in the reference's slot layout (what rnetw2007, reaclib_init, netgen_init,

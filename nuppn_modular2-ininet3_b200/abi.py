@@ -36,7 +36,8 @@ class Knobs(C.Structure):
                 ("delta_state_max", C.c_double), ("nse_min_t9", C.c_double),
                 ("lu_precision", C.c_int32), ("ir_max_iters", C.c_int32),
                 ("ir_rtol", C.c_double), ("threads_per_zone", C.c_int32),
-                ("lu_onewarp_max", C.c_int32), ("reserved", C.c_int32 * 6)]
+                ("lu_onewarp_max", C.c_int32), ("lu_tile_max", C.c_int32),
+                ("reserved", C.c_int32 * 5)]
 
 
 def default_knobs(**over) -> Knobs:

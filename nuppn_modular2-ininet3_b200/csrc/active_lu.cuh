@@ -3,53 +3,56 @@
 // The reference solves only the species its dynamic network selects (jac_rhs.F90:134-197: mask,
 // pack, then SuperLU on the reduced matrix, with a new COLAMD/symbolic analysis every time). Here the
 // fill-reducing order and the filled pattern are computed once for the whole network (net_host.cpp);
-// the filled pattern restricted to the active rows and columns is closed under fill in that order,
-// so each zone only has to compact it (once per Jacobian) and can then factor and solve it with no
-// symbolic work. Compacted structures live in shared memory when they fit the CTA's budget and in
-// the CTA's global workspace otherwise.
+// the filled pattern restricted to the active rows and columns contains the fill of the active
+// submatrix in that order, so each zone only has to compact it (once per Jacobian) and can then
+// factor and solve it with no symbolic work. Compacted structures live in shared memory when they
+// fit the CTA's budget and in the CTA's global workspace otherwise.
 //
 // Per Jacobian (dev_jacobian_mask, then):
 //   dev_compact          active rows and the restricted filled pattern
 //   dev_jacobian_active  Jacobian values and entry flags of the active entries (all reactions)
-//   dev_compact_rhs      the reactions a step needs and the per-species gather lists
+//   dev_compact_rhs      per-species gather items of the right-hand side
 // Per factorization / right-hand side / solve: dev_factor_active, dev_dxdt_active, dev_solve_active,
-// all on compact vectors indexed by the active row number c.
+// all on compact vectors indexed by the active row number c. Systems of up to kTileMax rows (the
+// usual case: a few tens of species) are factored as a dense tile and solved with rows held in the
+// registers of one warp; larger ones use the sparse row-oriented factorization.
 #pragma once
 
 namespace nuppn {
 
 constexpr int kSpinLimit = 1 << 22;  // per wait; a timeout marks the zone as failed, never hangs
 
-// Active subsystems up to this size are factored and solved by one warp, row after row, with no
-// inter-warp flags: for the few tens of species a dynamic network usually keeps, the dependency
-// chain is the whole cost and a single warp walks it fastest.
+// Sparse active subsystems up to this size are factored and solved by one warp, row after row,
+// with no inter-warp flags; larger ones by all warps with per-row ready flags.
 constexpr int kOneWarpMax = 192;
+
+// Flags of a compact LU position (jflag): entry set, diagonal, fill (no Jacobian entry).
+enum : uint8_t { JF_SET = 1, JF_DIAG = 2, JF_FILL = 4 };
 
 struct Act {
   int na, nnz;
   int *crp, *cdiag, *arow, *flagF, *flagS, *ccol, *csrc;
-  bool onewarp;  // factor/solve by one warp (small systems)
-  double *cval, *xs, *wbuf;
+  bool onewarp;      // sparse factor/solve by one warp (small systems)
+  bool tile;         // tile_rows > 0
+  int tile_rows;     // 0, 32 or 64: dense tile factorization, register-resident solve
+  double *cval, *xs, *wbuf;  // sparse path only: L\U values in CSR order, multi-warp scratch
+  double *jval;      // [nnz] Jacobian value of each position (the reference's 1e-99 + contributions)
+  uint8_t *jflag;    // [nnz] JF_* flags; JF_SET is cleared when a level drops the entry
+  double *anc;       // [na] mass number of active row c
+  double *xnc;       // [na+1] molar abundances of the active rows; xnc[na] = 1 (gamma)
+  double *T, *rinv;  // tile: T[c*tile_rows + r] = entry (r, c) of L\U; rinv[r] = 1 / U(r, r)
   int genF, genS;
   bool in_smem;
   // right-hand side restricted to the dynamic network (see dev_compact_rhs)
-  int nar, ngi;
-  int *ar, *gptr, *gitem;
-  float *gcoef;
-  double *flux;
+  int ngi;
+  int *gptr;         // [na+1] gather items of active row c: gptr[c] .. gptr[c+1]-1
+  float *gcoef;      // [ngi] term coefficient (-k2, -1, k6 or k8)
+  uint32_t *grpk;    // [ngi] compact index of reactant 1 | reactant 2 (na = gamma) << 14 | k2 << 28
+  double *grcv;      // [ngi] (1/k2!) * rate of the term's reaction
   bool rhs_in_smem;
 };
 
-// Bytes of the restricted right-hand side: int ar[nar], gptr[na+1], gitem[ngi]; float gcoef[ngi];
-// double flux[nar]; 16-byte aligned arrays.
-__host__ __device__ inline size_t rhs_bytes(int na, int nar, int ngi) {
-  auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };
-  return a16((size_t)nar * 4) + a16((size_t)(na + 1) * 4) + a16((size_t)ngi * 4) + a16((size_t)ngi * 4) +
-         a16((size_t)nar * 8);
-}
-
-__device__ __forceinline__ void act_bind(Act &A, char *base, int na, int nnz, int nwarps) {
-  auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };
+__device__ __forceinline__ void act_bind(Act &A, char *base, int na, int nnz, int nwarps, int tile_rows) {
   char *p = base;
   A.crp = (int *)p; p += a16((size_t)(na + 1) * 4);
   A.cdiag = (int *)p; p += a16((size_t)na * 4);
@@ -58,35 +61,55 @@ __device__ __forceinline__ void act_bind(Act &A, char *base, int na, int nnz, in
   A.flagS = (int *)p; p += a16((size_t)na * 4);
   A.ccol = (int *)p; p += a16((size_t)nnz * 4);
   A.csrc = (int *)p; p += a16((size_t)nnz * 4);
-  A.cval = (double *)p; p += a16((size_t)nnz * 8);
+  if (tile_rows == 0) {
+    A.cval = (double *)p; p += a16((size_t)nnz * 8);
+    A.wbuf = (double *)p; p += a16((size_t)nwarps * na * 8);
+  } else {
+    A.cval = nullptr;
+    A.wbuf = nullptr;
+  }
   A.xs = (double *)p; p += a16((size_t)na * 8);
-  A.wbuf = (double *)p;
+  A.jval = (double *)p; p += a16((size_t)nnz * 8);
+  A.anc = (double *)p; p += a16((size_t)na * 8);
+  A.xnc = (double *)p; p += a16((size_t)(na + 1) * 8);
+  A.jflag = (uint8_t *)p; p += a16((size_t)nnz);
+  A.tile_rows = tile_rows;
+  A.tile = tile_rows > 0;
+  if (A.tile) {
+    A.T = (double *)p; p += (size_t)na * tile_rows * 8;
+    A.rinv = (double *)p;
+  } else {
+    A.T = nullptr;
+    A.rinv = nullptr;
+  }
 }
 
-// Exclusive scan of v[0..n) in place (block-wide, deterministic); returns the total.
+// Exclusive scan of v[0..n) in place (block-wide, deterministic); returns the total. Each warp takes
+// a contiguous segment and walks it 32 elements at a time, so every load and store is coalesced.
 __device__ int block_scan_excl(int *v, int n, int *sint) {
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
-  const int ch = (n + nt - 1) / nt, b0 = min(n, tid * ch), b1 = min(n, b0 + ch);
-  int s = 0;
-  for (int i = b0; i < b1; ++i) s += v[i];
-  int incl = s;
-  for (int o = 1; o < 32; o <<= 1) {
-    int t = __shfl_up_sync(NUPPN_FULL, incl, o);
-    if (lane >= o) incl += t;
-  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int seg = (n + nw - 1) / nw, b0 = min(n, w * seg), b1 = min(n, b0 + seg);
+  int tot = 0;
+  for (int i = b0 + lane; i < b1; i += 32) tot += v[i];
+  for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(NUPPN_FULL, tot, o);
+  __syncthreads();  // sint may still be read by the previous scan
+  if (lane == 0) sint[w] = tot;
   __syncthreads();
-  if (lane == 31) sint[w] = incl;
-  __syncthreads();
-  int wbase = 0, total = 0;
+  int base = 0, total = 0;
   for (int i = 0; i < nw; ++i) {
-    if (i < w) wbase += sint[i];
+    if (i < w) base += sint[i];
     total += sint[i];
   }
-  int run = wbase + incl - s;
-  for (int i = b0; i < b1; ++i) {
-    int x = v[i];
-    v[i] = run;
-    run += x;
+  for (int i0 = b0; i0 < b1; i0 += 32) {
+    const int i = i0 + lane;
+    const int x = i < b1 ? v[i] : 0;
+    int incl = x;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(NUPPN_FULL, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (i < b1) v[i] = base + incl - x;
+    base += __shfl_sync(NUPPN_FULL, incl, 31);
   }
   __syncthreads();
   return total;
@@ -135,11 +158,12 @@ __device__ void dev_compact(const DevNet &N, const Ws &W, Act &A, char *smem, si
   }
   __syncthreads();
   const int nnz = block_scan_excl(cnt, na, sint);
-  const size_t need = act_bytes(na, nnz, nw);
+  const int trows = tile_rows_for(na, N.kn.lu_tile_max);
+  const size_t need = act_bytes(na, nnz, nw, trows);
   A.na = na;
   A.nnz = nnz;
   A.in_smem = need <= smem_bytes;
-  act_bind(A, A.in_smem ? smem : W.act, na, nnz, nw);
+  act_bind(A, A.in_smem ? smem : W.act, na, nnz, nw, trows);
   A.genF = 0;
   A.genS = 0;
   for (int c = tid; c < na; c += nt) {
@@ -147,8 +171,12 @@ __device__ void dev_compact(const DevNet &N, const Ws &W, Act &A, char *smem, si
     A.arow[c] = tmp_arow[c];
     A.flagF[c] = 0;
     A.flagS[c] = 0;
+    A.anc[c] = N.an[N.sp_of_sys[tmp_arow[c]]];
   }
-  if (tid == 0) A.crp[na] = nnz;
+  if (tid == 0) {
+    A.crp[na] = nnz;
+    A.xnc[na] = 1.0;  // gamma's molar abundance
+  }
   for (int c = w; c < na; c += nw) {
     int i = tmp_arow[c], base = cnt[c];
     for (int p0 = N.lu_rowptr[i]; p0 < N.lu_rowptr[i + 1]; p0 += 32) {
@@ -205,9 +233,9 @@ __device__ __forceinline__ double jac_contrib(const DevNet &N, const Ws &W, int 
 }
 
 // Jacobian values (1e-99 + the reaction contributions, every reaction as in the reference) and entry
-// flags for the entries of the active subsystem. The contributions of all active entries are
+// flags for the positions of the active subsystem. The contributions of all active entries are
 // evaluated as one flattened, block-parallel list; each entry is then summed by a warp.
-__device__ void dev_jacobian_active(const DevNet &N, const Ws &W, const Act &A, int *sint) {
+__device__ void dev_jacobian_active(const DevNet &N, const Ws &W, Act &A, int *sint) {
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
   int *off = W.act_otmp;  // [nnz+1] <= nnzLU + 1
   for (int p = tid; p < A.nnz; p += nt) {
@@ -231,7 +259,13 @@ __device__ void dev_jacobian_active(const DevNet &N, const Ws &W, const Act &A, 
   __syncthreads();
   for (int p = w; p < A.nnz; p += nw) {
     const int e = N.lu_src[A.csrc[p]];
-    if (e < 0) continue;
+    if (e < 0) {
+      if (lane == 0) {
+        A.jval[p] = 0.0;
+        A.jflag[p] = JF_FILL;
+      }
+      continue;
+    }
     double acc = 0.0;
     int set = 0;
     for (int t = off[p] + lane; t < off[p + 1]; t += 32) {
@@ -243,33 +277,164 @@ __device__ void dev_jacobian_active(const DevNet &N, const Ws &W, const Act &A, 
       set |= __shfl_xor_sync(NUPPN_FULL, set, o);
     }
     if (lane == 0) {
-      W.jac[e] = 1.e-99 + acc;
-      W.eset[e] = (uint8_t)set;
+      A.jval[p] = 1.e-99 + acc;
+      A.jflag[p] = (uint8_t)((set ? JF_SET : 0) | (N.jdiag[N.jrow[e]] == e ? JF_DIAG : 0));
     }
   }
   __syncthreads();
 }
 
-// I - hJ on the active subsystem (reduce_jacobian semantics) and its factorization.
-// Returns false if a dependency wait timed out.
-__device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h) {
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
-  for (int p = tid; p < A.nnz; p += nt) {
-    int e = N.lu_src[A.csrc[p]];
-    double val = 0.0;
-    if (e >= 0) {
-      double v = W.jac[e] * (-h);
-      bool set = W.eset[e] != 0;
-      if (set && (fabs(v) == 0.0 || v == -1.0)) { set = false; W.eset[e] = 0; }
-      if (N.jdiag[N.jrow[e]] == e) { set = true; W.eset[e] = 1; v = v + 1.0; }  // active rows are masked
-      if (set) val = v;
+// Jacobian values and flags of the compact positions from a full Jacobian in W.jac / W.eset (the
+// reduced-solve parity entry point supplies them instead of dev_jacobian_active).
+__device__ void dev_load_active_jacobian(const DevNet &N, const Ws &W, Act &A) {
+  for (int p = threadIdx.x; p < A.nnz; p += blockDim.x) {
+    const int e = N.lu_src[A.csrc[p]];
+    if (e < 0) {
+      A.jval[p] = 0.0;
+      A.jflag[p] = JF_FILL;
+    } else {
+      A.jval[p] = W.jac[e];
+      A.jflag[p] = (uint8_t)((W.eset[e] ? JF_SET : 0) | (N.jdiag[N.jrow[e]] == e ? JF_DIAG : 0));
     }
-    A.cval[p] = val;
   }
   __syncthreads();
+}
+
+// Entry p of I - hJ under reduce_jacobian's rules (jac_rhs.F90:97-140): an entry that was set but
+// scales to 0 or -1 is dropped for the rest of this Jacobian's levels; the diagonal of every active
+// row is set and gets the identity added.
+__device__ __forceinline__ double assemble_entry(Act &A, int p, double h) {
+  const uint8_t f = A.jflag[p];
+  if (f & JF_FILL) return 0.0;
+  double v = A.jval[p] * (-h);
+  bool set = (f & JF_SET) != 0;
+  if (set && (fabs(v) == 0.0 || v == -1.0)) {
+    set = false;
+    A.jflag[p] = (uint8_t)(f & ~JF_SET);
+  }
+  if (f & JF_DIAG) {
+    set = true;
+    A.jflag[p] = (uint8_t)(A.jflag[p] | JF_SET);
+    v = v + 1.0;
+  }
+  return set ? v : 0.0;
+}
+
+__device__ __forceinline__ bool pivot_ok(double d) { return d != 0.0 && isfinite(d); }
+
+// Right-looking elimination of a dense tile by one warp; lane l owns rows l + 32 i (i < R), so the
+// updates of one pivot step are independent across lanes. The L column is scaled by the reciprocal
+// of the pivot, as SuperLU does (dpivotL.c:178-180). Returns false on a zero or non-finite pivot.
+template <int R>
+__device__ bool tile_factor_warp(double *T, double *rinv, int na, int lane) {
+  constexpr int S = 32 * R;
+  int bad = 0;
+  for (int k = 0; k < na; ++k) {
+    const double piv = T[k * (S + 1)];
+    bad |= !pivot_ok(piv);
+    const double rp = 1.0 / piv;
+    if (lane == 0) rinv[k] = rp;
+    double l[R];
+    bool any = false;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int r = lane + 32 * i;
+      l[i] = 0.0;
+      if (r > k && r < na) {
+        double a = T[k * S + r];
+        if (a != 0.0) {
+          a = a * rp;
+          T[k * S + r] = a;
+        }
+        l[i] = a;
+      }
+      any |= l[i] != 0.0;
+    }
+    if (any)
+      for (int m = k + 1; m < na; ++m) {
+        const double u = T[m * S + k];
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+          if (l[i] != 0.0) T[m * S + lane + 32 * i] -= l[i] * u;
+      }
+    __syncwarp();
+  }
+  return bad == 0;
+}
+
+// Forward and backward substitution of a factored tile by one warp, x[i] holding row lane + 32 i:
+// per column one broadcast and one fused multiply-add per row. Column-oriented like SuperLU's
+// dgstrs; the diagonal is applied as the reciprocal computed by the factorization.
+template <int R>
+__device__ __forceinline__ void tile_solve_regs(const double *T, int na, double (&x)[R], const double (&ri)[R],
+                                                int lane) {
+  constexpr int S = 32 * R;
+  for (int c = 0; c < na - 1; ++c) {
+    const double xc = __shfl_sync(NUPPN_FULL, (R == 1 || c < 32) ? x[0] : x[R - 1], c & 31);
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int r = lane + 32 * i;
+      if (r > c) {
+        const double l = T[c * S + r];
+        if (l != 0.0) x[i] -= l * xc;
+      }
+    }
+  }
+  for (int c = na - 1; c >= 0; --c) {
+#pragma unroll
+    for (int i = 0; i < R; ++i)
+      if (lane + 32 * i == c) x[i] *= ri[i];
+    const double xc = __shfl_sync(NUPPN_FULL, (R == 1 || c < 32) ? x[0] : x[R - 1], c & 31);
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int r = lane + 32 * i;
+      if (r < c) {
+        const double u = T[c * S + r];
+        if (u != 0.0) x[i] -= u * xc;
+      }
+    }
+  }
+}
+
+// Tile solve in place on A.xs by the calling warp.
+template <int R>
+__device__ void tile_solve_xs(const Act &A, int lane) {
+  double x[R], ri[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int r = lane + 32 * i;
+    x[i] = r < A.na ? A.xs[r] : 0.0;
+    ri[i] = r < A.na ? A.rinv[r] : 0.0;
+  }
+  tile_solve_regs<R>(A.T, A.na, x, ri, lane);
+#pragma unroll
+  for (int i = 0; i < R; ++i)
+    if (lane + 32 * i < A.na) A.xs[lane + 32 * i] = x[i];
+}
+
+// I - hJ on the active subsystem and its factorization in the static order, no pivoting.
+// Returns false on a zero or non-finite pivot, or if a dependency wait timed out.
+__device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h) {
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
+  const int na = A.na;
+  if (A.tile) {
+    // dense tile, column-major: T[c*S + r] = entry (r, c); rows na..S-1 stay zero
+    const int S = A.tile_rows;
+    double *T = A.T;
+    for (int i = tid; i < na * S; i += nt) T[i] = 0.0;
+    __syncthreads();
+    for (int c = w; c < na; c += nw)
+      for (int p = A.crp[c] + lane; p < A.crp[c + 1]; p += 32) T[A.ccol[p] * S + c] = assemble_entry(A, p, h);
+    __syncthreads();
+    int bad = 0;
+    if (w == 0) bad = !(S == 32 ? tile_factor_warp<1>(T, A.rinv, na, lane) : tile_factor_warp<2>(T, A.rinv, na, lane));
+    return __syncthreads_or(bad) == 0;
+  }
+  for (int p = tid; p < A.nnz; p += nt) A.cval[p] = assemble_entry(A, p, h);
+  __syncthreads();
   if (A.onewarp) {  // one warp, rows in order
+    int bad = 0;
     if (w == 0) {
-      const int na = A.na;
       const int *crp = A.crp, *cdiag = A.cdiag, *ccol = A.ccol;  // plain: rewritten per Jacobian
       double *cval = A.cval, *wb = A.wbuf;
       for (int c = 0; c < na; ++c) {
@@ -280,7 +445,7 @@ __device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h
           const int j = ccol[p];
           const double a = wb[j];
           if (a != 0.0) {
-            const double l = a / cval[cdiag[j]];
+            const double l = a * (1.0 / cval[cdiag[j]]);
             const int qe = crp[j + 1];
             for (int q = cdiag[j] + 1 + lane; q < qe; q += 32) wb[ccol[q]] -= l * cval[q];
             __syncwarp();
@@ -290,15 +455,15 @@ __device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h
         }
         for (int p = rs + lane; p < re; p += 32) cval[p] = wb[ccol[p]];
         __syncwarp();
+        bad |= !pivot_ok(cval[dg]);
       }
     }
-    __syncthreads();
-    return true;
+    return __syncthreads_or(bad) == 0;
   }
   const int gen = ++A.genF;
   bool ok = true;
-  double *wb = A.wbuf + (size_t)w * A.na;
-  for (int c = w; c < A.na; c += nw) {
+  double *wb = A.wbuf + (size_t)w * na;
+  for (int c = w; c < na; c += nw) {
     const int rs = A.crp[c], re = A.crp[c + 1], dg = A.cdiag[c];
     for (int p = rs + lane; p < re; p += 32) wb[A.ccol[p]] = A.cval[p];
     __syncwarp();
@@ -308,7 +473,7 @@ __device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h
       __syncwarp();
       const double a = wb[j];
       if (a != 0.0) {
-        const double l = a / A.cval[A.cdiag[j]];
+        const double l = a * (1.0 / A.cval[A.cdiag[j]]);
         const int qe = A.crp[j + 1];
         for (int q = A.cdiag[j] + 1 + lane; q < qe; q += 32) wb[A.ccol[q]] -= l * A.cval[q];
         __syncwarp();
@@ -317,6 +482,8 @@ __device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h
       __syncwarp();
     }
     for (int p = rs + lane; p < re; p += 32) A.cval[p] = wb[A.ccol[p]];
+    __syncwarp();
+    if (!pivot_ok(A.cval[dg])) ok = false;
     __threadfence_block();
     __syncwarp();
     if (lane == 0) *(volatile int *)&A.flagF[c] = gen;
@@ -328,10 +495,18 @@ __device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h
 // Solve the factored active subsystem in place on A.xs (compact right-hand side in, solution out).
 __device__ bool dev_solve_active(Act &A) {
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
+  if (A.tile) {
+    if (w == 0) {
+      if (A.tile_rows == 32) tile_solve_xs<1>(A, lane);
+      else tile_solve_xs<2>(A, lane);
+    }
+    __syncthreads();
+    return true;
+  }
   if (A.onewarp) {  // one warp: forward then backward substitution, a row at a time
     if (w == 0) {
-      // plain pointers: the factors and levels are rewritten within the kernel, so loads must not
-      // go through the non-coherent read-only cache
+      // plain pointers: the factors are rewritten within the kernel, so loads must not go through
+      // the non-coherent read-only cache
       const int *crp = A.crp, *cdiag = A.cdiag, *ccol = A.ccol;
       const double *cval = A.cval;
       double *xs = A.xs;
@@ -408,42 +583,36 @@ __device__ bool dev_solve_species(const DevNet &N, Act &A, const double *rhs, do
 //
 // Within one step only dX/dt of masked species is used (the rest of the correction is zero, as in
 // ddecompac, jac_rhs.F90:584-608) and unmasked abundances stay frozen. A reaction with an unmasked
-// reactant did not pass the dynamic-network test (its flux is <= cyminformal/dt, jac_rhs.F90:350-353,
-// or all its participants would be masked), and that flux cannot grow within the step beyond the
-// change of its masked reactant. So the step keeps exactly the reactions whose reactants are all
-// masked (or gamma), and each masked species sums their contributions in the reference's order
-// (reaction order, then k1, k3, k5, k7).
+// reactant did not pass the dynamic-network test itself (jac_rhs.F90:350-353: otherwise all its
+// participants would be masked), so its flux is at most y * cyminformal / dt for the frozen
+// reactant's abundance y, and it changes X by at most ~1e-30 over the step; such reactions are left
+// out. Each masked species keeps, in the reference's accumulation order (reaction order, then k1,
+// k3, k5, k7), one gather item per term of a kept reaction: the term's coefficient, the reaction's
+// (1/k2!) * rate and the compact indices of its reactants. A sub-step recomputes each term's flux
+// from those with the reference's operations, so no per-reaction pass or flux array is needed.
 __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem, size_t smem_bytes, int *sint) {
   const int tid = threadIdx.x, nt = blockDim.x, nw = nt >> 5;
-  int *rmap = W.act_rtmp;                    // [nact]
-  int *off = W.act_tmp + 3 * (N.nsys + 1);   // [na+1] segment offsets of the static species lists
-  int *flag = W.act_itmp;                    // [T] kept flags -> positions
-  const int g = N.ig;
-  for (int a = tid; a < N.nact; a += nt) {
-    const int *k = N.act_k + (size_t)a * 8;
-    rmap[a] = (W.mask[k[0]] && (k[2] == g || W.mask[k[2]])) ? 1 : 0;
-  }
-  for (int c = tid; c < A.na; c += nt) {
+  int *off = W.act_tmp + 3 * (N.nsys + 1);  // [na+1] segment offsets of the static species lists
+  int *flag = W.act_itmp;                   // [T] kept flags -> positions
+  const int *sys2c = W.act_tmp;             // system index -> active row (dev_compact), -1 if frozen
+  const int g = N.ig, na = A.na;
+  for (int c = tid; c < na; c += nt) {
     const int s = N.sp_of_sys[A.arow[c]];
     off[c] = N.dg_ptr[s + 1] - N.dg_ptr[s];
   }
   __syncthreads();
-  const int nar = block_scan_excl(rmap, N.nact, sint);
-  const int T = block_scan_excl(off, A.na, sint);
-  if (tid == 0) off[A.na] = T;
-  for (int a = tid; a < N.nact; a += nt) {  // rmap: kept reaction -> compact index, else -1
-    const int *k = N.act_k + (size_t)a * 8;
-    if (!(W.mask[k[0]] && (k[2] == g || W.mask[k[2]]))) rmap[a] = -1;
-  }
+  const int T = block_scan_excl(off, na, sint);
+  if (tid == 0) off[na] = T;
   __syncthreads();
   for (int t = tid; t < T; t += nt) {  // flattened static lists of the masked species
-    const int c = seg_of(off, A.na, t);
-    const int s = N.sp_of_sys[A.arow[c]];
-    flag[t] = rmap[N.dg_item[N.dg_ptr[s] + (t - off[c])] >> 2] >= 0 ? 1 : 0;
+    const int c = seg_of(off, na, t);
+    const int a = N.dg_item[N.dg_ptr[N.sp_of_sys[A.arow[c]]] + (t - off[c])] >> 2;
+    const int *k = N.act_k + (size_t)a * 8;
+    flag[t] = (W.mask[k[0]] && (k[2] == g || W.mask[k[2]])) ? 1 : 0;
   }
   __syncthreads();
   const int ngi = block_scan_excl(flag, T, sint);
-  const size_t lu_need = act_bytes(A.na, A.nnz, nw), need = rhs_bytes(A.na, nar, ngi);
+  const size_t lu_need = act_bytes(na, A.nnz, nw, A.tile_rows), need = rhs_bytes(na, ngi);
   char *base;
   if (A.in_smem && lu_need + need <= smem_bytes) {
     base = smem + lu_need;
@@ -452,50 +621,47 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
     base = W.act_r;
     A.rhs_in_smem = false;
   }
-  auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };
-  A.ar = (int *)base; base += a16((size_t)nar * 4);
-  A.gptr = (int *)base; base += a16((size_t)(A.na + 1) * 4);
-  A.gitem = (int *)base; base += a16((size_t)ngi * 4);
+  A.gptr = (int *)base; base += a16((size_t)(na + 1) * 4);
   A.gcoef = (float *)base; base += a16((size_t)ngi * 4);
-  A.flux = (double *)base;
-  A.nar = nar;
+  A.grpk = (uint32_t *)base; base += a16((size_t)ngi * 4);
+  A.grcv = (double *)base;
   A.ngi = ngi;
-  for (int a = tid; a < N.nact; a += nt)
-    if (rmap[a] >= 0) A.ar[rmap[a]] = a;
-  for (int c = tid; c <= A.na; c += nt) A.gptr[c] = (c < A.na && off[c] < T) ? flag[off[c]] : ngi;
+  for (int c = tid; c <= na; c += nt) A.gptr[c] = (c < na && off[c] < T) ? flag[off[c]] : ngi;
   for (int t = tid; t < T; t += nt) {
-    const int c = seg_of(off, A.na, t);
-    const int s = N.sp_of_sys[A.arow[c]];
-    const int p = N.dg_ptr[s] + (t - off[c]);
-    const int r = rmap[N.dg_item[p] >> 2];
-    if (r >= 0) {
-      A.gitem[flag[t]] = r;
-      A.gcoef[flag[t]] = (float)N.dg_coef[p];
-    }
+    const int c = seg_of(off, na, t);
+    const int p = N.dg_ptr[N.sp_of_sys[A.arow[c]]] + (t - off[c]);
+    const int a = N.dg_item[p] >> 2;
+    const int *k = N.act_k + (size_t)a * 8;
+    if (!(W.mask[k[0]] && (k[2] == g || W.mask[k[2]]))) continue;
+    const int q = flag[t];
+    const uint32_t i1 = (uint32_t)sys2c[N.sys_of_sp[k[0]]];
+    const uint32_t i2 = k[2] == g ? (uint32_t)na : (uint32_t)sys2c[N.sys_of_sp[k[2]]];
+    A.gcoef[q] = (float)N.dg_coef[p];  // -k2, -1, k6 or k8: small integers, exact in float
+    A.grcv[q] = c_fact[k[1]] * W.v[N.act_slot[a]];
+    A.grpk[q] = i1 | (i2 << 14) | ((uint32_t)k[1] << 28);
   }
-  if (tid == 0) W.xn[g] = 1.0;  // gamma's molar abundance
   __syncthreads();
 }
 
-// calculate_dxdt restricted to the kept reactions: compact abundances yc in, compact dX/dt out.
-__device__ void dev_dxdt_active(const DevNet &N, const Ws &W, const Act &A, const double *yc, double *dxc) {
+// dX/dt of active row c from the compact molar abundances A.xnc: each term's flux is
+// (1/k2!) v xn(k1)^k2 xn(k3) as in calculate_dxdt (jac_rhs.F90:245-252), accumulated in the
+// reference's order and multiplied by A at the end (jac_rhs.F90:266-270).
+__device__ __forceinline__ double gather_dxdt(const Act &A, int c) {
+  double acc = 0.0;
+  for (int q = A.gptr[c]; q < A.gptr[c + 1]; ++q) {
+    const uint32_t pk = A.grpk[q];
+    const double flux = A.grcv[q] * powi(A.xnc[pk & 0x3fff], (int)(pk >> 28)) * A.xnc[(pk >> 14) & 0x3fff];
+    acc = acc + (double)A.gcoef[q] * flux;
+  }
+  return acc * A.anc[c];
+}
+
+// calculate_dxdt on the active rows: compact abundances yc in, compact dX/dt out.
+__device__ void dev_dxdt_active(const Act &A, const double *yc, double *dxc) {
   const int tid = threadIdx.x, nt = blockDim.x;
-  for (int c = tid; c < A.na; c += nt) {
-    const int s = N.sp_of_sys[A.arow[c]];
-    W.xn[s] = yc[c] / N.an[s];
-  }
+  for (int c = tid; c < A.na; c += nt) A.xnc[c] = yc[c] / A.anc[c];
   __syncthreads();
-  for (int r = tid; r < A.nar; r += nt) {
-    const int a = A.ar[r];
-    const int *k = N.act_k + (size_t)a * 8;
-    A.flux[r] = c_fact[k[1]] * W.v[N.act_slot[a]] * powi(W.xn[k[0]], k[1]) * W.xn[k[2]];
-  }
-  __syncthreads();
-  for (int c = tid; c < A.na; c += nt) {
-    double acc = 0.0;
-    for (int p = A.gptr[c]; p < A.gptr[c + 1]; ++p) acc = acc + (double)A.gcoef[p] * A.flux[A.gitem[p]];
-    dxc[c] = acc * N.an[N.sp_of_sys[A.arow[c]]];
-  }
+  for (int c = tid; c < A.na; c += nt) dxc[c] = gather_dxdt(A, c);
   __syncthreads();
 }
 

@@ -67,7 +67,7 @@ struct nuppn_net {
   DevBuf ws, stage, counter;
   int ws_slots = 0;
   int block = 256;
-  int act_smem = 64 * 1024;  // shared-memory budget per CTA for the active-subsystem LU
+  int act_smem = 72 * 1024;  // shared-memory budget per CTA for the active subsystem (3 CTAs per SM)
   int device = 0;
   int nsm = 0;
   int64_t launches = 0;
@@ -185,12 +185,10 @@ WsLayout layout(const HostNet &H) {
   L.yerr = take((size_t)(kMaxLevels + 1) * H.nsp * d); L.lu = take((size_t)H.nnzLU * d);
   L.bsys = take(H.nsys * d); L.xsys = take(H.nsys * d); L.rhs = take(H.nsp * d);
   L.act_tmp = take((size_t)4 * (H.nsys + 1) * sizeof(int));
-  L.act = take(act_bytes(H.nsys, H.nnzLU, 8));
-  L.act_rtmp = take((size_t)(H.nact + 1) * sizeof(int));
+  L.act = take(act_bytes_max(H.nsys, H.nnzLU, 8));
   {
-    auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };
-    size_t ngi = H.dg_item.size(), nar = H.nact, na = H.nsys;
-    L.act_r = take(a16(nar * 4) + a16((na + 1) * 4) + a16(ngi * 4) + a16(ngi * 4) + a16(nar * 8));
+    size_t ngi = H.dg_item.size();
+    L.act_r = take(rhs_bytes(H.nsys, (int)ngi));
     size_t njg = H.jg_item.size();
     L.act_itmp = take((std::max(ngi, njg) + 1) * sizeof(int));
     L.act_otmp = take(((size_t)H.nnzLU + 1) * sizeof(int));
@@ -297,6 +295,11 @@ nuppn_status nuppn_net_create(const nuppn_net_desc *desc, const nuppn_knobs *kno
   net->nsm = prop.multiProcessorCount;
   net->block = kn.threads_per_zone > 0 ? kn.threads_per_zone : 256;
   if (net->block % 32 || net->block > 256) { delete net; set_error("threads_per_zone must be a multiple of 32, <= 256"); return NUPPN_ERR_ARG; }
+  if (kn.lu_precision != 0) {
+    delete net;
+    set_error("lu_precision: only 0 (FP64 factorization) is available in this build");
+    return NUPPN_ERR_ARG;
+  }
   nuppn_status st = upload(net);
   if (st != NUPPN_OK) { delete net; return st; }
   if (configure_kernels(net->act_smem) != cudaSuccess) {

@@ -101,7 +101,7 @@ __device__ int dev_backward_euler(const DevNet &N, const Ws &W, ZoneCtl &C, doub
     bool ok = dev_factor_active(N, W, A, dt);
     for (int c = tid; c < A.na; c += nt) yc[c] = W.y_cur[N.sp_of_sys[A.arow[c]]];
     __syncthreads();
-    dev_dxdt_active(N, W, A, yc, dxc);
+    dev_dxdt_active(A, yc, dxc);
     for (int c = tid; c < A.na; c += nt) {
       const int s = N.sp_of_sys[A.arow[c]];
       A.xs[c] = W.y_old[s] - W.y_cur[s] + dt * dxc[c];
@@ -151,7 +151,7 @@ __device__ int dev_bd_substep(const DevNet &N, const Ws &W, ZoneCtl &C, const Bd
                               bool huge_frozen) {
   const int tid = threadIdx.x, nt = blockDim.x;
   Act &A = C.act;
-  dev_dxdt_active(N, W, A, B.yk, B.dxc);
+  dev_dxdt_active(A, B.yk, B.dxc);
   if (stage == 1) for (int c = tid; c < A.na; c += nt) A.xs[c] = h * B.dxc[c];
   else for (int c = tid; c < A.na; c += nt) A.xs[c] = h * B.dxc[c] - B.dk[c];
   __syncthreads();
@@ -166,6 +166,81 @@ __device__ int dev_bd_substep(const DevNet &N, const Ws &W, ZoneCtl &C, const Bd
     if (yk > 2.0) huge = true;
   }
   return (block_any(huge) || huge_frozen) ? HUGE_ABUNDS : 0;
+}
+
+// All sub-steps of one level (semi_implicit_extrapolation, bader_deuflhard.F90:276-316) for a
+// tile-sized active system, by one warp: lane l keeps y_k and delta_k of active rows l + 32 i in
+// registers, computes their dX/dt from the gather items, and the tile solve needs no block barrier.
+// Same arithmetic as dev_bd_substep. Leaves y_k / delta_k in B.yk / B.dk, and in sflag[0] 0 or
+// HUGE_ABUNDS, in sflag[1] the number of solves.
+template <int R>
+__device__ void bd_level_tile_warp(const Act &A, const BdVec &B, double h, int nseq, bool huge_frozen, int *sflag) {
+  const int lane = threadIdx.x & 31, na = A.na;
+  double y[R], d[R], ri[R], an[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int r = lane + 32 * i;
+    const bool on = r < na;
+    y[i] = on ? B.yk[r] : 0.0;
+    d[i] = 0.0;
+    ri[i] = on ? A.rinv[r] : 0.0;
+    an[i] = on ? A.anc[r] : 1.0;
+  }
+  int err = 0, ns = 0;
+  for (int j = 0; j <= nseq; ++j) {
+    const int stage = j == 0 ? 1 : (j < nseq ? 2 : 3);  // FIRST, MID, LAST
+    __syncwarp();  // every lane has finished reading xnc of the previous sub-step
+#pragma unroll
+    for (int i = 0; i < R; ++i)
+      if (lane + 32 * i < na) A.xnc[lane + 32 * i] = y[i] / an[i];
+    __syncwarp();
+    double x[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int r = lane + 32 * i;
+      x[i] = 0.0;
+      if (r < na) {
+        const double dx = gather_dxdt(A, r);
+        x[i] = stage == 1 ? h * dx : h * dx - d[i];
+      }
+    }
+    tile_solve_regs<R>(A.T, na, x, ri, lane);
+    ++ns;
+    bool huge = false;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      d[i] = stage == 2 ? d[i] + 2.0 * x[i] : x[i];
+      y[i] = y[i] + d[i];
+      huge |= lane + 32 * i < na && y[i] > 2.0;
+    }
+    if (__any_sync(NUPPN_FULL, huge) || huge_frozen) {
+      err = HUGE_ABUNDS;
+      break;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < R; ++i)
+    if (lane + 32 * i < na) {
+      B.yk[lane + 32 * i] = y[i];
+      B.dk[lane + 32 * i] = d[i];
+    }
+  if (lane == 0) {
+    sflag[0] = err;
+    sflag[1] = ns;
+  }
+}
+
+__device__ int dev_bd_level_tile(const Act &A, const BdVec &B, double h, int nseq, bool huge_frozen, int &nsolve,
+                                 int *sflag) {
+  if ((threadIdx.x >> 5) == 0) {
+    if (A.tile_rows == 32) bd_level_tile_warp<1>(A, B, h, nseq, huge_frozen, sflag);
+    else bd_level_tile_warp<2>(A, B, h, nseq, huge_frozen, sflag);
+  }
+  __syncthreads();
+  const int err = sflag[0];
+  nsolve += sflag[1];
+  __syncthreads();
+  return err;
 }
 
 // extrapolate (bader_deuflhard.F90:371-407): Neville tableau, column k, on the active rows
@@ -234,9 +309,14 @@ __device__ int dev_bader_deuflhard(const DevNet &N, const Ws &W, ZoneCtl &C, dou
       return BAD_STEP;
     }
     C.st.nfact++;
-    int ierr = dev_bd_substep(N, W, C, B, h, 1, huge_fz);
-    for (int i = 1; ierr == 0 && i <= N.nseq[k] - 1; ++i) ierr = dev_bd_substep(N, W, C, B, h, 2, huge_fz);
-    if (ierr == 0) ierr = dev_bd_substep(N, W, C, B, h, 3, huge_fz);
+    int ierr;
+    if (A.tile) {
+      ierr = dev_bd_level_tile(A, B, h, N.nseq[k], huge_fz, C.st.nsolve, C.sint);
+    } else {
+      ierr = dev_bd_substep(N, W, C, B, h, 1, huge_fz);
+      for (int i = 1; ierr == 0 && i <= N.nseq[k] - 1; ++i) ierr = dev_bd_substep(N, W, C, B, h, 2, huge_fz);
+      if (ierr == 0) ierr = dev_bd_substep(N, W, C, B, h, 3, huge_fz);
+    }
     if (ierr != 0) {
       dtrcmd = dt * 0.2;
       return ierr;

@@ -146,6 +146,9 @@ std::string build_host_net(const nuppn_net_desc &d, const nuppn_knobs &kn, HostN
       if (k[s] < 0 || k[s] >= nsp) return "descriptor: k index out of range in reaction " + std::to_string(l);
     if (k[1] < 0 || k[1] > 4 || k[3] < 0 || k[3] > 4) return "descriptor: reactant count outside 0..4";
     if (k[0] == H.ig || k[6] == H.ig) return "descriptor: k1/k7 is the gamma slot";
+    for (int s = 0; s < 8; s += 2)
+      if (k[s] != H.ig && !H.ciso[k[s]])
+        return "descriptor: considered reaction " + std::to_string(l) + " has a species that is not considered";
     if (H.irev[l] >= nre) return "descriptor: irev out of range";
   }
   // ---- nuclear data (nse_swj.F90:186-196)
@@ -334,6 +337,7 @@ std::string build_host_net(const nuppn_net_desc &d, const nuppn_knobs &kn, HostN
   for (int i = 0; i < nsp; ++i)
     if (H.ciso[i] && i != H.ig) sys0.push_back(i);
   int n = (int)sys0.size();
+  if (n >= (1 << 14) - 1) return "more than 16382 species in the linear system";  // 14-bit compact indices
   H.nsys = n;
   std::vector<int> sidx0(nsp, -1);
   for (int q = 0; q < n; ++q) sidx0[sys0[q]] = q;

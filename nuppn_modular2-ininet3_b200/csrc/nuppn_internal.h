@@ -92,23 +92,57 @@ struct WsLayout {
   size_t v, rv, ngv, ffv, kdv, partinter, G, flux, contrib, first_l, eset, jac, mask, xn, dxdt;
   size_t y, y_old, y_cur, y_new, y_k, delta_k, y_ext, yscal, qcol, yerr, lu, bsys, xsys, rhs;
   size_t act_tmp, act;           // compaction scratch (ints) and the global fallback of the active LU
-  size_t act_rtmp, act_r;        // reaction keep-map scratch and the restricted right-hand side
+  size_t act_r;                  // global fall-back of the restricted right-hand side
   size_t act_itmp, act_otmp, act_dtmp, act_btmp, bd;  // flattened-gather scratch, compact BD vectors
   size_t bytes;
 };
 
-// Bytes of the active-subsystem LU for na rows, nnz entries and nwarps warps (see active_lu.cuh):
-// int crp[na+1], cdiag[na], arow[na], flagF[na], flagS[na], ccol[nnz], csrc[nnz];
-// double cval[nnz], xs[na], wbuf[nwarps*na]; every array 16-byte aligned.
 #ifdef __CUDACC__
-__host__ __device__
+#define NUPPN_HD __host__ __device__
+#else
+#define NUPPN_HD
 #endif
-inline size_t act_bytes(int na, int nnz, int nwarps) {
-  auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };
-  size_t b = 0;
-  b += a16((size_t)(na + 1) * 4) + 4 * a16((size_t)na * 4) + 2 * a16((size_t)nnz * 4);
-  b += a16((size_t)nnz * 8) + a16((size_t)na * 8) + a16((size_t)nwarps * na * 8);
+
+// Active systems up to kTileMax rows are factored in a dense tile of 32 or 64 rows and solved with
+// one (or two) rows per lane of a warp (active_lu.cuh).
+constexpr int kTileMax = 64;
+
+NUPPN_HD inline size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
+
+// Tile rows (0, 32 or 64) for an active system of na rows under the knob lu_tile_max
+// (0 = kTileMax, negative = never).
+NUPPN_HD inline int tile_rows_for(int na, int limit) {
+  if (limit < 0) return 0;
+  const int lim = (limit == 0 || limit > kTileMax) ? kTileMax : limit;
+  return na > lim ? 0 : (na <= 32 ? 32 : 64);
+}
+
+// Bytes of the active-subsystem LU for na rows, nnz entries, nwarps warps and a tile of tile_rows
+// rows (see active_lu.cuh): int crp[na+1], cdiag[na], arow[na], flagF[na], flagS[na], ccol[nnz],
+// csrc[nnz]; without a tile double cval[nnz], wbuf[nwarps*na]; double xs[na], jval[nnz], anc[na],
+// xnc[na+1]; uint8 jflag[nnz]; with a tile double T[na * tile_rows] (na columns of tile_rows rows),
+// rinv[tile_rows]. Every array 16-byte aligned.
+NUPPN_HD inline size_t act_bytes(int na, int nnz, int nwarps, int tile_rows) {
+  size_t b = a16((size_t)(na + 1) * 4) + 4 * a16((size_t)na * 4) + 2 * a16((size_t)nnz * 4);
+  if (tile_rows == 0) b += a16((size_t)nnz * 8) + a16((size_t)nwarps * na * 8);
+  b += a16((size_t)na * 8);
+  b += a16((size_t)nnz * 8) + a16((size_t)na * 8) + a16((size_t)(na + 1) * 8) + a16((size_t)nnz);
+  b += (size_t)na * tile_rows * 8 + (size_t)tile_rows * 8;
   return b;
+}
+
+// Largest act_bytes over every active system of a network with nsys rows and nnz filled entries.
+NUPPN_HD inline size_t act_bytes_max(int nsys, int nnz, int nwarps) {
+  const int nt = nsys < kTileMax ? nsys : kTileMax;
+  size_t full = act_bytes(nsys, nnz, nwarps, 0);
+  size_t tile = act_bytes(nt, nt * nt < nnz ? nt * nt : nnz, nwarps, nt <= 32 ? 32 : 64);
+  return full > tile ? full : tile;
+}
+
+// Bytes of the restricted right-hand side for na rows and ngi gather items:
+// int gptr[na+1]; float gcoef[ngi]; uint32 grpk[ngi]; double grcv[ngi].
+NUPPN_HD inline size_t rhs_bytes(int na, int ngi) {
+  return a16((size_t)(na + 1) * 4) + 2 * a16((size_t)ngi * 4) + a16((size_t)ngi * 8);
 }
 
 // arguments of the persistent integration kernel

@@ -6,8 +6,10 @@
 //   dxdt        calculate_dxdt              solver/source/jac_rhs.F90:217-278
 //   jacobian    calculate_jacobian          solver/source/jac_rhs.F90:282-455
 //   assemble    reduce_jacobian as I-hJ     solver/source/jac_rhs.F90:134-197
-//   factor      static-pivot sparse LU      (replaces SuperLU dgstrf, c_fortran_dgssv.c:80-155)
-//   solve       level-scheduled L/U solves  (replaces SuperLU dgstrs, c_fortran_dgssv.c:157-174)
+//   factor      static-order LU of the active subsystem, dense tile up to 64 rows, sparse above
+//               (replaces SuperLU dgstrf, c_fortran_dgssv.c:80-155)
+//   solve       column-oriented substitution in registers (tile) or row-oriented sparse solves
+//               (replaces SuperLU dgstrs, c_fortran_dgssv.c:157-174)
 // and the step control of backward_euler.F90:29-176, bader_deuflhard.F90:139-488 and
 // solver.F90:53-238 evaluated uniformly by every thread.
 //
@@ -554,7 +556,7 @@ namespace nuppn {
 // ---------------------------------------------------------------------------------------------
 // kernels: persistent CTAs, one zone at a time, workspace slab per CTA; dynamic shared memory holds
 // the active-subsystem LU when it fits (act_smem bytes).
-__global__ void __launch_bounds__(256) k_integrate(const __grid_constant__ DevNet N, const __grid_constant__ WsLayout L,
+__global__ void __launch_bounds__(256, 3) k_integrate(const __grid_constant__ DevNet N, const __grid_constant__ WsLayout L,
                                                    char *ws, const __grid_constant__ IntegrateArgs A, int act_smem) {
   extern __shared__ __align__(16) char smem_dyn[];
   __shared__ double sred[32];
@@ -628,6 +630,7 @@ __global__ void __launch_bounds__(256) k_phase(const __grid_constant__ DevNet N,
       __syncthreads();
       Act act;
       dev_compact(N, W, act, smem_dyn, act_smem, sint);
+      dev_load_active_jacobian(N, W, act);
       bool ok = dev_factor_active(N, W, act, A.dt[z]);
       ok = dev_solve_species(N, act, W.rhs, W.dxdt) && ok;
       for (int s = tid; s < N.nsp; s += nt) A.out_x[(size_t)z * N.nsp + s] = ok ? W.dxdt[s] : NAN;

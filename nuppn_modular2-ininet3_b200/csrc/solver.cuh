@@ -27,7 +27,6 @@ struct Ws {
   uint8_t *eset, *mask;
   int *act_tmp;  // compaction scratch: sys2c, arow, counts
   char *act;     // global fallback of the active-subsystem LU
-  int *act_rtmp; // reaction keep-map scratch [nact]
   char *act_r;   // global fallback of the restricted right-hand side
   int *act_itmp; // flattened-list flags / positions [max(list items) + 1]
   int *act_otmp; // segment offsets of the active Jacobian entries [nnzLU + 1]
@@ -52,7 +51,6 @@ __device__ __forceinline__ Ws ws_bind(char *base, const WsLayout &L) {
   w.rhs = (double *)(base + L.rhs);
   w.act_tmp = (int *)(base + L.act_tmp);
   w.act = base + L.act;
-  w.act_rtmp = (int *)(base + L.act_rtmp);
   w.act_r = base + L.act_r;
   w.act_itmp = (int *)(base + L.act_itmp);
   w.act_otmp = (int *)(base + L.act_otmp);

@@ -68,11 +68,12 @@ def test_pattern_matches_checker(solver_mod, abi, orc, net300):
     assert (r == rr).all() and (c == cr).all() and (m == mr).all()
 
 
-def test_reduced_solve_matches_superlu(solver_mod, abi, orc, net300, batch):
-    dev = _dev(solver_mod, net300, abi)
+@pytest.mark.parametrize("tile", [0, -1], ids=["tile", "sparse"])
+@pytest.mark.parametrize("dt", [1.0e2, 1.0e8])
+def test_reduced_solve_matches_superlu(solver_mod, abi, orc, net300, batch, tile, dt):
+    dev = _dev(solver_mod, net300, abi, lu_tile_max=tile)
     ref = orc.Oracle(net300, abi.default_knobs())
     vr = ref.evaluate_all_rates(batch.t9_0, batch.rho_0, batch.ye, batch.X)
-    dt = 1.0e8
     jr, esr, mkr = ref.calculate_jacobian(vr, batch.X, dt)
     rng = np.random.default_rng(5)
     b = rng.normal(size=(batch.nz, net300.nsp)) * 1e-3
@@ -90,9 +91,10 @@ def _compare_X(X, Xr):
     return rel.max(initial=0.0), small.max(initial=0.0)
 
 
-def test_integrate_bd_matches_checker(solver_mod, abi, orc, net300, batch):
+@pytest.mark.parametrize("tile", [0, -1], ids=["tile", "sparse"])
+def test_integrate_bd_matches_checker(solver_mod, abi, orc, net300, batch, tile):
     kn = abi.default_knobs(integration_method=1)
-    dev = _dev(solver_mod, net300, abi, integration_method=1)
+    dev = _dev(solver_mod, net300, abi, integration_method=1, lu_tile_max=tile)
     ref = orc.Oracle(net300, kn)
     args = (batch.X, batch.t9_0, batch.t9_1, batch.rho_0, batch.rho_1, batch.ye, batch.dtwant)
     X, ye, ierr, st, _ = dev.integrate_network(*args)
@@ -104,17 +106,46 @@ def test_integrate_bd_matches_checker(solver_mod, abi, orc, net300, batch):
     assert np.abs(X.sum(axis=1) - 1.0).max() < 1e-10
 
 
-def test_integrate_be_hburn_matches_checker(solver_mod, abi, orc, wl):
+@pytest.mark.parametrize("tile", [0, -1], ids=["tile", "sparse"])
+def test_integrate_be_hburn_matches_checker(solver_mod, abi, orc, wl, tile):
+    """ppn frame of the H-burning zone, backward Euler. The first frame step from the initial
+    composition is ill-conditioned in the reference's own algorithm (its Newton iteration does not
+    converge on the first try, and 1-ulp changes of the input change its sub-step sequence; see
+    test_cpu_oracle.test_hburn_first_step_ill_conditioned), so that step is checked for success and
+    mass conservation only; frame steps 1..39 then run on both sides from the checker's state."""
     net = wl.network(300)
     zb, dts = wl.hburn_zone(net)
     kn = abi.default_knobs(integration_method=0)
-    dev = _dev(solver_mod, net, abi, integration_method=0)
+    dev = _dev(solver_mod, net, abi, integration_method=0, lu_tile_max=tile)
     ref = orc.Oracle(net, kn)
-    X, Xr = zb.X.copy(), zb.X.copy()
-    ye, yer = zb.ye.copy(), zb.ye.copy()
-    for dt in dts[:40]:
-        X, ye, ierr, _, _ = dev.integrate_network(X, zb.t9_0, zb.t9_1, zb.rho_0, zb.rho_1, ye, dt)
-        Xr, yer, ierr_r, _, _ = ref.integrate_network(Xr, zb.t9_0, zb.t9_1, zb.rho_0, zb.rho_1, yer, dt)
+    args = (zb.t9_0, zb.t9_1, zb.rho_0, zb.rho_1)
+    X0, ye0, ierr0, _, _ = dev.integrate_network(zb.X, *args, zb.ye, dts[0])
+    Xr, yer, ierr_r, _, _ = ref.integrate_network(zb.X, *args, zb.ye, dts[0])
+    assert ierr0[0] == ierr_r[0] == 0
+    assert abs(X0.sum() - 1.0) < 1e-10
+    X, ye = Xr.copy(), yer.copy()
+    for dt in dts[1:40]:
+        X, ye, ierr, _, _ = dev.integrate_network(X, *args, ye, dt)
+        Xr, yer, ierr_r, _, _ = ref.integrate_network(Xr, *args, yer, dt)
         assert ierr[0] == ierr_r[0] == 0
+    rel, ab = _compare_X(X, Xr)
+    assert rel <= 1e-6 and ab <= 1e-15, (rel, ab)
+
+
+def test_integrate_bd_wide_tile_matches_checker(solver_mod, abi, orc, wl):
+    """The hottest He-shell zones of the 1109-species network keep 33..64 species active, which runs
+    the 64-row tile (two rows per lane); checked against the checker at the same tolerance."""
+    net = wl.network(1107)
+    full = wl.heshell_batch(1024, net=net, seed=2)
+    zb = full.take(np.argsort(-full.t9_0)[:4])
+    kn = abi.default_knobs(integration_method=1)
+    dev = _dev(solver_mod, net, abi, integration_method=1)
+    ref = orc.Oracle(net, kn)
+    args = (zb.X, zb.t9_0, zb.t9_1, zb.rho_0, zb.rho_1, zb.ye, zb.dtwant)
+    X, ye, ierr, st, _ = dev.integrate_network(*args)
+    Xr, yer, ierr_r, str_, _ = ref.integrate_network(*args, nthreads=4)
+    assert max(s.nvar1_max for s in st) > 32
+    assert (ierr == ierr_r).all()
+    assert [s.nsucc for s in st] == [s.nsucc for s in str_]
     rel, ab = _compare_X(X, Xr)
     assert rel <= 1e-6 and ab <= 1e-15, (rel, ab)
