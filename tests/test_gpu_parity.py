@@ -132,20 +132,60 @@ def test_integrate_be_hburn_matches_checker(solver_mod, abi, orc, wl, tile):
     assert rel <= 1e-6 and ab <= 1e-15, (rel, ab)
 
 
-def test_integrate_bd_wide_tile_matches_checker(solver_mod, abi, orc, wl):
-    """The hottest He-shell zones of the 1109-species network keep 33..64 species active, which runs
-    the 64-row tile (two rows per lane); checked against the checker at the same tolerance."""
+@pytest.fixture(scope="module")
+def hot1107(wl, orc, abi):
+    """The four hottest He-shell zones of the 1109-species network, advanced 1e9 s by the checker:
+    their dynamic networks keep 33..64 species at dt >= 1e8 s (the 64-row tile, two rows per lane)."""
     net = wl.network(1107)
     full = wl.heshell_batch(1024, net=net, seed=2)
     zb = full.take(np.argsort(-full.t9_0)[:4])
-    kn = abi.default_knobs(integration_method=1)
+    ref = orc.Oracle(net, abi.default_knobs(integration_method=1))
+    X, _, ierr, _, _ = ref.integrate_network(zb.X, zb.t9_0, zb.t9_1, zb.rho_0, zb.rho_1, zb.ye, np.full(4, 1e9),
+                                             nthreads=4)
+    assert (ierr == 0).all()
+    return net, zb, X, ref
+
+
+@pytest.mark.parametrize("tile", [0, -1], ids=["tile", "sparse"])
+@pytest.mark.parametrize("dt", [1.0e2, 1.0e8, 1.0e10])
+def test_reduced_solve_wide_matches_superlu(solver_mod, abi, hot1107, tile, dt):
+    net, zb, X, ref = hot1107
+    v = ref.evaluate_all_rates(zb.t9_1, zb.rho_1, zb.ye, X)
+    jr, esr, mkr = ref.calculate_jacobian(v, X, dt)
+    na = mkr.sum(axis=1)
+    if dt >= 1.0e8:
+        assert ((na > 32) & (na <= 64)).all(), na
+    dev = _dev(solver_mod, net, abi, lu_tile_max=tile)
+    b = np.random.default_rng(7).normal(size=(zb.nz, net.nsp)) * 1e-3
+    x = dev.solve_reduced(jr, esr, mkr, dt, b)
+    xr, ierr = ref.solve_reduced(jr, esr, mkr, dt, b)
+    assert (ierr == 0).all()
+    err = np.abs(x - xr).max(axis=1) / np.abs(xr).max(axis=1)
+    assert err.max() < 1e-9, err
+
+
+def test_integrate_bd_hot_zones_within_reference_spread(solver_mod, abi, orc, wl):
+    """Full 1e10 s integrations of the four hottest He-shell zones. Half of their Bader-Deuflhard
+    steps are rejected, and in the reference's own algorithm 1-ulp changes of the input change the
+    step sequence and the final abundances by up to tens of percent (see
+    test_cpu_oracle.test_hot_heshell_zones_ill_conditioned). The device result must succeed, conserve
+    mass, and lie within the spread that the checker itself shows under such perturbations."""
+    net = wl.network(1107)
+    full = wl.heshell_batch(1024, net=net, seed=2)
+    zb = full.take(np.argsort(-full.t9_0)[:4])
+    args = (zb.t9_0, zb.t9_1, zb.rho_0, zb.rho_1, zb.ye, zb.dtwant)
+    ref = orc.Oracle(net, abi.default_knobs(integration_method=1))
+    X0, _, ierr_r, _, _ = ref.integrate_network(zb.X, *args, nthreads=4)
+    big = X0 > 1e-12
+    rel = lambda X: (np.abs(X - X0) * big / np.where(big, X0, 1.0)).max(axis=1)
+    spread = np.zeros(zb.nz)
+    for trial in (1, 2, 3):
+        Xp = zb.X * (1.0 + np.random.default_rng(trial).choice([-1.0, 0.0, 1.0], size=zb.X.shape) * 2.2e-16)
+        X1, _, _, _, _ = ref.integrate_network(Xp, *args, nthreads=4)
+        spread = np.maximum(spread, rel(X1))
     dev = _dev(solver_mod, net, abi, integration_method=1)
-    ref = orc.Oracle(net, kn)
-    args = (zb.X, zb.t9_0, zb.t9_1, zb.rho_0, zb.rho_1, zb.ye, zb.dtwant)
-    X, ye, ierr, st, _ = dev.integrate_network(*args)
-    Xr, yer, ierr_r, str_, _ = ref.integrate_network(*args, nthreads=4)
+    X, ye, ierr, st, _ = dev.integrate_network(zb.X, *args)
+    assert (ierr == 0).all() and (ierr_r == 0).all()
     assert max(s.nvar1_max for s in st) > 32
-    assert (ierr == ierr_r).all()
-    assert [s.nsucc for s in st] == [s.nsucc for s in str_]
-    rel, ab = _compare_X(X, Xr)
-    assert rel <= 1e-6 and ab <= 1e-15, (rel, ab)
+    assert np.abs(X.sum(axis=1) - 1.0).max() < 1e-10
+    assert (rel(X) <= np.maximum(2.0 * spread, 1e-6)).all(), (rel(X), spread)
