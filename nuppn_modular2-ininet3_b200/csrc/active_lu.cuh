@@ -49,6 +49,7 @@ struct Act {
   float *gcoef;      // [ngi] term coefficient (-k2, -1, k6 or k8)
   uint32_t *grpk;    // [ngi] compact index of reactant 1 | reactant 2 (na = gamma) << 14 | k2 << 28
   double *grcv;      // [ngi] (1/k2!) * rate of the term's reaction
+  double *gterm;     // [ngi] term values of the current sub-step
   bool rhs_in_smem;
 };
 
@@ -624,7 +625,8 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
   A.gptr = (int *)base; base += a16((size_t)(na + 1) * 4);
   A.gcoef = (float *)base; base += a16((size_t)ngi * 4);
   A.grpk = (uint32_t *)base; base += a16((size_t)ngi * 4);
-  A.grcv = (double *)base;
+  A.grcv = (double *)base; base += a16((size_t)ngi * 8);
+  A.gterm = (double *)base;
   A.ngi = ngi;
   for (int c = tid; c <= na; c += nt) A.gptr[c] = (c < na && off[c] < T) ? flag[off[c]] : ngi;
   for (int t = tid; t < T; t += nt) {
@@ -643,16 +645,21 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
   __syncthreads();
 }
 
-// dX/dt of active row c from the compact molar abundances A.xnc: each term's flux is
-// (1/k2!) v xn(k1)^k2 xn(k3) as in calculate_dxdt (jac_rhs.F90:245-252), accumulated in the
-// reference's order and multiplied by A at the end (jac_rhs.F90:266-270).
+// Term q of the right-hand side from the compact molar abundances A.xnc: coefficient times the
+// reaction's flux (1/k2!) v xn(k1)^k2 xn(k3), as in calculate_dxdt (jac_rhs.F90:245-252).
+__device__ __forceinline__ double rhs_term(const Act &A, int q) {
+  const uint32_t pk = A.grpk[q];
+  const double flux = A.grcv[q] * powi(A.xnc[pk & 0x3fff], (int)(pk >> 28)) * A.xnc[(pk >> 14) & 0x3fff];
+  return (double)A.gcoef[q] * flux;
+}
+
+// dX/dt of active row c from the terms in A.gterm, accumulated in the reference's order and
+// multiplied by A at the end (jac_rhs.F90:266-270).
 __device__ __forceinline__ double gather_dxdt(const Act &A, int c) {
   double acc = 0.0;
-  for (int q = A.gptr[c]; q < A.gptr[c + 1]; ++q) {
-    const uint32_t pk = A.grpk[q];
-    const double flux = A.grcv[q] * powi(A.xnc[pk & 0x3fff], (int)(pk >> 28)) * A.xnc[(pk >> 14) & 0x3fff];
-    acc = acc + (double)A.gcoef[q] * flux;
-  }
+  const int q1 = A.gptr[c + 1];
+#pragma unroll 4
+  for (int q = A.gptr[c]; q < q1; ++q) acc = acc + A.gterm[q];
   return acc * A.anc[c];
 }
 
@@ -660,6 +667,8 @@ __device__ __forceinline__ double gather_dxdt(const Act &A, int c) {
 __device__ void dev_dxdt_active(const Act &A, const double *yc, double *dxc) {
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int c = tid; c < A.na; c += nt) A.xnc[c] = yc[c] / A.anc[c];
+  __syncthreads();
+  for (int q = tid; q < A.ngi; q += nt) A.gterm[q] = rhs_term(A, q);
   __syncthreads();
   for (int c = tid; c < A.na; c += nt) dxc[c] = gather_dxdt(A, c);
   __syncthreads();

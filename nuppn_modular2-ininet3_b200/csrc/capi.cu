@@ -67,7 +67,7 @@ struct nuppn_net {
   DevBuf ws, stage, counter;
   int ws_slots = 0;
   int block = 256;
-  int act_smem = 72 * 1024;  // shared-memory budget per CTA for the active subsystem (3 CTAs per SM)
+  int act_smem = 64 * 1024;  // shared-memory budget per CTA for the active subsystem (2 CTAs per SM)
   int device = 0;
   int nsm = 0;
   int64_t launches = 0;

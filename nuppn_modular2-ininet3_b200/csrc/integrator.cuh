@@ -189,10 +189,12 @@ __device__ void bd_level_tile_warp(const Act &A, const BdVec &B, double h, int n
   int err = 0, ns = 0;
   for (int j = 0; j <= nseq; ++j) {
     const int stage = j == 0 ? 1 : (j < nseq ? 2 : 3);  // FIRST, MID, LAST
-    __syncwarp();  // every lane has finished reading xnc of the previous sub-step
+    __syncwarp();  // every lane has finished reading xnc and gterm of the previous sub-step
 #pragma unroll
     for (int i = 0; i < R; ++i)
       if (lane + 32 * i < na) A.xnc[lane + 32 * i] = y[i] / an[i];
+    __syncwarp();
+    for (int q = lane; q < A.ngi; q += 32) A.gterm[q] = rhs_term(A, q);
     __syncwarp();
     double x[R];
 #pragma unroll

@@ -140,9 +140,9 @@ NUPPN_HD inline size_t act_bytes_max(int nsys, int nnz, int nwarps) {
 }
 
 // Bytes of the restricted right-hand side for na rows and ngi gather items:
-// int gptr[na+1]; float gcoef[ngi]; uint32 grpk[ngi]; double grcv[ngi].
+// int gptr[na+1]; float gcoef[ngi]; uint32 grpk[ngi]; double grcv[ngi], gterm[ngi].
 NUPPN_HD inline size_t rhs_bytes(int na, int ngi) {
-  return a16((size_t)(na + 1) * 4) + 2 * a16((size_t)ngi * 4) + a16((size_t)ngi * 8);
+  return a16((size_t)(na + 1) * 4) + 2 * a16((size_t)ngi * 4) + 2 * a16((size_t)ngi * 8);
 }
 
 // arguments of the persistent integration kernel
