@@ -295,9 +295,10 @@ nuppn_status nuppn_net_create(const nuppn_net_desc *desc, const nuppn_knobs *kno
   net->nsm = prop.multiProcessorCount;
   net->block = kn.threads_per_zone > 0 ? kn.threads_per_zone : 256;
   if (net->block % 32 || net->block > 256) { delete net; set_error("threads_per_zone must be a multiple of 32, <= 256"); return NUPPN_ERR_ARG; }
-  if (kn.lu_precision != 0) {
+  if (kn.lu_precision != 0 || kn.i_nse != 0) {
     delete net;
-    set_error("lu_precision: only 0 (FP64 factorization) is available in this build");
+    set_error(kn.lu_precision != 0 ? "lu_precision: only 0 (FP64 factorization) is available in this build"
+                                    : "i_nse: NSE switching is not available in this build");
     return NUPPN_ERR_ARG;
   }
   nuppn_status st = upload(net);
@@ -337,6 +338,10 @@ nuppn_status nuppn_net_info_get(const nuppn_net *net, nuppn_net_info *info) {
 
 nuppn_status nuppn_set_knobs(nuppn_net *net, const nuppn_knobs *knobs) {
   if (!net || !knobs) return NUPPN_ERR_ARG;
+  if (knobs->lu_precision != 0 || knobs->i_nse != 0) {
+    set_error("lu_precision 1 and i_nse 1 are not available in this build");
+    return NUPPN_ERR_ARG;
+  }
   double old_dgrd = net->H.kn.dgrd;
   net->H.kn = *knobs;
   if (knobs->dgrd != old_dgrd) bd_constants(net->H);
