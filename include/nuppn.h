@@ -242,6 +242,29 @@ nuppn_status nuppn_integrate_device(nuppn_net *net, int32_t nz, double *d_X, int
                                     int32_t *d_ierr, nuppn_zone_stats *d_stats, int32_t *d_bd_state,
                                     void *stream);
 
+/* Same as nuppn_integrate_device, but this call allocates no device memory. It has no counterpart
+ * in the reference (whose solver allocates through SuperLU on every call); it is for callers that
+ * cannot call cudaMalloc while they step: programs that hand all of the GPU's memory to their own
+ * allocator at start-up, or that keep cudaMalloc/cudaFree (which can synchronize the whole device)
+ * out of their time-step loop. The handle itself is still made by nuppn_net_create at set-up.
+ *
+ * The per-CTA workspace and the zone counter live in one static device array of
+ * NUPPN_NOALLOC_SCRATCH_BYTES (64 MiB), held on every GPU the library is used on until the process
+ * exits. The call runs as many CTAs as whole workspace slabs fit in it (nuppn_net_info_get's
+ * device_bytes does not count it); if one slab of this network does not fit it returns
+ * NUPPN_ERR_LIMIT. The zone counter is cleared on the stream before each launch; the rest of the
+ * array keeps the previous call's contents, which the kernel never reads before writing. Every call
+ * on a device shares the array, so calls whose kernels overlap on the GPU (other streams, other
+ * handles, other host threads) race: order them on one stream or synchronize between them.
+ * The first call on a device looks up the array's address on that device (which may load the
+ * library's device code); make that first call before any stream capture. */
+#define NUPPN_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
+nuppn_status nuppn_integrate_device_noalloc(nuppn_net *net, int32_t nz, double *d_X, int32_t ldx,
+                                            const double *d_t9_0, const double *d_t9_1,
+                                            const double *d_rho_0, const double *d_rho_1, double *d_ye,
+                                            const double *d_dtwant, int32_t *d_ierr,
+                                            nuppn_zone_stats *d_stats, int32_t *d_bd_state, void *stream);
+
 /* Number of kernel launches issued by the library since the handle was created. */
 int64_t nuppn_launch_count(const nuppn_net *net);
 

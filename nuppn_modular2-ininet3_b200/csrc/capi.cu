@@ -233,6 +233,34 @@ struct Stager {
 
 }  // namespace
 
+// ---- scratch for nuppn_integrate_device_noalloc -------------------------------------------------
+// One fixed device array holds that entry point's zone counter (first 256 bytes) and its per-CTA
+// workspace slabs, so the call needs no cudaMalloc. In host code the name g_noalloc_scratch is
+// only a host-side stand-in for the symbol: kernels get the address cudaGetSymbolAddress returns,
+// looked up once per device with that device current.
+static __device__ __align__(256) char g_noalloc_scratch[NUPPN_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr size_t kNoAllocCounterBytes = 256;
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[kMaxDevices] = {};
+
+// Device address of the scratch array on `device` (which must be current).
+cudaError_t noalloc_scratch(int device, void **out) {
+  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_addr[device] = p;
+  }
+  *out = g_noalloc_addr[device];
+  return cudaSuccess;
+}
+}  // namespace
+
 extern "C" {
 
 int32_t nuppn_abi_version(void) { return NUPPN_ABI_VERSION; }
@@ -363,6 +391,41 @@ nuppn_status nuppn_jac_pattern(const nuppn_net *net, int32_t *row, int32_t *col,
 }
 
 int64_t nuppn_launch_count(const nuppn_net *net) { return net ? net->launches : 0; }
+
+nuppn_status nuppn_integrate_device_noalloc(nuppn_net *net, int32_t nz, double *d_X, int32_t ldx,
+                                            const double *d_t9_0, const double *d_t9_1, const double *d_rho_0,
+                                            const double *d_rho_1, double *d_ye, const double *d_dtwant,
+                                            int32_t *d_ierr, nuppn_zone_stats *d_stats, int32_t *d_bd_state,
+                                            void *stream) {
+  nuppn_status st = check_zone_args(net, nz, ldx);
+  if (st != NUPPN_OK) return st;
+  if (nz == 0) return NUPPN_OK;
+  if (!d_X || !d_t9_0 || !d_t9_1 || !d_rho_0 || !d_rho_1 || !d_ye || !d_dtwant || !d_ierr) {
+    set_error("null device argument");
+    return NUPPN_ERR_ARG;
+  }
+  const size_t slab = net->L.bytes;
+  if (kNoAllocCounterBytes + slab > (size_t)NUPPN_NOALLOC_SCRATCH_BYTES) {
+    set_error("nuppn_integrate_device_noalloc: this network needs " + std::to_string(slab) +
+              " bytes of workspace per CTA, more than the static scratch of " +
+              std::to_string((size_t)NUPPN_NOALLOC_SCRATCH_BYTES) + " bytes; use nuppn_integrate_device");
+    return NUPPN_ERR_LIMIT;
+  }
+  CK(cudaSetDevice(net->device));
+  void *base = nullptr;
+  CK(noalloc_scratch(net->device, &base));
+  const int slabs = (int)(((size_t)NUPPN_NOALLOC_SCRATCH_BYTES - kNoAllocCounterBytes) / slab);
+  const int grid = std::min(std::min(nz, resident_slots(net)), slabs);
+  cudaStream_t s = (cudaStream_t)stream;
+  CK(cudaMemsetAsync(base, 0, sizeof(int), s));  // the zone counter starts at zero every call
+  IntegrateArgs A;
+  A.nz = nz; A.ldx = ldx; A.X = d_X; A.t9_0 = d_t9_0; A.t9_1 = d_t9_1; A.rho_0 = d_rho_0; A.rho_1 = d_rho_1;
+  A.dtwant = d_dtwant; A.ye = d_ye; A.ierr = d_ierr; A.stats = d_stats; A.bd_state = d_bd_state;
+  A.counter = (int *)base;
+  CK(launch_integrate(net->D, net->L, (char *)base + kNoAllocCounterBytes, grid, net->block, net->act_smem, A, s));
+  net->launches++;
+  return NUPPN_OK;
+}
 
 // ---- phase entry points (host buffers) ----------------------------------------------------------
 static nuppn_status run_phase(nuppn_net *net, int nz, int op, const double *X, int ldx, const double *t9,
