@@ -43,6 +43,10 @@ struct Act {
   double *T, *rinv;  // tile: T[c*tile_rows + r] = entry (r, c) of L\U; rinv[r] = 1 / U(r, r)
   int genF, genS;
   bool in_smem;
+  // reactions of the step (see dev_active_reactions), in the CTA's workspace
+  int nK, nP;
+  int *Klist;        // [nK] kept: first reactant masked, second masked or gamma
+  int *Plist;        // [nP] passing the rate test of dev_jacobian_mask (a subset of the kept)
   // right-hand side restricted to the dynamic network (see dev_compact_rhs)
   int ngi;
   int *gptr;         // [na+1] gather items of active row c: gptr[c] .. gptr[c+1]-1
@@ -233,15 +237,64 @@ __device__ __forceinline__ double jac_contrib(const DevNet &N, const Ws &W, int 
   return d;
 }
 
-// Jacobian values (1e-99 + the reaction contributions, every reaction as in the reference) and entry
-// flags for the positions of the active subsystem. The contributions of all active entries are
-// evaluated as one flattened, block-parallel list; each entry is then summed by a warp.
+// Reactions of the step, found through the active species' lists of the reactions they lead (k1):
+// every considered reaction whose first reactant is masked, in one flattened pass. K (kept) = those
+// whose second reactant is masked or gamma, the terms of the restricted right-hand side. P (passing)
+// = those that passed the rate test of dev_jacobian_mask, the only reactions that contribute to the
+// Jacobian (jac_rhs.F90:350-392); a passing reaction masks all its participants, so P is part of K.
+// Both lists are in flattened order (active row, then reaction index).
+__device__ void dev_active_reactions(const DevNet &N, const Ws &W, Act &A, int *sint) {
+  const int tid = threadIdx.x, nt = blockDim.x, na = A.na, g = N.ig;
+  int *off = W.rx;                  // [na+1]
+  int *ra = off + (N.nsys + 1);     // [T] reaction of each flattened position
+  int *kf = ra + (N.nact + 1);      // [T+1] kept flags, then their positions
+  int *pf = kf + (N.nact + 1);      // [T+1] passing flags, then their positions
+  A.Klist = pf + (N.nact + 1);
+  A.Plist = A.Klist + (N.nact + 1);
+  for (int c = tid; c < na; c += nt) {
+    const int s = N.sp_of_sys[A.arow[c]];
+    off[c] = N.k1_ptr[s + 1] - N.k1_ptr[s];
+  }
+  __syncthreads();
+  const int T = block_scan_excl(off, na, sint);
+  if (tid == 0) off[na] = T;
+  __syncthreads();
+  for (int t = tid; t < T; t += nt) {
+    const int c = seg_of(off, na, t);
+    const int a = N.k1_list[N.k1_ptr[N.sp_of_sys[A.arow[c]]] + (t - off[c])];
+    const int k3 = N.act_k[(size_t)a * 8 + 2];
+    ra[t] = a;
+    kf[t] = (k3 == g || W.mask[k3]) ? 1 : 0;
+    pf[t] = W.flux[a] != 0.0 ? 1 : 0;
+  }
+  __syncthreads();
+  const int nK = block_scan_excl(kf, T, sint);
+  const int nP = block_scan_excl(pf, T, sint);
+  if (tid == 0) {
+    kf[T] = nK;
+    pf[T] = nP;
+  }
+  __syncthreads();
+  for (int t = tid; t < T; t += nt) {
+    if (kf[t + 1] > kf[t]) A.Klist[kf[t]] = ra[t];
+    if (pf[t + 1] > pf[t]) A.Plist[pf[t]] = ra[t];
+  }
+  A.nK = nK;
+  A.nP = nP;
+  __syncthreads();
+}
+
+// Jacobian values (1e-99 + the contributions of every passing reaction, as in the reference) and
+// entry flags for the positions of the active subsystem. Entries with a short static gather list
+// evaluate it as one flattened, block-parallel list; the few entries with long lists (among n, p
+// and alpha) take their contributions from the passing reactions P. Each entry is summed by a warp.
 __device__ void dev_jacobian_active(const DevNet &N, const Ws &W, Act &A, int *sint) {
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
   int *off = W.act_otmp;  // [nnz+1] <= nnzLU + 1
   for (int p = tid; p < A.nnz; p += nt) {
     const int e = N.lu_src[A.csrc[p]];
-    off[p] = e >= 0 ? N.jg_ptr[e + 1] - N.jg_ptr[e] : 0;
+    const int len = e >= 0 ? N.jg_ptr[e + 1] - N.jg_ptr[e] : 0;
+    off[p] = len <= kLongList ? len : 0;
   }
   __syncthreads();
   const int T = block_scan_excl(off, A.nnz, sint);
@@ -269,9 +322,20 @@ __device__ void dev_jacobian_active(const DevNet &N, const Ws &W, Act &A, int *s
     }
     double acc = 0.0;
     int set = 0;
-    for (int t = off[p] + lane; t < off[p + 1]; t += 32) {
-      acc += dv[t];
-      set |= sf[t];
+    if (N.jg_ptr[e + 1] - N.jg_ptr[e] <= kLongList) {
+      for (int t = off[p] + lane; t < off[p + 1]; t += 32) {
+        acc += dv[t];
+        set |= sf[t];
+      }
+    } else {
+      for (int i = lane; i < A.nP * 8; i += 32) {
+        const int a = A.Plist[i >> 3], s = i & 7;
+        if (N.act_ice[(size_t)a * 8 + s] == e) {
+          bool st;
+          acc += jac_contrib(N, W, a, s, st);
+          set |= st ? 1 : 0;
+        }
+      }
     }
     for (int o = 16; o > 0; o >>= 1) {
       acc += __shfl_xor_sync(NUPPN_FULL, acc, o);
@@ -580,39 +644,69 @@ __device__ bool dev_solve_species(const DevNet &N, Act &A, const double *rhs, do
 }
 
 // ---------------------------------------------------------------------------------------------
-// Right-hand side restricted to the dynamic network (after dev_compact).
+// Right-hand side restricted to the dynamic network (after dev_compact and dev_active_reactions).
 //
 // Within one step only dX/dt of masked species is used (the rest of the correction is zero, as in
 // ddecompac, jac_rhs.F90:584-608) and unmasked abundances stay frozen. A reaction with an unmasked
 // reactant did not pass the dynamic-network test itself (jac_rhs.F90:350-353: otherwise all its
 // participants would be masked), so its flux is at most y * cyminformal / dt for the frozen
 // reactant's abundance y, and it changes X by at most ~1e-30 over the step; such reactions are left
-// out. Each masked species keeps, in the reference's accumulation order (reaction order, then k1,
-// k3, k5, k7), one gather item per term of a kept reaction: the term's coefficient, the reaction's
-// (1/k2!) * rate and the compact indices of its reactants. A sub-step recomputes each term's flux
-// from those with the reference's operations, so no per-reaction pass or flux array is needed.
+// out. Each masked species keeps one gather item per term of a kept reaction: the term's coefficient
+// (-k2, -1, k6 or k8 for its slot k1, k3, k5, k7), the reaction's (1/k2!) * rate and the compact
+// indices of its reactants. Species with a short static list keep the reference's accumulation
+// order (reaction order, then slot); the few with long lists (n, p, alpha) take their terms from the
+// kept reactions K, in K's order. A sub-step recomputes each term's flux from the item.
+__device__ __forceinline__ void put_rhs_item(const DevNet &N, const Ws &W, Act &A, const int *sys2c, int q, int a,
+                                             int m) {
+  const int *k = N.act_k + (size_t)a * 8;
+  const uint32_t i1 = (uint32_t)sys2c[N.sys_of_sp[k[0]]];
+  const uint32_t i2 = k[2] == N.ig ? (uint32_t)A.na : (uint32_t)sys2c[N.sys_of_sp[k[2]]];
+  A.gcoef[q] = (float)(m == 0 ? -k[1] : m == 1 ? -1 : m == 2 ? k[5] : k[7]);  // small integers, exact
+  A.grcv[q] = c_fact[k[1]] * W.v[N.act_slot[a]];
+  A.grpk[q] = i1 | (i2 << 14) | ((uint32_t)k[1] << 28);
+}
+
 __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem, size_t smem_bytes, int *sint) {
-  const int tid = threadIdx.x, nt = blockDim.x, nw = nt >> 5;
-  int *off = W.act_tmp + 3 * (N.nsys + 1);  // [na+1] segment offsets of the static species lists
-  int *flag = W.act_itmp;                   // [T] kept flags -> positions
-  const int *sys2c = W.act_tmp;             // system index -> active row (dev_compact), -1 if frozen
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
+  const int *sys2c = W.act_tmp;              // system index -> active row (dev_compact), -1 if frozen
+  int *cnt = W.act_tmp + 2 * (N.nsys + 1);   // [na+1] items per row, then row offsets
+  int *off = W.act_tmp + 3 * (N.nsys + 1);   // [na+1] offsets of the short rows' static lists
+  int *flag = W.act_itmp;                    // [T+1] kept flags, then positions
   const int g = N.ig, na = A.na;
   for (int c = tid; c < na; c += nt) {
     const int s = N.sp_of_sys[A.arow[c]];
-    off[c] = N.dg_ptr[s + 1] - N.dg_ptr[s];
+    const int len = N.dg_ptr[s + 1] - N.dg_ptr[s];
+    off[c] = len <= kLongList ? len : 0;
   }
   __syncthreads();
   const int T = block_scan_excl(off, na, sint);
   if (tid == 0) off[na] = T;
   __syncthreads();
-  for (int t = tid; t < T; t += nt) {  // flattened static lists of the masked species
+  for (int t = tid; t < T; t += nt) {  // flattened static lists of the short rows
     const int c = seg_of(off, na, t);
     const int a = N.dg_item[N.dg_ptr[N.sp_of_sys[A.arow[c]]] + (t - off[c])] >> 2;
     const int *k = N.act_k + (size_t)a * 8;
     flag[t] = (W.mask[k[0]] && (k[2] == g || W.mask[k[2]])) ? 1 : 0;
   }
   __syncthreads();
-  const int ngi = block_scan_excl(flag, T, sint);
+  const int nS = block_scan_excl(flag, T, sint);
+  if (tid == 0) flag[T] = nS;
+  __syncthreads();
+  for (int c = tid; c < na; c += nt) cnt[c] = flag[off[c + 1]] - flag[off[c]];  // 0 for long rows
+  __syncthreads();
+  for (int c = w; c < na; c += nw) {  // long rows: count their slots among the kept reactions
+    const int s = N.sp_of_sys[A.arow[c]];
+    if (N.dg_ptr[s + 1] - N.dg_ptr[s] <= kLongList) continue;
+    int n = 0;
+    for (int i = lane; i < A.nK; i += 32) {
+      const int *k = N.act_k + (size_t)A.Klist[i] * 8;
+      n += (k[0] == s) + (k[2] == s) + (k[4] == s) + (k[6] == s);
+    }
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(NUPPN_FULL, n, o);
+    if (lane == 0) cnt[c] = n;
+  }
+  __syncthreads();
+  const int ngi = block_scan_excl(cnt, na, sint);
   const size_t lu_need = act_bytes(na, A.nnz, nw, A.tile_rows), need = rhs_bytes(na, ngi);
   char *base;
   if (A.in_smem && lu_need + need <= smem_bytes) {
@@ -628,19 +722,32 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
   A.grcv = (double *)base; base += a16((size_t)ngi * 8);
   A.gterm = (double *)base;
   A.ngi = ngi;
-  for (int c = tid; c <= na; c += nt) A.gptr[c] = (c < na && off[c] < T) ? flag[off[c]] : ngi;
+  for (int c = tid; c <= na; c += nt) A.gptr[c] = c < na ? cnt[c] : ngi;
   for (int t = tid; t < T; t += nt) {
+    if (flag[t + 1] == flag[t]) continue;
     const int c = seg_of(off, na, t);
-    const int p = N.dg_ptr[N.sp_of_sys[A.arow[c]]] + (t - off[c]);
-    const int a = N.dg_item[p] >> 2;
-    const int *k = N.act_k + (size_t)a * 8;
-    if (!(W.mask[k[0]] && (k[2] == g || W.mask[k[2]]))) continue;
-    const int q = flag[t];
-    const uint32_t i1 = (uint32_t)sys2c[N.sys_of_sp[k[0]]];
-    const uint32_t i2 = k[2] == g ? (uint32_t)na : (uint32_t)sys2c[N.sys_of_sp[k[2]]];
-    A.gcoef[q] = (float)N.dg_coef[p];  // -k2, -1, k6 or k8: small integers, exact in float
-    A.grcv[q] = c_fact[k[1]] * W.v[N.act_slot[a]];
-    A.grpk[q] = i1 | (i2 << 14) | ((uint32_t)k[1] << 28);
+    const int it = N.dg_item[N.dg_ptr[N.sp_of_sys[A.arow[c]]] + (t - off[c])];
+    put_rhs_item(N, W, A, sys2c, cnt[c] + flag[t] - flag[off[c]], it >> 2, it & 3);
+  }
+  for (int c = w; c < na; c += nw) {  // long rows: their terms in the order of K, then slot
+    const int s = N.sp_of_sys[A.arow[c]];
+    if (N.dg_ptr[s + 1] - N.dg_ptr[s] <= kLongList) continue;
+    int base_q = cnt[c];
+    for (int i0 = 0; i0 < A.nK; i0 += 32) {
+      const int i = i0 + lane;
+      const int a = i < A.nK ? A.Klist[i] : -1;
+      const int *k = N.act_k + (size_t)(a < 0 ? 0 : a) * 8;
+      const int n = a < 0 ? 0 : (k[0] == s) + (k[2] == s) + (k[4] == s) + (k[6] == s);
+      int incl = n;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(NUPPN_FULL, incl, o);
+        if (lane >= o) incl += v;
+      }
+      int q = base_q + incl - n;
+      for (int m = 0; m < 4 && n > 0; ++m)
+        if (k[2 * m] == s) put_rhs_item(N, W, A, sys2c, q++, a, m);
+      base_q += __shfl_sync(NUPPN_FULL, incl, 31);
+    }
   }
   __syncthreads();
 }

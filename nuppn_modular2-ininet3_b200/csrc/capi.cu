@@ -67,7 +67,7 @@ struct nuppn_net {
   DevBuf ws, stage, counter;
   int ws_slots = 0;
   int block = 256;
-  int act_smem = 64 * 1024;  // shared-memory budget per CTA for the active subsystem (2 CTAs per SM)
+  int act_smem = 72 * 1024;  // shared-memory budget per CTA for the active subsystem (3 CTAs per SM)
   int device = 0;
   int nsm = 0;
   int64_t launches = 0;
@@ -118,6 +118,7 @@ nuppn_status upload(nuppn_net *net) {
   P(H.jg_long); P(H.dg_long);
   P(H.sys_of_sp); P(H.sp_of_sys); P(H.pos_of_entry); P(H.lu_src); P(H.lu_rowptr); P(H.lu_diag); P(H.lu_col); P(H.upd_start);
   P(H.upd_off); P(H.lvL_ptr); P(H.lvL_rows); P(H.lvL_grp); P(H.lvU_ptr); P(H.lvU_rows); P(H.lvU_grp);
+  P(H.k1_ptr); P(H.k1_list);
   CK(cudaMalloc(&net->arena, A.total));
   net->arena_bytes = A.total;
   std::vector<char> host(A.total, 0);
@@ -153,6 +154,7 @@ nuppn_status upload(nuppn_net *net) {
   D.upd_start = (const int *)nx(); D.upd_off = (const uint16_t *)nx();
   D.lvL_ptr = (const int *)nx(); D.lvL_rows = (const int *)nx(); D.lvL_grp = (const int *)nx();
   D.lvU_ptr = (const int *)nx(); D.lvU_rows = (const int *)nx(); D.lvU_grp = (const int *)nx();
+  D.k1_ptr = (const int *)nx(); D.k1_list = (const int *)nx();
   // scalars
   D.nsp = H.nsp; D.nre = H.nre; D.nact = H.nact; D.ig = H.ig; D.nsys = H.nsys; D.nnzJ = H.nnzJ; D.nnzLU = H.nnzLU;
   D.ihe4 = H.ihe4; D.ibe8 = H.ibe8;
@@ -196,6 +198,7 @@ WsLayout layout(const HostNet &H) {
     L.act_btmp = take(njg);
     L.bd = take((size_t)(2 * kMaxLevels + 8) * H.nsys * sizeof(double));
   }
+  L.rx = take(((size_t)H.nsys + 1 + 5 * ((size_t)H.nact + 1)) * sizeof(int));
   L.bytes = t;
   return L;
 }

@@ -301,6 +301,15 @@ std::string build_host_net(const nuppn_net_desc &d, const nuppn_knobs &kn, HostN
       H.act_k[(size_t)a * 8 + s] = k[s];
     }
   }
+  // ---- reactions by their first reactant (every considered reaction once; k1 is never gamma)
+  H.k1_ptr.assign(nsp + 1, 0);
+  for (int a = 0; a < H.nact; ++a) H.k1_ptr[H.act_k[(size_t)a * 8] + 1]++;
+  for (int i = 0; i < nsp; ++i) H.k1_ptr[i + 1] += H.k1_ptr[i];
+  H.k1_list.assign(H.nact, 0);
+  {
+    std::vector<int> fill(H.k1_ptr.begin(), H.k1_ptr.end() - 1);
+    for (int a = 0; a < H.nact; ++a) H.k1_list[fill[H.act_k[(size_t)a * 8]]++] = a;
+  }
   // ---- gather lists in the reference's accumulation order
   {
     std::vector<std::vector<int>> lists(H.nnzJ);

@@ -47,6 +47,7 @@ struct HostNet {
   // pattern
   std::vector<int> jrow, jcol, jdiag, dmap_all;  // dmap_all[nre*8] (-1 for unconsidered)
   std::vector<int> jg_ptr, jg_item, dg_ptr, dg_item, jg_long, dg_long;
+  std::vector<int> k1_ptr, k1_list;  // species -> considered reactions it leads as k1, in order
   std::vector<double> dg_coef;
   // system / LU
   std::vector<int> sys_of_sp, sp_of_sys, pos_of_entry, lu_src;

@@ -67,6 +67,7 @@ struct DevNet {
   const double *dg_coef;                   // coefficient of each dg item: -k2, -1, k6, k8
   int njg_long, ndg_long;
   const int *jg_long, *dg_long;            // entries / species whose gather lists are long
+  const int *k1_ptr, *k1_list;             // species -> considered reactions it leads (k1), in order
   // system and LU
   const int *sys_of_sp, *sp_of_sys;        // [nsp], [nsys]
   const int *pos_of_entry;                 // [nnzJ] LU position or -1
@@ -94,6 +95,7 @@ struct WsLayout {
   size_t act_tmp, act;           // compaction scratch (ints) and the global fallback of the active LU
   size_t act_r;                  // global fall-back of the restricted right-hand side
   size_t act_itmp, act_otmp, act_dtmp, act_btmp, bd;  // flattened-gather scratch, compact BD vectors
+  size_t rx;                     // active-reaction lists: offsets, flags, kept and passing reactions
   size_t bytes;
 };
 

@@ -556,7 +556,7 @@ namespace nuppn {
 // ---------------------------------------------------------------------------------------------
 // kernels: persistent CTAs, one zone at a time, workspace slab per CTA; dynamic shared memory holds
 // the active-subsystem LU when it fits (act_smem bytes).
-__global__ void __launch_bounds__(256, 2) k_integrate(const __grid_constant__ DevNet N, const __grid_constant__ WsLayout L,
+__global__ void __launch_bounds__(256, 3) k_integrate(const __grid_constant__ DevNet N, const __grid_constant__ WsLayout L,
                                                    char *ws, const __grid_constant__ IntegrateArgs A, int act_smem) {
   extern __shared__ __align__(16) char smem_dyn[];
   __shared__ double sred[32];

@@ -28,6 +28,7 @@ struct Ws {
   int *act_tmp;  // compaction scratch: sys2c, arow, counts
   char *act;     // global fallback of the active-subsystem LU
   char *act_r;   // global fallback of the restricted right-hand side
+  int *rx;       // active-reaction lists [nsys+1 + 5*(nact+1)]
   int *act_itmp; // flattened-list flags / positions [max(list items) + 1]
   int *act_otmp; // segment offsets of the active Jacobian entries [nnzLU + 1]
   double *act_dtmp;   // flattened Jacobian contributions [jg items]
@@ -52,6 +53,7 @@ __device__ __forceinline__ Ws ws_bind(char *base, const WsLayout &L) {
   w.act_tmp = (int *)(base + L.act_tmp);
   w.act = base + L.act;
   w.act_r = base + L.act_r;
+  w.rx = (int *)(base + L.rx);
   w.act_itmp = (int *)(base + L.act_itmp);
   w.act_otmp = (int *)(base + L.act_otmp);
   w.act_dtmp = (double *)(base + L.act_dtmp);
