@@ -387,18 +387,22 @@ __device__ __forceinline__ double assemble_entry(Act &A, int p, double h) {
 
 __device__ __forceinline__ bool pivot_ok(double d) { return d != 0.0 && isfinite(d); }
 
-// Right-looking elimination of a dense tile by one warp; lane l owns rows l + 32 i (i < R), so the
-// updates of one pivot step are independent across lanes. The L column is scaled by the reciprocal
-// of the pivot, as SuperLU does (dpivotL.c:178-180). Returns false on a zero or non-finite pivot.
+// Right-looking elimination of a dense tile by all warps of the CTA. At pivot k every warp forms
+// the multipliers l_r = a_rk / a_kk of the rows below in registers (lane l owns rows l + 32 i) and
+// updates its share of the trailing columns (m = k+1+w, step nw); one barrier per pivot. Column k is
+// left unscaled during the elimination and scaled at the end by the stored reciprocal, the same
+// product a_rk * (1 / a_kk) that SuperLU forms (dpivotL.c:178-180). Returns false on a zero or
+// non-finite pivot.
 template <int R>
-__device__ bool tile_factor_warp(double *T, double *rinv, int na, int lane) {
+__device__ bool tile_factor_block(double *T, double *rinv, int na) {
   constexpr int S = 32 * R;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   int bad = 0;
   for (int k = 0; k < na; ++k) {
     const double piv = T[k * (S + 1)];
     bad |= !pivot_ok(piv);
     const double rp = 1.0 / piv;
-    if (lane == 0) rinv[k] = rp;
+    if (threadIdx.x == 0) rinv[k] = rp;
     double l[R];
     bool any = false;
 #pragma unroll
@@ -406,36 +410,81 @@ __device__ bool tile_factor_warp(double *T, double *rinv, int na, int lane) {
       const int r = lane + 32 * i;
       l[i] = 0.0;
       if (r > k && r < na) {
-        double a = T[k * S + r];
-        if (a != 0.0) {
-          a = a * rp;
-          T[k * S + r] = a;
-        }
-        l[i] = a;
+        const double a = T[k * S + r];
+        l[i] = a != 0.0 ? a * rp : 0.0;
       }
       any |= l[i] != 0.0;
     }
-    if (any)
-      for (int m = k + 1; m < na; ++m) {
+    if (__any_sync(NUPPN_FULL, any)) {
+#pragma unroll 2
+      for (int m = k + 1 + w; m < na; m += nw) {
         const double u = T[m * S + k];
 #pragma unroll
         for (int i = 0; i < R; ++i)
           if (l[i] != 0.0) T[m * S + lane + 32 * i] -= l[i] * u;
       }
-    __syncwarp();
+    }
+    __syncthreads();
   }
-  return bad == 0;
+  for (int i = threadIdx.x; i < na * S; i += blockDim.x) {  // L columns: a_rk * (1 / a_kk)
+    const int c = i / S, r = i - c * S;
+    if (r > c && r < na) {
+      const double a = T[i];
+      if (a != 0.0) T[i] = a * rinv[c];
+    }
+  }
+  return __syncthreads_or(bad) == 0;
 }
 
-// Forward and backward substitution of a factored tile by one warp, x[i] holding row lane + 32 i:
-// per column one broadcast and one fused multiply-add per row. Column-oriented like SuperLU's
-// dgstrs; the diagonal is applied as the reciprocal computed by the factorization.
+// Forward and backward substitution of a factored tile by one warp, x[i] holding row lane + 32 i.
+// Columns go in blocks of four: every lane forms the block's four final values from four broadcasts
+// (the small triangle solved redundantly), then applies the four columns to its rows. Each row
+// sees exactly the operations of the column-by-column order (column-oriented, like SuperLU's
+// dgstrs); the diagonal is applied as the reciprocal computed by the factorization.
 template <int R>
-__device__ __forceinline__ void tile_solve_regs(const double *T, int na, double (&x)[R], const double (&ri)[R],
-                                                int lane) {
+__device__ __forceinline__ double tile_row(const double (&x)[R], int r) {
+  return (R == 1 || r < 32) ? x[0] : x[R - 1];
+}
+
+template <int R>
+__device__ __forceinline__ void tile_solve_regs(const double *T, const double *rinv, int na, double (&x)[R],
+                                                const double (&ri)[R], int lane) {
   constexpr int S = 32 * R;
-  for (int c = 0; c < na - 1; ++c) {
-    const double xc = __shfl_sync(NUPPN_FULL, (R == 1 || c < 32) ? x[0] : x[R - 1], c & 31);
+  int c = 0;
+  for (; c + 4 < na; c += 4) {  // forward, columns c .. c+3 (the last column has no entries below)
+    const double u0 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
+    const double u1 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c + 1), (c + 1) & 31);
+    const double u2 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c + 2), (c + 2) & 31);
+    const double u3 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c + 3), (c + 3) & 31);
+    const double l10 = T[c * S + c + 1], l20 = T[c * S + c + 2], l30 = T[c * S + c + 3];
+    const double l21 = T[(c + 1) * S + c + 2], l31 = T[(c + 1) * S + c + 3], l32 = T[(c + 2) * S + c + 3];
+    const double v0 = u0;
+    double v1 = u1;
+    if (l10 != 0.0) v1 -= l10 * v0;
+    double v2 = u2;
+    if (l20 != 0.0) v2 -= l20 * v0;
+    if (l21 != 0.0) v2 -= l21 * v1;
+    double v3 = u3;
+    if (l30 != 0.0) v3 -= l30 * v0;
+    if (l31 != 0.0) v3 -= l31 * v1;
+    if (l32 != 0.0) v3 -= l32 * v2;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int r = lane + 32 * i;
+      if (r == c + 1) x[i] = v1;
+      else if (r == c + 2) x[i] = v2;
+      else if (r == c + 3) x[i] = v3;
+      else if (r > c + 3) {
+        const double a0 = T[c * S + r], a1 = T[(c + 1) * S + r], a2 = T[(c + 2) * S + r], a3 = T[(c + 3) * S + r];
+        if (a0 != 0.0) x[i] -= a0 * v0;
+        if (a1 != 0.0) x[i] -= a1 * v1;
+        if (a2 != 0.0) x[i] -= a2 * v2;
+        if (a3 != 0.0) x[i] -= a3 * v3;
+      }
+    }
+  }
+  for (; c < na - 1; ++c) {
+    const double xc = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       const int r = lane + 32 * i;
@@ -445,11 +494,49 @@ __device__ __forceinline__ void tile_solve_regs(const double *T, int na, double 
       }
     }
   }
-  for (int c = na - 1; c >= 0; --c) {
+  c = na - 1;
+  for (; c >= 3; c -= 4) {  // backward, columns c, c-1, c-2, c-3
+    const double u3 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
+    const double u2 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c - 1), (c - 1) & 31);
+    const double u1 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c - 2), (c - 2) & 31);
+    const double u0 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c - 3), (c - 3) & 31);
+    const double r3 = rinv[c], r2 = rinv[c - 1], r1 = rinv[c - 2], r0 = rinv[c - 3];
+    const double e23 = T[c * S + c - 1], e13 = T[c * S + c - 2], e03 = T[c * S + c - 3];
+    const double e12 = T[(c - 1) * S + c - 2], e02 = T[(c - 1) * S + c - 3], e01 = T[(c - 2) * S + c - 3];
+    const double w3 = u3 * r3;
+    double w2 = u2;
+    if (e23 != 0.0) w2 -= e23 * w3;
+    w2 *= r2;
+    double w1 = u1;
+    if (e13 != 0.0) w1 -= e13 * w3;
+    if (e12 != 0.0) w1 -= e12 * w2;
+    w1 *= r1;
+    double w0 = u0;
+    if (e03 != 0.0) w0 -= e03 * w3;
+    if (e02 != 0.0) w0 -= e02 * w2;
+    if (e01 != 0.0) w0 -= e01 * w1;
+    w0 *= r0;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int r = lane + 32 * i;
+      if (r == c) x[i] = w3;
+      else if (r == c - 1) x[i] = w2;
+      else if (r == c - 2) x[i] = w1;
+      else if (r == c - 3) x[i] = w0;
+      else if (r < c - 3) {
+        const double a3 = T[c * S + r], a2 = T[(c - 1) * S + r], a1 = T[(c - 2) * S + r], a0 = T[(c - 3) * S + r];
+        if (a3 != 0.0) x[i] -= a3 * w3;
+        if (a2 != 0.0) x[i] -= a2 * w2;
+        if (a1 != 0.0) x[i] -= a1 * w1;
+        if (a0 != 0.0) x[i] -= a0 * w0;
+      }
+    }
+  }
+  for (; c >= 0; --c) {
 #pragma unroll
     for (int i = 0; i < R; ++i)
       if (lane + 32 * i == c) x[i] *= ri[i];
-    const double xc = __shfl_sync(NUPPN_FULL, (R == 1 || c < 32) ? x[0] : x[R - 1], c & 31);
+    const double xc = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       const int r = lane + 32 * i;
@@ -471,7 +558,7 @@ __device__ void tile_solve_xs(const Act &A, int lane) {
     x[i] = r < A.na ? A.xs[r] : 0.0;
     ri[i] = r < A.na ? A.rinv[r] : 0.0;
   }
-  tile_solve_regs<R>(A.T, A.na, x, ri, lane);
+  tile_solve_regs<R>(A.T, A.rinv, A.na, x, ri, lane);
 #pragma unroll
   for (int i = 0; i < R; ++i)
     if (lane + 32 * i < A.na) A.xs[lane + 32 * i] = x[i];
@@ -491,9 +578,7 @@ __device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h
     for (int c = w; c < na; c += nw)
       for (int p = A.crp[c] + lane; p < A.crp[c + 1]; p += 32) T[A.ccol[p] * S + c] = assemble_entry(A, p, h);
     __syncthreads();
-    int bad = 0;
-    if (w == 0) bad = !(S == 32 ? tile_factor_warp<1>(T, A.rinv, na, lane) : tile_factor_warp<2>(T, A.rinv, na, lane));
-    return __syncthreads_or(bad) == 0;
+    return S == 32 ? tile_factor_block<1>(T, A.rinv, na) : tile_factor_block<2>(T, A.rinv, na);
   }
   for (int p = tid; p < A.nnz; p += nt) A.cval[p] = assemble_entry(A, p, h);
   __syncthreads();

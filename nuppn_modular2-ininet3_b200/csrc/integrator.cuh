@@ -207,7 +207,7 @@ __device__ void bd_level_tile_warp(const Act &A, const BdVec &B, double h, int n
         x[i] = stage == 1 ? h * dx : h * dx - d[i];
       }
     }
-    tile_solve_regs<R>(A.T, na, x, ri, lane);
+    tile_solve_regs<R>(A.T, A.rinv, na, x, ri, lane);
     ++ns;
     bool huge = false;
 #pragma unroll
