@@ -437,13 +437,19 @@ __device__ bool tile_factor_block(double *T, double *rinv, int na) {
 }
 
 // Forward and backward substitution of a factored tile by one warp, x[i] holding row lane + 32 i.
-// Columns go in blocks of four: every lane forms the block's four final values from four broadcasts
-// (the small triangle solved redundantly), then applies the four columns to its rows. Each row
-// sees exactly the operations of the column-by-column order (column-oriented, like SuperLU's
-// dgstrs); the diagonal is applied as the reciprocal computed by the factorization.
+// Columns go in blocks of four: every lane loads the block's entries of its rows first (they do not
+// depend on x), forms the block's four final values from four broadcasts (the small triangle solved
+// redundantly), then applies the four columns to its rows. Each row sees exactly the operations of
+// the column-by-column order (column-oriented, like SuperLU's dgstrs; a zero entry is skipped); the
+// diagonal is applied as the reciprocal computed by the factorization.
 template <int R>
 __device__ __forceinline__ double tile_row(const double (&x)[R], int r) {
   return (R == 1 || r < 32) ? x[0] : x[R - 1];
+}
+
+__device__ __forceinline__ double sub_nz(double x, double a, double v) {  // x - a*v, skipped for a == 0
+  const double t = x - a * v;
+  return a != 0.0 ? t : x;
 }
 
 template <int R>
@@ -452,99 +458,72 @@ __device__ __forceinline__ void tile_solve_regs(const double *T, const double *r
   constexpr int S = 32 * R;
   int c = 0;
   for (; c + 4 < na; c += 4) {  // forward, columns c .. c+3 (the last column has no entries below)
-    const double u0 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
+    double a[R][4];
+#pragma unroll
+    for (int i = 0; i < R; ++i)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) a[i][k] = T[(c + k) * S + lane + 32 * i];
+    const double l10 = T[c * S + c + 1], l20 = T[c * S + c + 2], l30 = T[c * S + c + 3];
+    const double l21 = T[(c + 1) * S + c + 2], l31 = T[(c + 1) * S + c + 3], l32 = T[(c + 2) * S + c + 3];
+    const double v0 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
     const double u1 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c + 1), (c + 1) & 31);
     const double u2 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c + 2), (c + 2) & 31);
     const double u3 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c + 3), (c + 3) & 31);
-    const double l10 = T[c * S + c + 1], l20 = T[c * S + c + 2], l30 = T[c * S + c + 3];
-    const double l21 = T[(c + 1) * S + c + 2], l31 = T[(c + 1) * S + c + 3], l32 = T[(c + 2) * S + c + 3];
-    const double v0 = u0;
-    double v1 = u1;
-    if (l10 != 0.0) v1 -= l10 * v0;
-    double v2 = u2;
-    if (l20 != 0.0) v2 -= l20 * v0;
-    if (l21 != 0.0) v2 -= l21 * v1;
-    double v3 = u3;
-    if (l30 != 0.0) v3 -= l30 * v0;
-    if (l31 != 0.0) v3 -= l31 * v1;
-    if (l32 != 0.0) v3 -= l32 * v2;
+    const double v1 = sub_nz(u1, l10, v0);
+    const double v2 = sub_nz(sub_nz(u2, l20, v0), l21, v1);
+    const double v3 = sub_nz(sub_nz(sub_nz(u3, l30, v0), l31, v1), l32, v2);
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       const int r = lane + 32 * i;
-      if (r == c + 1) x[i] = v1;
-      else if (r == c + 2) x[i] = v2;
-      else if (r == c + 3) x[i] = v3;
-      else if (r > c + 3) {
-        const double a0 = T[c * S + r], a1 = T[(c + 1) * S + r], a2 = T[(c + 2) * S + r], a3 = T[(c + 3) * S + r];
-        if (a0 != 0.0) x[i] -= a0 * v0;
-        if (a1 != 0.0) x[i] -= a1 * v1;
-        if (a2 != 0.0) x[i] -= a2 * v2;
-        if (a3 != 0.0) x[i] -= a3 * v3;
-      }
+      const double t = sub_nz(sub_nz(sub_nz(sub_nz(x[i], a[i][0], v0), a[i][1], v1), a[i][2], v2), a[i][3], v3);
+      x[i] = r == c + 1 ? v1 : r == c + 2 ? v2 : r == c + 3 ? v3 : (r > c + 3 ? t : x[i]);
     }
   }
   for (; c < na - 1; ++c) {
+    double a[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) a[i] = T[c * S + lane + 32 * i];
     const double xc = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
 #pragma unroll
-    for (int i = 0; i < R; ++i) {
-      const int r = lane + 32 * i;
-      if (r > c) {
-        const double l = T[c * S + r];
-        if (l != 0.0) x[i] -= l * xc;
-      }
-    }
+    for (int i = 0; i < R; ++i)
+      if (lane + 32 * i > c) x[i] = sub_nz(x[i], a[i], xc);
   }
   c = na - 1;
   for (; c >= 3; c -= 4) {  // backward, columns c, c-1, c-2, c-3
+    double a[R][4];
+#pragma unroll
+    for (int i = 0; i < R; ++i)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) a[i][k] = T[(c - k) * S + lane + 32 * i];
+    const double r3 = rinv[c], r2 = rinv[c - 1], r1 = rinv[c - 2], r0 = rinv[c - 3];
+    const double e23 = T[c * S + c - 1], e13 = T[c * S + c - 2], e03 = T[c * S + c - 3];
+    const double e12 = T[(c - 1) * S + c - 2], e02 = T[(c - 1) * S + c - 3], e01 = T[(c - 2) * S + c - 3];
     const double u3 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
     const double u2 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c - 1), (c - 1) & 31);
     const double u1 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c - 2), (c - 2) & 31);
     const double u0 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c - 3), (c - 3) & 31);
-    const double r3 = rinv[c], r2 = rinv[c - 1], r1 = rinv[c - 2], r0 = rinv[c - 3];
-    const double e23 = T[c * S + c - 1], e13 = T[c * S + c - 2], e03 = T[c * S + c - 3];
-    const double e12 = T[(c - 1) * S + c - 2], e02 = T[(c - 1) * S + c - 3], e01 = T[(c - 2) * S + c - 3];
     const double w3 = u3 * r3;
-    double w2 = u2;
-    if (e23 != 0.0) w2 -= e23 * w3;
-    w2 *= r2;
-    double w1 = u1;
-    if (e13 != 0.0) w1 -= e13 * w3;
-    if (e12 != 0.0) w1 -= e12 * w2;
-    w1 *= r1;
-    double w0 = u0;
-    if (e03 != 0.0) w0 -= e03 * w3;
-    if (e02 != 0.0) w0 -= e02 * w2;
-    if (e01 != 0.0) w0 -= e01 * w1;
-    w0 *= r0;
+    const double w2 = sub_nz(u2, e23, w3) * r2;
+    const double w1 = sub_nz(sub_nz(u1, e13, w3), e12, w2) * r1;
+    const double w0 = sub_nz(sub_nz(sub_nz(u0, e03, w3), e02, w2), e01, w1) * r0;
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       const int r = lane + 32 * i;
-      if (r == c) x[i] = w3;
-      else if (r == c - 1) x[i] = w2;
-      else if (r == c - 2) x[i] = w1;
-      else if (r == c - 3) x[i] = w0;
-      else if (r < c - 3) {
-        const double a3 = T[c * S + r], a2 = T[(c - 1) * S + r], a1 = T[(c - 2) * S + r], a0 = T[(c - 3) * S + r];
-        if (a3 != 0.0) x[i] -= a3 * w3;
-        if (a2 != 0.0) x[i] -= a2 * w2;
-        if (a1 != 0.0) x[i] -= a1 * w1;
-        if (a0 != 0.0) x[i] -= a0 * w0;
-      }
+      const double t = sub_nz(sub_nz(sub_nz(sub_nz(x[i], a[i][0], w3), a[i][1], w2), a[i][2], w1), a[i][3], w0);
+      x[i] = r == c ? w3 : r == c - 1 ? w2 : r == c - 2 ? w1 : r == c - 3 ? w0 : (r < c - 3 ? t : x[i]);
     }
   }
   for (; c >= 0; --c) {
-#pragma unroll
-    for (int i = 0; i < R; ++i)
-      if (lane + 32 * i == c) x[i] *= ri[i];
-    const double xc = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
+    double a[R];
 #pragma unroll
     for (int i = 0; i < R; ++i) {
-      const int r = lane + 32 * i;
-      if (r < c) {
-        const double u = T[c * S + r];
-        if (u != 0.0) x[i] -= u * xc;
-      }
+      a[i] = T[c * S + lane + 32 * i];
+      if (lane + 32 * i == c) x[i] *= ri[i];
     }
+    const double xc = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
+#pragma unroll
+    for (int i = 0; i < R; ++i)
+      if (lane + 32 * i < c) x[i] = sub_nz(x[i], a[i], xc);
   }
 }
 
@@ -839,9 +818,13 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
 
 // Term q of the right-hand side from the compact molar abundances A.xnc: coefficient times the
 // reaction's flux (1/k2!) v xn(k1)^k2 xn(k3), as in calculate_dxdt (jac_rhs.F90:245-252).
+__device__ __forceinline__ double powi_small(double x, int m) {  // powi's products for m = 1, 2, 3
+  return m == 1 ? x : m == 2 ? x * x : m == 3 ? x * (x * x) : powi(x, m);
+}
+
 __device__ __forceinline__ double rhs_term(const Act &A, int q) {
   const uint32_t pk = A.grpk[q];
-  const double flux = A.grcv[q] * powi(A.xnc[pk & 0x3fff], (int)(pk >> 28)) * A.xnc[(pk >> 14) & 0x3fff];
+  const double flux = A.grcv[q] * powi_small(A.xnc[pk & 0x3fff], (int)(pk >> 28)) * A.xnc[(pk >> 14) & 0x3fff];
   return (double)A.gcoef[q] * flux;
 }
 
@@ -860,6 +843,7 @@ __device__ void dev_dxdt_active(const Act &A, const double *yc, double *dxc) {
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int c = tid; c < A.na; c += nt) A.xnc[c] = yc[c] / A.anc[c];
   __syncthreads();
+#pragma unroll 4
   for (int q = tid; q < A.ngi; q += nt) A.gterm[q] = rhs_term(A, q);
   __syncthreads();
   for (int c = tid; c < A.na; c += nt) dxc[c] = gather_dxdt(A, c);

@@ -170,80 +170,84 @@ __device__ int dev_bd_substep(const DevNet &N, const Ws &W, ZoneCtl &C, const Bd
 }
 
 // All sub-steps of one level (semi_implicit_extrapolation, bader_deuflhard.F90:276-316) for a
-// tile-sized active system, by one warp: lane l keeps y_k and delta_k of active rows l + 32 i in
-// registers, computes their dX/dt from the gather items, and the tile solve needs no block barrier.
-// Same arithmetic as dev_bd_substep. Leaves y_k / delta_k in B.yk / B.dk, and in sflag[0] 0 or
-// HUGE_ABUNDS, in sflag[1] the number of solves.
+// tile-sized active system. Each sub-step's right-hand-side terms are computed by the whole CTA;
+// the row sums, the tile solve and the update are done by warp 0, whose lane l keeps y_k and delta_k
+// of active rows l + 32 i in registers. Two barriers per sub-step. Same arithmetic as
+// dev_bd_substep. Leaves y_k / delta_k in B.yk / B.dk; returns 0 or HUGE_ABUNDS.
 template <int R>
-__device__ void bd_level_tile_warp(const Act &A, const BdVec &B, double h, int nseq, bool huge_frozen, int *sflag) {
-  const int lane = threadIdx.x & 31, na = A.na;
+__device__ int bd_level_tile(const Act &A, const BdVec &B, double h, int nseq, bool huge_frozen, int &nsolve,
+                             int *sflag) {
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, na = A.na;
   double y[R], d[R], ri[R], an[R];
-#pragma unroll
-  for (int i = 0; i < R; ++i) {
-    const int r = lane + 32 * i;
-    const bool on = r < na;
-    y[i] = on ? B.yk[r] : 0.0;
-    d[i] = 0.0;
-    ri[i] = on ? A.rinv[r] : 0.0;
-    an[i] = on ? A.anc[r] : 1.0;
-  }
-  int err = 0, ns = 0;
-  for (int j = 0; j <= nseq; ++j) {
-    const int stage = j == 0 ? 1 : (j < nseq ? 2 : 3);  // FIRST, MID, LAST
-    __syncwarp();  // every lane has finished reading xnc and gterm of the previous sub-step
-#pragma unroll
-    for (int i = 0; i < R; ++i)
-      if (lane + 32 * i < na) A.xnc[lane + 32 * i] = y[i] / an[i];
-    __syncwarp();
-    for (int q = lane; q < A.ngi; q += 32) A.gterm[q] = rhs_term(A, q);
-    __syncwarp();
-    double x[R];
+  if (w == 0) {
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       const int r = lane + 32 * i;
-      x[i] = 0.0;
-      if (r < na) {
-        const double dx = gather_dxdt(A, r);
-        x[i] = stage == 1 ? h * dx : h * dx - d[i];
+      const bool on = r < na;
+      y[i] = on ? B.yk[r] : 0.0;
+      d[i] = 0.0;
+      ri[i] = on ? A.rinv[r] : 0.0;
+      an[i] = on ? A.anc[r] : 1.0;
+      if (on) A.xnc[r] = y[i] / an[i];
+    }
+    if (lane == 0) {
+      sflag[0] = 0;  // stop: HUGE_ABUNDS
+      sflag[1] = 0;  // solves done
+    }
+  }
+  for (int j = 0;; ++j) {
+    __syncthreads();  // xnc of sub-step j and the stop flag are written
+    if (sflag[0] != 0 || j > nseq) break;
+#pragma unroll 4
+    for (int q = tid; q < A.ngi; q += nt) A.gterm[q] = rhs_term(A, q);
+    __syncthreads();
+    if (w == 0) {
+      const int stage = j == 0 ? 1 : (j < nseq ? 2 : 3);  // FIRST, MID, LAST
+      double x[R];
+#pragma unroll
+      for (int i = 0; i < R; ++i) {
+        const int r = lane + 32 * i;
+        x[i] = 0.0;
+        if (r < na) {
+          const double dx = gather_dxdt(A, r);
+          x[i] = stage == 1 ? h * dx : h * dx - d[i];
+        }
+      }
+      tile_solve_regs<R>(A.T, A.rinv, na, x, ri, lane);
+      bool huge = false;
+#pragma unroll
+      for (int i = 0; i < R; ++i) {
+        const int r = lane + 32 * i;
+        d[i] = stage == 2 ? d[i] + 2.0 * x[i] : x[i];
+        y[i] = y[i] + d[i];
+        huge |= r < na && y[i] > 2.0;
+        if (r < na) A.xnc[r] = y[i] / an[i];
+      }
+      huge = __any_sync(NUPPN_FULL, huge) || huge_frozen;
+      if (lane == 0) {
+        sflag[1] = j + 1;
+        if (huge) sflag[0] = HUGE_ABUNDS;
       }
     }
-    tile_solve_regs<R>(A.T, A.rinv, na, x, ri, lane);
-    ++ns;
-    bool huge = false;
+  }
+  if (w == 0) {
 #pragma unroll
-    for (int i = 0; i < R; ++i) {
-      d[i] = stage == 2 ? d[i] + 2.0 * x[i] : x[i];
-      y[i] = y[i] + d[i];
-      huge |= lane + 32 * i < na && y[i] > 2.0;
-    }
-    if (__any_sync(NUPPN_FULL, huge) || huge_frozen) {
-      err = HUGE_ABUNDS;
-      break;
-    }
+    for (int i = 0; i < R; ++i)
+      if (lane + 32 * i < na) {
+        B.yk[lane + 32 * i] = y[i];
+        B.dk[lane + 32 * i] = d[i];
+      }
   }
-#pragma unroll
-  for (int i = 0; i < R; ++i)
-    if (lane + 32 * i < na) {
-      B.yk[lane + 32 * i] = y[i];
-      B.dk[lane + 32 * i] = d[i];
-    }
-  if (lane == 0) {
-    sflag[0] = err;
-    sflag[1] = ns;
-  }
-}
-
-__device__ int dev_bd_level_tile(const Act &A, const BdVec &B, double h, int nseq, bool huge_frozen, int &nsolve,
-                                 int *sflag) {
-  if ((threadIdx.x >> 5) == 0) {
-    if (A.tile_rows == 32) bd_level_tile_warp<1>(A, B, h, nseq, huge_frozen, sflag);
-    else bd_level_tile_warp<2>(A, B, h, nseq, huge_frozen, sflag);
-  }
-  __syncthreads();
   const int err = sflag[0];
   nsolve += sflag[1];
   __syncthreads();
   return err;
+}
+
+__device__ int dev_bd_level_tile(const Act &A, const BdVec &B, double h, int nseq, bool huge_frozen, int &nsolve,
+                                 int *sflag) {
+  return A.tile_rows == 32 ? bd_level_tile<1>(A, B, h, nseq, huge_frozen, nsolve, sflag)
+                           : bd_level_tile<2>(A, B, h, nseq, huge_frozen, nsolve, sflag);
 }
 
 // extrapolate (bader_deuflhard.F90:371-407): Neville tableau, column k, on the active rows
