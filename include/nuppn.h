@@ -221,6 +221,13 @@ nuppn_status nuppn_solve_reduced(nuppn_net *net, int32_t nz, const double *jac,
                                  const uint8_t *entry_set, const uint8_t *mask, const double *dt,
                                  const double *b, double *x);
 
+/* compute_nse (physics/source/nse_swj.F90:272-384) for nz zones from a fresh solver state (guess:
+ * X(Ni56) = 1): the NSE mass fractions X[z*nsp + i] (1e-99 off the NSE set), the proton and neutron
+ * chemical potentials (MeV), Newton iterations and the outcome code (0, BAD_YE, BAD_STEP or
+ * NSE_CNVRG, where the reference stops the run). Host buffers. NUPPN_ERR_NET without protons or Ni56. */
+nuppn_status nuppn_nse(nuppn_net *net, int32_t nz, const double *t9, const double *rho, const double *ye, double *X,
+                       double *mu_p, double *mu_n, int32_t *iters, int32_t *ierr);
+
 /* integrate_network (solver.F90:53-238), batched: every zone z advances X[z*ldx + :] over
  * dtwant[z] with its own sub-steps; ye[z] is updated; ierr[z] gets the reference's code. Rates are
  * evaluated at entry (the frames call evaluate_all_rates right before integrate_network) and again

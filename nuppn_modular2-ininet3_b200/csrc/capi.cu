@@ -119,6 +119,7 @@ nuppn_status upload(nuppn_net *net) {
   P(H.sys_of_sp); P(H.sp_of_sys); P(H.pos_of_entry); P(H.lu_src); P(H.lu_rowptr); P(H.lu_diag); P(H.lu_col); P(H.upd_start);
   P(H.upd_off); P(H.lvL_ptr); P(H.lvL_rows); P(H.lvL_grp); P(H.lvU_ptr); P(H.lvU_rows); P(H.lvU_grp);
   P(H.k1_ptr); P(H.k1_list);
+  P(H.nse_idx); P(H.nse_part); P(H.nse_m); P(H.nse_q); P(H.nse_g); P(H.nse_z); P(H.nse_n); P(H.nse_zoa);
   CK(cudaMalloc(&net->arena, A.total));
   net->arena_bytes = A.total;
   std::vector<char> host(A.total, 0);
@@ -155,6 +156,10 @@ nuppn_status upload(nuppn_net *net) {
   D.lvL_ptr = (const int *)nx(); D.lvL_rows = (const int *)nx(); D.lvL_grp = (const int *)nx();
   D.lvU_ptr = (const int *)nx(); D.lvU_rows = (const int *)nx(); D.lvU_grp = (const int *)nx();
   D.k1_ptr = (const int *)nx(); D.k1_list = (const int *)nx();
+  D.nse_idx = (const int *)nx(); D.nse_part = (const int *)nx(); D.nse_m = (const double *)nx();
+  D.nse_q = (const double *)nx(); D.nse_g = (const double *)nx(); D.nse_z = (const double *)nx();
+  D.nse_n = (const double *)nx(); D.nse_zoa = (const double *)nx();
+  D.nse_num = (int)H.nse_idx.size(); D.nse_iprot = H.nse_iprot; D.nse_ini56 = H.nse_ini56; D.nse_p2 = H.nse_p2;
   // scalars
   D.nsp = H.nsp; D.nre = H.nre; D.nact = H.nact; D.ig = H.ig; D.nsys = H.nsys; D.nnzJ = H.nnzJ; D.nnzLU = H.nnzLU;
   D.ihe4 = H.ihe4; D.ibe8 = H.ibe8;
@@ -199,6 +204,8 @@ WsLayout layout(const HostNet &H) {
     L.bd = take((size_t)(2 * kMaxLevels + 8) * H.nsys * sizeof(double));
   }
   L.rx = take(((size_t)H.nsys + 1 + 5 * ((size_t)H.nact + 1)) * sizeof(int));
+  L.nse = take((5 * (size_t)H.nsp + (size_t)H.nse_p2) * sizeof(double));
+  L.nse_stride = (size_t)H.nsp;
   L.bytes = t;
   return L;
 }
@@ -326,10 +333,9 @@ nuppn_status nuppn_net_create(const nuppn_net_desc *desc, const nuppn_knobs *kno
   net->nsm = prop.multiProcessorCount;
   net->block = kn.threads_per_zone > 0 ? kn.threads_per_zone : 256;
   if (net->block % 32 || net->block > 256) { delete net; set_error("threads_per_zone must be a multiple of 32, <= 256"); return NUPPN_ERR_ARG; }
-  if (kn.lu_precision != 0 || kn.i_nse != 0) {
+  if (kn.lu_precision != 0) {
     delete net;
-    set_error(kn.lu_precision != 0 ? "lu_precision: only 0 (FP64 factorization) is available in this build"
-                                    : "i_nse: NSE switching is not available in this build");
+    set_error("lu_precision: only 0 (FP64 factorization) is available in this build");
     return NUPPN_ERR_ARG;
   }
   nuppn_status st = upload(net);
@@ -369,9 +375,13 @@ nuppn_status nuppn_net_info_get(const nuppn_net *net, nuppn_net_info *info) {
 
 nuppn_status nuppn_set_knobs(nuppn_net *net, const nuppn_knobs *knobs) {
   if (!net || !knobs) return NUPPN_ERR_ARG;
-  if (knobs->lu_precision != 0 || knobs->i_nse != 0) {
-    set_error("lu_precision 1 and i_nse 1 are not available in this build");
+  if (knobs->lu_precision != 0) {
+    set_error("lu_precision 1 is not available in this build");
     return NUPPN_ERR_ARG;
+  }
+  if (knobs->i_nse == 1 && (net->H.nse_iprot < 0 || net->H.nse_ini56 < 0)) {
+    set_error("i_nse = 1 needs protons and Ni56 among the considered species");
+    return NUPPN_ERR_NET;
   }
   double old_dgrd = net->H.kn.dgrd;
   net->H.kn = *knobs;
@@ -480,6 +490,46 @@ static nuppn_status run_phase(nuppn_net *net, int nz, int op, const double *X, i
   CK(down(out_v, oov, (size_t)nz * H.nre * 8)); CK(down(out_dxdt, ood, (size_t)nz * H.nsp * 8));
   CK(down(out_jac, ooj, (size_t)nz * H.nnzJ * 8)); CK(down(out_eset, ooe, (size_t)nz * H.nnzJ));
   CK(down(out_mask, oom, (size_t)nz * H.nsp)); CK(down(out_x, oox, (size_t)nz * H.nsp * 8));
+  return NUPPN_OK;
+}
+
+nuppn_status nuppn_nse(nuppn_net *net, int32_t nz, const double *t9, const double *rho, const double *ye, double *X,
+                       double *mu_p, double *mu_n, int32_t *iters, int32_t *ierr) {
+  if (!net) { set_error("null handle"); return NUPPN_ERR_ARG; }
+  if (nz < 0) { set_error("nz < 0"); return NUPPN_ERR_ARG; }
+  if (!t9 || !rho || !ye || !X || !mu_p || !mu_n || !iters || !ierr) { set_error("null argument"); return NUPPN_ERR_ARG; }
+  if (net->H.nse_iprot < 0 || net->H.nse_ini56 < 0) {
+    set_error("NSE needs protons and Ni56 among the considered species");
+    return NUPPN_ERR_NET;
+  }
+  if (nz == 0) return NUPPN_OK;
+  CK(cudaSetDevice(net->device));
+  const int nsp = net->H.nsp;
+  Stager S;
+  size_t o1 = S.add(nz * 8), o2 = S.add(nz * 8), o3 = S.add(nz * 8), oX = S.add((size_t)nz * nsp * 8);
+  size_t op = S.add(nz * 8), on = S.add(nz * 8), oi = S.add(nz * 4), oe = S.add(nz * 4);
+  CK(net->stage.ensure(S.total));
+  char *sb = (char *)net->stage.p;
+  CK(cudaMemcpy(sb + o1, t9, nz * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + o2, rho, nz * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + o3, ye, nz * 8, cudaMemcpyHostToDevice));
+  int grid = std::min(nz, resident_slots(net));
+  nuppn_status st = ensure_ws(net, grid);
+  if (st != NUPPN_OK) return st;
+  PhaseArgs A;
+  memset(&A, 0, sizeof(A));
+  A.nz = nz; A.ldx = nsp; A.op = 4;
+  A.t9 = (const double *)(sb + o1); A.rho = (const double *)(sb + o2); A.ye = (const double *)(sb + o3);
+  A.out_x = (double *)(sb + oX); A.out_mu_p = (double *)(sb + op); A.out_mu_n = (double *)(sb + on);
+  A.out_iters = (int *)(sb + oi); A.out_ierr = (int *)(sb + oe);
+  CK(launch_phase(net->D, net->L, (char *)net->ws.p, grid, net->block, net->act_smem, A, 0));
+  net->launches++;
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(X, sb + oX, (size_t)nz * nsp * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(mu_p, sb + op, nz * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(mu_n, sb + on, nz * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(iters, sb + oi, nz * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ierr, sb + oe, nz * 4, cudaMemcpyDeviceToHost));
   return NUPPN_OK;
 }
 

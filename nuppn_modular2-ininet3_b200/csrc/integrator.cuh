@@ -24,6 +24,7 @@ struct ZoneCtl {
   int smem_bytes;
   int *sint;      // shared scan scratch (>= 32 ints)
   Act act;        // active subsystem of the current Jacobian
+  NseCtl nse;     // NSE solver state of the zone (kept across its NSE calls within one call)
 };
 
 __device__ void vcopy(double *dst, const double *src, int n) {
@@ -453,11 +454,21 @@ __device__ int dev_integrate_zone(const DevNet &N, const Ws &W, ZoneCtl &C, doub
       dev_eval_rates(N, W, my_t9, my_rho, ye, yps, sred);
       t9_last = my_t9; rho_last = my_rho;
     }
+    // NSE above nse_min_t9 (solver.F90:153-158; do_one_time_step, solver.F90:260-266)
+    const bool do_nse = kn.i_nse == 1 && my_t9 >= kn.nse_min_t9;
+    if (do_nse) dev_nse_cache_lm(N, W);
     int ierr = 0;
     if (my_t9 >= kn.min_t9_for_slv) {
-      if (kn.integration_method == 0) ierr = dev_backward_euler(N, W, C, yps, dttry, dtrcmd, sred);
-      else ierr = dev_bader_deuflhard(N, W, C, yps, dttry, dtrcmd, frst, sred);
-      ye = dev_ye(N, yps, sred);
+      if (do_nse) {
+        if (kn.nse_weak_method == 0)
+          ierr = dev_nse_euler(N, W, C.nse, yps, my_t9, my_rho, ye, dttry, dtrcmd, C.smem, C.smem_bytes, sred);
+        else
+          ierr = dev_nse_rk4(N, W, C.nse, yps, my_t9, my_rho, ye, dttry, dtrcmd, C.smem, C.smem_bytes, sred);
+      } else {
+        if (kn.integration_method == 0) ierr = dev_backward_euler(N, W, C, yps, dttry, dtrcmd, sred);
+        else ierr = dev_bader_deuflhard(N, W, C, yps, dttry, dtrcmd, frst, sred);
+        ye = dev_ye(N, yps, sred);
+      }
       if (dttry < K_SMALL) return SMALL_DT;
     }
     if (ierr == 0) {

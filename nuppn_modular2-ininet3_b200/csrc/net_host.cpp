@@ -164,6 +164,23 @@ std::string build_host_net(const nuppn_net_desc &d, const nuppn_knobs &kn, HostN
     if (H.an[i] == 1.0 && (z == 0.0 || z == 1.0)) ppn_q[i] = 0.0;
     if (H.ciso[i] && H.an[i] != 0 && gs[i] != 0 && ppn_m[i] != 0) H.gspin_nse[i] = gs[i];
   }
+  for (int i = 0; i < nsp; ++i) {
+    if (H.gspin_nse[i] == 0.0) continue;
+    const int j = (int)H.nse_idx.size();
+    if (H.zn[i] == 1 && H.an[i] == 1) H.nse_iprot = j;
+    if (H.zn[i] == 28 && H.an[i] == 56) H.nse_ini56 = j;
+    H.nse_idx.push_back(i);
+    H.nse_part.push_back(H.spart[i]);
+    H.nse_m.push_back(ppn_m[i]);
+    H.nse_q.push_back(ppn_q[i]);
+    H.nse_g.push_back(gs[i]);
+    H.nse_z.push_back(H.zn[i]);
+    H.nse_n.push_back(H.an[i] - H.zn[i]);
+    H.nse_zoa.push_back(H.zn[i] / H.an[i]);
+  }
+  while (H.nse_p2 < nsp) H.nse_p2 *= 2;
+  if (kn.i_nse == 1 && (H.nse_iprot < 0 || H.nse_ini56 < 0))
+    return "i_nse = 1 needs protons and Ni56 among the considered species (compute_nse's guess and Coulomb terms)";
   // ---- rate slots: screening, reverse constants, 'RVRSE' targets
   H.scr_mode.assign(nre, 0); H.scr_z1.assign(nre, 0.0); H.scr_z2.assign(nre, 0.0);
   H.rev_target.assign(nre, 0);

@@ -21,6 +21,11 @@ struct HostNet {
   int nsp = 0, nre = 0, ig = 0, nact = 0, nsys = 0, nnzJ = 0, nnzLU = 0, ihe4 = -1, ibe8 = -1;
   int nvar = 0;
   std::vector<double> an, zn, gspin_nse;
+  // NSE set (nse_init, nse_swj.F90:208-245): species, nuclear mass (g), binding energy (MeV), 2J+1,
+  // Z, N, Z/A, partition row (-1: none); positions of the proton and of Ni56 in the set (-1: absent)
+  std::vector<int> nse_idx, nse_part;
+  std::vector<double> nse_m, nse_q, nse_g, nse_z, nse_n, nse_zoa;
+  int nse_iprot = -1, nse_ini56 = -1, nse_p2 = 1;
   std::vector<uint8_t> ciso, crea, rev_target;
   std::vector<int> spart, src, sidx, ilabb, scr_mode, irev, rev_sp, rev_kind;
   std::vector<double> rfac, scr_z1, scr_z2, rev_mc, rev_Q;

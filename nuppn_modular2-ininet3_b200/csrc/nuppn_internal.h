@@ -68,6 +68,10 @@ struct DevNet {
   int njg_long, ndg_long;
   const int *jg_long, *dg_long;            // entries / species whose gather lists are long
   const int *k1_ptr, *k1_list;             // species -> considered reactions it leads (k1), in order
+  // NSE set (nse_swj.F90:208-245)
+  int nse_num, nse_iprot, nse_ini56, nse_p2;
+  const int *nse_idx, *nse_part;
+  const double *nse_m, *nse_q, *nse_g, *nse_z, *nse_n, *nse_zoa;
   // system and LU
   const int *sys_of_sp, *sp_of_sys;        // [nsp], [nsys]
   const int *pos_of_entry;                 // [nnzJ] LU position or -1
@@ -96,6 +100,8 @@ struct WsLayout {
   size_t act_r;                  // global fall-back of the restricted right-hand side
   size_t act_itmp, act_otmp, act_dtmp, act_btmp, bd;  // flattened-gather scratch, compact BD vectors
   size_t rx;                     // active-reaction lists: offsets, flags, kept and passing reactions
+  size_t nse;                    // NSE work arrays [5 * nsp + nse_p2] doubles
+  size_t nse_stride;             // nsp: the length of each NSE work array but the last
   size_t bytes;
 };
 
@@ -161,11 +167,13 @@ struct IntegrateArgs {
 
 // arguments of the single-phase parity kernel
 struct PhaseArgs {
-  int nz, ldx, op;  // op: 0 rates, 1 dxdt, 2 jacobian, 3 reduced solve
+  int nz, ldx, op;  // op: 0 rates, 1 dxdt, 2 jacobian, 3 reduced solve, 4 NSE distribution
   const double *X, *t9, *rho, *ye, *v_in, *dt, *jac_in, *b;
   const uint8_t *eset_in, *mask_in;
   double *out_v, *out_dxdt, *out_jac, *out_x;
   uint8_t *out_eset, *out_mask;
+  double *out_mu_p, *out_mu_n;
+  int *out_iters, *out_ierr;
 };
 
 }  // namespace nuppn

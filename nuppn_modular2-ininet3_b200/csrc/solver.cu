@@ -549,6 +549,7 @@ __device__ void dev_jacobian_mask(const DevNet &N, const Ws &W, double dzeit, co
 }  // namespace nuppn
 
 #include "active_lu.cuh"
+#include "nse.cuh"
 #include "integrator.cuh"
 
 namespace nuppn {
@@ -580,6 +581,7 @@ __global__ void __launch_bounds__(256, 3) k_integrate(const __grid_constant__ De
     C.smem = smem_dyn;
     C.smem_bytes = act_smem;
     C.sint = sint;
+    nse_reset(C.nse);
     double ye = A.ye[z];
     int ierr = dev_integrate_zone(N, W, C, A.t9_0[z], A.t9_1[z], A.rho_0[z], A.rho_1[z], ye, A.dtwant[z], st <= 0, sred);
     for (int s = threadIdx.x; s < N.nsp; s += blockDim.x) A.X[(size_t)z * A.ldx + s] = W.y[s];
@@ -618,7 +620,7 @@ __global__ void __launch_bounds__(256) k_phase(const __grid_constant__ DevNet N,
         A.out_eset[(size_t)z * N.nnzJ + e] = W.eset[e];
       }
       for (int s = tid; s < N.nsp; s += nt) A.out_mask[(size_t)z * N.nsp + s] = W.mask[s];
-    } else {
+    } else if (A.op == 3) {
       for (int e = tid; e < N.nnzJ; e += nt) {
         W.jac[e] = A.jac_in[(size_t)z * N.nnzJ + e];
         W.eset[e] = A.eset_in[(size_t)z * N.nnzJ + e];
@@ -634,6 +636,19 @@ __global__ void __launch_bounds__(256) k_phase(const __grid_constant__ DevNet N,
       bool ok = dev_factor_active(N, W, act, A.dt[z]);
       ok = dev_solve_species(N, act, W.rhs, W.dxdt) && ok;
       for (int s = tid; s < N.nsp; s += nt) A.out_x[(size_t)z * N.nsp + s] = ok ? W.dxdt[s] : NAN;
+    } else if (A.op == 4) {
+      NseCtl S;
+      nse_reset(S);
+      double mu_p, mu_n;
+      int it;
+      const int ierr = dev_compute_nse(N, W, S, A.t9[z], A.rho[z], A.ye[z], W.nse_y1, mu_p, mu_n, it, sred);
+      for (int s = tid; s < N.nsp; s += nt) A.out_x[(size_t)z * N.nsp + s] = ierr == 0 ? W.nse_y1[s] : 0.0;
+      if (tid == 0) {
+        A.out_mu_p[z] = mu_p;
+        A.out_mu_n[z] = mu_n;
+        A.out_iters[z] = it;
+        A.out_ierr[z] = ierr;
+      }
     }
     __syncthreads();
   }

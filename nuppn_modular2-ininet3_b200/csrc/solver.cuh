@@ -29,6 +29,7 @@ struct Ws {
   char *act;     // global fallback of the active-subsystem LU
   char *act_r;   // global fallback of the restricted right-hand side
   int *rx;       // active-reaction lists [nsys+1 + 5*(nact+1)]
+  double *nse_x, *nse_gtot, *nse_mc, *nse_lm, *nse_y1, *nse_sort;  // NSE work arrays
   int *act_itmp; // flattened-list flags / positions [max(list items) + 1]
   int *act_otmp; // segment offsets of the active Jacobian entries [nnzLU + 1]
   double *act_dtmp;   // flattened Jacobian contributions [jg items]
@@ -54,6 +55,12 @@ __device__ __forceinline__ Ws ws_bind(char *base, const WsLayout &L) {
   w.act = base + L.act;
   w.act_r = base + L.act_r;
   w.rx = (int *)(base + L.rx);
+  w.nse_x = (double *)(base + L.nse);
+  w.nse_gtot = w.nse_x + L.nse_stride;
+  w.nse_mc = w.nse_gtot + L.nse_stride;
+  w.nse_lm = w.nse_mc + L.nse_stride;
+  w.nse_y1 = w.nse_lm + L.nse_stride;
+  w.nse_sort = w.nse_y1 + L.nse_stride;
   w.act_itmp = (int *)(base + L.act_itmp);
   w.act_otmp = (int *)(base + L.act_otmp);
   w.act_dtmp = (double *)(base + L.act_dtmp);

@@ -55,9 +55,10 @@ def load_library():
     L.nuppn_integrate_device.argtypes = [vp, i32, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.nuppn_launch_count.argtypes = [vp]
     L.nuppn_launch_count.restype = i64
+    L.nuppn_nse.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp]
     for name in ("nuppn_net_create", "nuppn_net_destroy", "nuppn_net_info_get", "nuppn_set_knobs",
                  "nuppn_jac_pattern", "nuppn_eval_rates", "nuppn_dxdt", "nuppn_jacobian",
-                 "nuppn_solve_reduced", "nuppn_integrate", "nuppn_integrate_device"):
+                 "nuppn_solve_reduced", "nuppn_integrate", "nuppn_integrate_device", "nuppn_nse"):
         getattr(L, name).restype = i32
     _LIB = L
     return L
@@ -166,6 +167,18 @@ class NetworkSolver:
         x = np.zeros((nz, self.nsp))
         self._check(self.L.nuppn_solve_reduced(self.h, nz, _p(jac), _p(es), _p(mk), _p(dt), _p(b), _p(x)))
         return x
+
+    def compute_nse(self, t9, rho, ye):
+        """compute_nse per zone (nuppn_nse): X[nz, nsp], mu_p, mu_n, iterations, ierr."""
+        t9 = np.ascontiguousarray(np.atleast_1d(t9), dtype=np.float64)
+        nz = len(t9)
+        rho, ye = _f64(rho, nz), _f64(ye, nz)
+        X = np.zeros((nz, self.nsp))
+        mu_p, mu_n = np.zeros(nz), np.zeros(nz)
+        it, ierr = np.zeros(nz, np.int32), np.zeros(nz, np.int32)
+        p = lambda a: C.c_void_p(a.ctypes.data)
+        self._check(self.L.nuppn_nse(self.h, nz, p(t9), p(rho), p(ye), p(X), p(mu_p), p(mu_n), p(it), p(ierr)))
+        return X, mu_p, mu_n, it, ierr
 
     def integrate_network(self, X, t9_0, t9_1, rho_0, rho_1, ye, dtwant, bd_state=None):
         """Advance every zone; returns (X, ye, ierr, stats, bd_state). X is not modified."""

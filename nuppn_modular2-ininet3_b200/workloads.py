@@ -71,6 +71,21 @@ def heshell_batch(nz: int, net: sn.Network | None = None, seed: int = 2, dtwant:
                      ye=_ye_of(net, X), dtwant=np.full(nz, dtwant))
 
 
+def nse_batch(nz: int, net: sn.Network | None = None, seed: int = 5, dtwant: float = 1.0e-2) -> ZoneBatch:
+    """Hot zones in nuclear statistical equilibrium: T9 ~ U[6, 10], rho log-U[1e6, 1e8],
+    Ye ~ U[0.46, 0.50]; the starting composition is a Si28 seed (replaced by the NSE distribution
+    on the first step). One integrate_network call of dtwant seconds each."""
+    net = net or network(1107)
+    rng = np.random.default_rng(seed)
+    X = np.full((nz, net.nsp), 1.0e-99)
+    X[:, net.species_index("SI 28")] = 1.0
+    t9 = rng.uniform(6.0, 10.0, nz)
+    rho = 10.0 ** rng.uniform(6.0, 8.0, nz)
+    ye = rng.uniform(0.46, 0.50, nz)
+    return ZoneBatch(X=X, t9_0=t9.copy(), t9_1=t9.copy(), rho_0=rho.copy(), rho_1=rho.copy(), ye=ye,
+                     dtwant=np.full(nz, dtwant))
+
+
 def hburn_zone(net: sn.Network | None = None) -> tuple[ZoneBatch, np.ndarray]:
     """One H-burning zone and its 200 frame time steps (dt log-spaced 1e3 .. 1e13 s)."""
     net = net or network(300)

@@ -228,6 +228,9 @@ struct Net {
   int kmax, kopt0;
   // special species
   int ihe4, ibe8;
+  // NSE set (nse_init, nse_swj.F90:208-245): species indices, positions of p, n, Ni56 in it
+  vector<int> nse_idx;
+  int nse_iprot = -1, nse_ineut = -1, nse_ini56 = -1;
 };
 
 template <class T>
@@ -313,9 +316,15 @@ struct Zone {
   vector<double> qc, ye_rr;  // qcol(nsp,8), yerr(nsp,8) flattened [k*nsp + i]
   double err[9], errmax, abuerr, negerr, sumerr;
   bool reduce = false;
+  // NSE state (nse_swj.F90 module variables): work arrays and the last converged guess
+  vector<double> nse_x, nse_gtot, nse_mucoul, lm_ov_a;
+  double mu_p_coul = 0.0, nse_mu[2] = {0.0, 0.0}, nse_mu_last[2] = {-9.0, -9.0}, nse_the = 0.0, nse_phi = 0.0;
+  bool nse_first = true;
   // stats
   nuppn_zone_stats st;
   explicit Zone(const Net *n) : N(n) {
+    nse_x.assign(N->nse_idx.size(), 0.0); nse_gtot.assign(N->nse_idx.size(), 0.0);
+    nse_mucoul.assign(N->nse_idx.size(), 0.0); lm_ov_a.assign(N->nsp, 0.0);
     v.assign(N->nre, 0.0); v_rev.assign(N->nre, 0.0);
     rv.assign(N->nr, 0.0); reacv.assign(N->nr, 0.0);
     partinter.assign(N->npart, 1.0);
@@ -1149,6 +1158,346 @@ double calculate_ye(const Net &N, const double *x) {  // utils.F90:537-553
   return (1.0 - sortedsum(eta.data(), N.nsp)) * 0.5;
 }
 
+// ---- NSE (physics/source/nse_swj.F90:272-625, solver/source/nse_solver.F90:33-291) ------------
+const double twopi = 2.0 * pi, FIVE_THIRDS = 5.0 * THIRD, SIX_FIFTHS = 6.0 * FIFTH;
+const double ye_tol = 1.e-5;  // solver_knobs.F90:13
+
+void nse_coulomb(Zone &Z, double t9, double rho, double ye) {  // coulomb_corrections, nse_swj.F90:545-580
+  const Net &N = *Z.N;
+  const double a1 = -0.9052, a2 = 0.6322, a3 = -HALF * std::sqrt(THREE) - a1 / std::sqrt(a2);
+  const double kT_erg = boltzmann * t9 * 1.e9, kT_mev = kT_erg * erg2mev;
+  const double ae = std::pow(FOUR * pi * rho * ye * avogadro / THREE, -THIRD);
+  const double Gam_e = qe * qe / kT_erg / ae;
+  for (size_t j = 0; j < N.nse_idx.size(); ++j) {
+    const double G = Gam_e * std::pow(N.zn[N.nse_idx[j]], FIVE_THIRDS);
+    double mc = a1 * (std::sqrt(G * (a2 + G)) - a2 * std::log(std::sqrt(G / a2) + std::sqrt(ONE + G / a2))) +
+                TWO * a3 * (std::sqrt(G) - std::atan(std::sqrt(G)));
+    Z.nse_mucoul[j] = mc * kT_mev;
+  }
+  Z.mu_p_coul = Z.nse_mucoul[N.nse_iprot];
+}
+
+void nse_partition(Zone &Z, double t9) {  // partition_functions, nse_swj.F90:585-597
+  const Net &N = *Z.N;
+  reaclib_partition(Z, t9);
+  for (size_t j = 0; j < N.nse_idx.size(); ++j) {
+    const int i = N.nse_idx[j];
+    Z.nse_gtot[j] = (N.spart[i] >= 0 ? Z.partinter[N.spart[i]] : ONE) * N.ppn_g[i];
+  }
+}
+
+void nse_distribution(Zone &Z, double mu_p, double mu_n, double t9, double rho, double *out) {  // :524-541
+  const Net &N = *Z.N;
+  const double kT_erg = boltzmann * t9 * 1.e9, kT_mev = kT_erg * erg2mev;
+  for (size_t j = 0; j < N.nse_idx.size(); ++j) {
+    const int i = N.nse_idx[j];
+    const double m = N.ppn_m[i], z = N.zn[i], n = N.an[i] - N.zn[i];
+    const double lam = std::sqrt(planck_erg * planck_erg / (twopi * m * kT_erg));
+    const double fac = z * (mu_p + Z.mu_p_coul) + n * mu_n - Z.nse_mucoul[j] + N.ppn_q[i];
+    const double pre = m / rho * Z.nse_gtot[j] / (lam * lam * lam);
+    out[j] = pre * std::exp(fac / kT_mev);
+  }
+}
+
+void nse_rhs(Zone &Z, double ye) {  // calculate_rhs, nse_swj.F90:510-520
+  const Net &N = *Z.N;
+  const int n = (int)N.nse_idx.size();
+  vector<double> zx(n);
+  for (int j = 0; j < n; ++j) zx[j] = (N.zn[N.nse_idx[j]] / N.an[N.nse_idx[j]]) * Z.nse_x[j];
+  Z.nse_the = sortedsum(Z.nse_x.data(), n) - ONE;
+  Z.nse_phi = sortedsum(zx.data(), n) - ye;
+}
+
+void nse_jac(Zone &Z, double t9, double jac[2][2]) {  // calculate_jac, nse_swj.F90:483-506
+  const Net &N = *Z.N;
+  const int n = (int)N.nse_idx.size();
+  const double kT_mev = boltzmann * t9 * 1.e9 * erg2mev;
+  vector<double> dp(n), dn(n), zp(n), zn(n);
+  for (int j = 0; j < n; ++j) {
+    const int i = N.nse_idx[j];
+    const double zoa = N.zn[i] / N.an[i];
+    dp[j] = Z.nse_x[j] * N.zn[i] / kT_mev;
+    dn[j] = Z.nse_x[j] * (N.an[i] - N.zn[i]) / kT_mev;
+    zp[j] = zoa * dp[j];
+    zn[j] = zoa * dn[j];
+  }
+  jac[0][0] = sortedsum(dp.data(), n); jac[0][1] = sortedsum(dn.data(), n);
+  jac[1][0] = sortedsum(zp.data(), n); jac[1][1] = sortedsum(zn.data(), n);
+}
+
+// Crout LU with implicit partial pivoting, and its back substitution, for the 2x2 NSE Jacobian
+// (ludcmp_nse / lubksb_nse, nse_swj.F90:751-883). Returns false for a zero row.
+bool nse_lu2(double a[2][2], int indx[2]) {
+  const int n = 2;
+  double vv[2];
+  for (int i = 0; i < n; ++i) {
+    double aamax = 0.0;
+    for (int j = 0; j < n; ++j) aamax = std::max(aamax, std::fabs(a[i][j]));
+    if (aamax == ZERO) return false;
+    vv[i] = 1.0 / aamax;
+  }
+  for (int j = 0; j < n; ++j) {
+    for (int i = 0; i < j; ++i) {
+      double sum = a[i][j];
+      for (int k = 0; k < i; ++k) sum = sum - a[i][k] * a[k][j];
+      a[i][j] = sum;
+    }
+    double aamax = 0.0;
+    int imax = j;
+    for (int i = j; i < n; ++i) {
+      double sum = a[i][j];
+      for (int k = 0; k < j; ++k) sum = sum - a[i][k] * a[k][j];
+      a[i][j] = sum;
+      const double dum = vv[i] * std::fabs(sum);
+      if (dum >= aamax) { imax = i; aamax = dum; }
+    }
+    if (j != imax) {
+      for (int k = 0; k < n; ++k) std::swap(a[imax][k], a[j][k]);
+      vv[imax] = vv[j];
+    }
+    indx[j] = imax;
+    if (a[j][j] == ZERO) a[j][j] = 1.0e-20;
+    if (j != n - 1) {
+      const double dum = 1.0 / a[j][j];
+      for (int i = j + 1; i < n; ++i) a[i][j] = a[i][j] * dum;
+    }
+  }
+  return true;
+}
+
+void nse_lub2(const double a[2][2], const int indx[2], double b[2]) {
+  const int n = 2;
+  int ii = -1;
+  for (int i = 0; i < n; ++i) {
+    const int ll = indx[i];
+    double sum = b[ll];
+    b[ll] = b[i];
+    if (ii >= 0) {
+      for (int j = ii; j < i; ++j) sum = sum - a[i][j] * b[j];
+    } else if (sum != ZERO) {
+      ii = i;
+    }
+    b[i] = sum;
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    double sum = b[i];
+    for (int j = i + 1; j < n; ++j) sum = sum - a[i][j] * b[j];
+    b[i] = sum / a[i][i];
+  }
+}
+
+// solve_nse (nse_swj.F90:388-460): Newton on (theta, phi) in (mu_p, mu_n) with a x1e-2 line search.
+int solve_nse(Zone &Z, double t9, double rho, double ye, double &mu_p, double &mu_n, int &it, int max_iter) {
+  const int lnsrchmax = 100;
+  Z.nse_mu[0] = mu_p;
+  Z.nse_mu[1] = mu_n;
+  for (int i = 1; i <= max_iter; ++i) {
+    it = i;
+    const double mu_old[2] = {Z.nse_mu[0], Z.nse_mu[1]};
+    nse_rhs(Z, ye);
+    const double the_old = Z.nse_the, phi_old = Z.nse_phi;
+    double jac[2][2];
+    nse_jac(Z, t9, jac);
+    int indx[2];
+    if (!nse_lu2(jac, indx)) return BAD_STEP;
+    double del[2] = {Z.nse_the, Z.nse_phi};
+    nse_lub2(jac, indx, del);
+    double gamma = ONE;
+    for (int j = 1; j <= lnsrchmax; ++j) {
+      if (j == lnsrchmax) return NSE_CNVRG;
+      Z.nse_mu[0] = mu_old[0] - gamma * del[0];
+      Z.nse_mu[1] = mu_old[1] - gamma * del[1];
+      nse_distribution(Z, Z.nse_mu[0], Z.nse_mu[1], t9, rho, Z.nse_x.data());
+      nse_rhs(Z, ye);
+      if (std::fabs(Z.nse_the) > 1.e10 * std::fabs(the_old) + 1.e-10 ||
+          std::fabs(Z.nse_phi) > 1.e10 * std::fabs(phi_old) + 1.e-10)
+        gamma = gamma * 1.e-2;
+      else
+        break;
+    }
+    if (std::fabs(Z.nse_the) <= 1.e-9 && std::fabs(Z.nse_phi) <= 1.e-9) break;
+    if (i == max_iter) return NSE_CNVRG;
+  }
+  mu_p = Z.nse_mu[0];
+  mu_n = Z.nse_mu[1];
+  return 0;
+}
+
+// initial_guess with ni56_initial (nse_swj.F90:466-478): X(Ni56) = 1 and mu_p = mu_n, or the last
+// converged solution.
+void nse_initial_guess(Zone &Z, double &mu_p, double &mu_n, double t9, double rho) {
+  const Net &N = *Z.N;
+  if (!Z.nse_first) {
+    Z.nse_mu[0] = Z.nse_mu_last[0]; Z.nse_mu[1] = Z.nse_mu_last[1];
+    mu_p = Z.nse_mu[0]; mu_n = Z.nse_mu[1];
+    return;
+  }
+  const double kT_erg = boltzmann * t9 * 1.e9, kT_mev = kT_erg * erg2mev;
+  const int j = N.nse_ini56, i = N.nse_idx[j];
+  const double lam = std::sqrt(planck_erg * planck_erg / (twopi * N.ppn_m[i] * kT_erg));
+  mu_p = kT_mev * std::log(ONE * rho * powi(lam, 3) / Z.nse_gtot[j] / N.ppn_m[i]) - N.ppn_q[i] + Z.nse_mucoul[j] -
+         N.zn[i] * Z.mu_p_coul;
+  mu_p = mu_p / N.an[i];
+  mu_n = mu_p;
+}
+
+// compute_nse (nse_swj.F90:272-384). The reference stops the run when the temperature descent also
+// fails; here the failure comes back as the error code.
+int compute_nse(Zone &Z, double t9in, double rho, double ye, double *yps, double &mu_p, double &mu_n, int &iter) {
+  const Net &N = *Z.N;
+  const int nn = (int)N.nse_idx.size();
+  if (ye <= ZERO || ye >= ONE) return BAD_YE;
+  mu_n = ZERO; mu_p = ZERO; iter = 0;
+  for (int i = 0; i < N.nsp; ++i) yps[i] = ZERO;
+  int it = 0;
+  double t9 = t9in;
+  auto finish = [&]() {
+    nse_distribution(Z, mu_p, mu_n, t9, rho, Z.nse_x.data());
+    for (int i = 0; i < N.nsp; ++i) yps[i] = 1.e-99;
+    for (int j = 0; j < nn; ++j) yps[N.nse_idx[j]] = std::max(Z.nse_x[j], 1e-99);
+    Z.nse_mu_last[0] = Z.nse_mu[0]; Z.nse_mu_last[1] = Z.nse_mu[1];
+    Z.nse_first = false;
+    return 0;
+  };
+  nse_coulomb(Z, t9, rho, ye);
+  nse_partition(Z, t9);
+  nse_initial_guess(Z, mu_p, mu_n, t9, rho);
+  nse_distribution(Z, mu_p, mu_n, t9, rho, Z.nse_x.data());
+  int ierr = solve_nse(Z, t9, rho, ye, mu_p, mu_n, it, 100);
+  iter += it;
+  if (ierr == 0) return finish();
+  // temperature descent from T9 = 100
+  const int tsteps = 10;
+  const double coeff = std::pow(100.0 / t9in, ONE / ((double)tsteps - ONE));
+  for (int i = 1; i <= tsteps; ++i) {
+    t9 = t9in * powi(coeff, tsteps - i);
+    nse_coulomb(Z, t9, rho, ye);
+    nse_partition(Z, t9);
+    if (i == 1) nse_initial_guess(Z, mu_p, mu_n, t9, rho);
+    nse_distribution(Z, mu_p, mu_n, t9, rho, Z.nse_x.data());
+    ierr = solve_nse(Z, t9, rho, ye, mu_p, mu_n, it, 500);
+    iter += it;
+  }
+  if (ierr == 0) return finish();
+  return ierr == BAD_STEP ? BAD_STEP : NSE_CNVRG;
+}
+
+// nse_solver_cache_lm_ov_a (nse_solver.F90:33-66): keep only the weak rates, and per parent
+// (lambda_beta - lambda_ec) / A.
+void nse_cache_lm_ov_a(Zone &Z) {
+  const Net &N = *Z.N;
+  for (int l = 0; l < N.nre; ++l) {
+    const int lab = N.ilabb[l];
+    if (!(lab == i_bm || lab == i_ec || lab == i_ve || lab == i_vp)) Z.v[l] = ZERO;
+  }
+  for (double &x : Z.lm_ov_a) x = ZERO;
+  for (int l = 0; l < N.nre; ++l) {
+    if (!N.crea[l] || Z.v[l] == ZERO) continue;
+    const int par = N.k[(size_t)l * 8 + 0], dau = N.k[(size_t)l * 8 + 6];
+    const double lm = Z.v[l], a = N.an[par];
+    if (N.zn[par] < N.zn[dau]) Z.lm_ov_a[par] = Z.lm_ov_a[par] + lm / a;
+    else Z.lm_ov_a[par] = Z.lm_ov_a[par] - lm / a;
+  }
+}
+
+// yedot (nse_solver.F90:104-113): sortedsum(x * lm_ov_a, mask = considerisotope). The reference's
+// sortedsum applies the mask by sorted position (utils.F90:489-495), restated as is.
+double nse_yedot(const Zone &Z, const double *x) {
+  const Net &N = *Z.N;
+  vector<double> t(N.nsp);
+  for (int i = 0; i < N.nsp; ++i) t[i] = x[i] * Z.lm_ov_a[i];
+  vector<int> idx;
+  indexx(N.nsp, t.data(), idx);
+  double s = 0.0;
+  for (int i = 1; i <= N.nsp; ++i)
+    if (N.ciso[i - 1]) s = s + t[idx[i] - 1];
+  return s;
+}
+
+// rk4_nse_step (nse_solver.F90:116-238): Cash-Karp Runge-Kutta for Ye in NSE.
+int rk4_nse_step(Zone &Z, double dt, double rho, double t9, double &ye, vector<double> &y1, double &error) {
+  const double b21 = FIFTH, b31 = 3.0 / 40.0, b32 = 9.0 / 40.0, b41 = 3.0 / 10.0, b42 = -9.0 / 10.0, b43 = SIX_FIFTHS,
+               b51 = -11.0 / 54.0, b52 = 5.0 * HALF, b53 = -70.0 / 27.0, b54 = 35.0 / 27.0, b61 = 1631.0 / 55296.0,
+               b62 = 175.0 / 512.0, b63 = 575.0 / 13824.0, b64 = 44275.0 / 110592.0, b65 = 253.0 / 4096.0,
+               c1 = 37.0 / 378.0, c1s = 2825.0 / 27648.0, c2 = ZERO, c2s = ZERO, c3 = 250.0 / 621.0,
+               c3s = 18575.0 / 48384.0, c4 = 125.0 / 594.0, c4s = 13525.0 / 55296.0, c5 = ZERO,
+               c5s = 277.0 / 14336.0, c6 = 512.0 / 1771.0, c6s = FOURTH;
+  double mu_p, mu_n;
+  int iters, ierr;
+  const double ye_0 = ye;
+  if ((ierr = compute_nse(Z, t9, rho, ye, y1.data(), mu_p, mu_n, iters)) != 0) return ierr;
+  const double k1 = dt * nse_yedot(Z, y1.data());
+  ye = ye_0 + (b21 * k1);
+  if ((ierr = compute_nse(Z, t9, rho, ye, y1.data(), mu_p, mu_n, iters)) != 0) return ierr;
+  const double k2 = dt * nse_yedot(Z, y1.data());
+  ye = ye_0 + (b31 * k1 + b32 * k2);
+  if ((ierr = compute_nse(Z, t9, rho, ye, y1.data(), mu_p, mu_n, iters)) != 0) return ierr;
+  const double k3 = dt * nse_yedot(Z, y1.data());
+  ye = ye_0 + (b41 * k1 + b42 * k2 + b43 * k3);
+  if ((ierr = compute_nse(Z, t9, rho, ye, y1.data(), mu_p, mu_n, iters)) != 0) return ierr;
+  const double k4 = dt * nse_yedot(Z, y1.data());
+  ye = ye_0 + (b51 * k1 + b52 * k2 + b53 * k3 + b54 * k4);
+  if ((ierr = compute_nse(Z, t9, rho, ye, y1.data(), mu_p, mu_n, iters)) != 0) return ierr;
+  const double k5 = dt * nse_yedot(Z, y1.data());
+  ye = ye_0 + (b61 * k1 + b62 * k2 + b63 * k3 + b64 * k4 + b65 * k5);
+  if ((ierr = compute_nse(Z, t9, rho, ye, y1.data(), mu_p, mu_n, iters)) != 0) return ierr;
+  const double k6 = dt * nse_yedot(Z, y1.data());
+  const double ye_5th = ye_0 + c1 * k1 + c2 * k2 + c3 * k3 + c4 * k4 + c5 * k5 + c6 * k6;
+  const double ye_4th = ye_0 + c1s * k1 + c2s * k2 + c3s * k3 + c4s * k4 + c5s * k5 + c6s * k6;
+  ye = ye_5th;
+  if ((ierr = compute_nse(Z, t9, rho, ye, y1.data(), mu_p, mu_n, iters)) != 0) return ierr;
+  error = std::fabs(ye_5th - ye_4th);
+  return 0;
+}
+
+// nse_yedot_rk4 (nse_solver.F90:72-101)
+int nse_yedot_rk4(Zone &Z, vector<double> &yps, double t9, double rho, double &ye, double dt, double &dtrcmd) {
+  const double maxfac = 2.0, minfac = 0.1;
+  const double ye_old = ye;
+  vector<double> y1 = yps;
+  double error = 0.0, fac;
+  int ierr = rk4_nse_step(Z, dt, rho, t9, ye, y1, error);
+  if (ierr != 0) error = ye_old;
+  if (ierr != 0 || ye < ZERO || ye > ONE) {
+    ierr = BAD_YE;
+    fac = HALF * std::pow(std::fabs(ye_tol * ye_old / std::max(error, SMALL)), FIFTH);
+  } else if (error / ye > ye_tol) {
+    ierr = NSE_WEAK;
+    fac = HALF * std::pow(std::fabs(ye_tol * ye / std::max(error, SMALL)), FIFTH);
+  } else {
+    ierr = 0;
+    fac = std::pow(std::fabs(ye_tol * ye / std::max(error, SMALL)), FIFTH);
+    yps = y1;
+  }
+  dtrcmd = dt * std::max(std::min(fac, maxfac), minfac);
+  return ierr;
+}
+
+// nse_yedot_euler (nse_solver.F90:241-289)
+int nse_yedot_euler(Zone &Z, vector<double> &yps, double t9, double rho, double &ye, double dt, double &dtrcmd) {
+  const double deltamax = 1.e-5;
+  vector<double> y1(yps.size());
+  double mu_p, mu_n;
+  int iters;
+  int ierr = compute_nse(Z, t9, rho, ye, y1.data(), mu_p, mu_n, iters);
+  if (ierr != 0 || ye < ZERO || ye > ONE) {
+    dtrcmd = 0.1 * dt;
+    return BAD_STEP;
+  }
+  const double dyedt = nse_yedot(Z, y1.data());
+  const double d_ye = dyedt * dt;
+  if (d_ye > deltamax) {
+    dtrcmd = deltamax / std::fabs(dyedt);
+    return NSE_WEAK;
+  }
+  ye = ye + d_ye;
+  ierr = compute_nse(Z, t9, rho, ye, y1.data(), mu_p, mu_n, iters);
+  if (ierr == 0) yps = y1;
+  else ierr = NSE_CNVRG;
+  dtrcmd = deltamax / std::fabs(dyedt);
+  return ierr;
+}
+
 double interp2(double x0, double x1, double y0, double y1, double xw) {  // interp.F90:29-50
   double xwant = std::max(xw, x0);
   xwant = std::min(xwant, x1);
@@ -1200,11 +1549,19 @@ int integrate_zone(Zone &Z, double *yps_io, double t9_0, double t9_1, double rho
       evaluate_all_rates(Z, ye, my_rho, my_t9, yps.data());
       my_rho_last = my_rho; my_t9_last = my_t9;
     }
+    // NSE above nse_min_t9 (solver.F90:153-158, do_one_time_step :260-266)
+    const bool do_nse = kn.i_nse == 1 && my_t9 >= kn.nse_min_t9;
+    if (do_nse) nse_cache_lm_ov_a(Z);
     ierr = 0;
     if (my_t9 >= kn.min_t9_for_slv) {
-      if (kn.integration_method == 0) ierr = backward_euler_newton(Z, nvar, yps, dttry, dtrcmd);
-      else ierr = bader_deuflhard_integration(Z, yps, dttry, dtrcmd, frst);
-      ye = calculate_ye(N, yps.data());
+      if (do_nse) {
+        if (kn.nse_weak_method == 0) ierr = nse_yedot_euler(Z, yps, my_t9, my_rho, ye, dttry, dtrcmd);
+        else ierr = nse_yedot_rk4(Z, yps, my_t9, my_rho, ye, dttry, dtrcmd);
+      } else {
+        if (kn.integration_method == 0) ierr = backward_euler_newton(Z, nvar, yps, dttry, dtrcmd);
+        else ierr = bader_deuflhard_integration(Z, yps, dttry, dtrcmd, frst);
+        ye = calculate_ye(N, yps.data());
+      }
       if (dttry < SMALL) {
         std::copy(yps.begin(), yps.end(), yps_io);
         if (bd_state) *bd_state = Z.kopt;
@@ -1310,6 +1667,14 @@ void *oracle_net_create(const nuppn_net_desc *d, const nuppn_knobs *kn) {
     if (N->zn[i] == 2 && N->an[i] == 4) N->ihe4 = i;
     if (N->zn[i] == 4 && N->an[i] == 8) N->ibe8 = i;
   }
+  for (int i = 0; i < N->nsp; ++i)
+    if (N->ciso[i] && N->an[i] != 0.0 && N->ppn_g[i] != 0.0 && N->ppn_m[i] != 0.0) {
+      const int j = (int)N->nse_idx.size();
+      N->nse_idx.push_back(i);
+      if (N->zn[i] == 28 && N->an[i] == 56) N->nse_ini56 = j;
+      if (N->zn[i] == 1 && N->an[i] == 1) N->nse_iprot = j;
+      if (N->zn[i] == 0 && N->an[i] == 1) N->nse_ineut = j;
+    }
   makemap(*N);
   bd_init(*N);
   return N;
@@ -1400,6 +1765,19 @@ int oracle_integrate(void *net, int32_t nz, double *X, int32_t ldx, const double
 }
 
 double oracle_calculate_ye(void *net, const double *X) { return calculate_ye(*(Net *)net, X); }
+
+int oracle_nse(void *net, int32_t nz, const double *t9, const double *rho, const double *ye, double *X,
+               int32_t ldx, double *mu_p, double *mu_n, int32_t *iters, int32_t *ierr) {
+  Net *N = (Net *)net;
+  if (N->nse_iprot < 0 || N->nse_ini56 < 0) return -1;
+  for (int z = 0; z < nz; ++z) {
+    Zone Zn(N);
+    int it = 0;
+    ierr[z] = compute_nse(Zn, t9[z], rho[z], ye[z], X + (size_t)z * ldx, mu_p[z], mu_n[z], it);
+    iters[z] = it;
+  }
+  return 0;
+}
 double oracle_sortedsum(const double *a, int32_t n) { return sortedsum(a, n); }
 
 }  // extern "C"

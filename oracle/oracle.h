@@ -49,6 +49,10 @@ int oracle_integrate(void *net, int32_t nz, double *X, int32_t ldx, const double
 
 /* Ye from composition, calculate_ye (utils.F90:537-553) */
 double oracle_calculate_ye(void *net, const double *X);
+// compute_nse (nse_swj.F90:272-384) per zone from a fresh state: X[z*ldx + i], chemical potentials,
+// Newton iterations and the outcome code. Returns -1 if the network has no protons or no Ni56.
+int oracle_nse(void *net, int32_t nz, const double *t9, const double *rho, const double *ye, double *X,
+               int32_t ldx, double *mu_p, double *mu_n, int32_t *iters, int32_t *ierr);
 /* sortedsum (utils.F90:481-501) with the NR heapsort indexx (sort.F90:73-127) */
 double oracle_sortedsum(const double *a, int32_t n);
 

@@ -46,6 +46,7 @@ def load():
     L.oracle_calculate_ye.restype = d
     L.oracle_sortedsum.argtypes = [vp, i32]
     L.oracle_sortedsum.restype = d
+    L.oracle_nse.argtypes = [vp, i32, vp, vp, vp, vp, i32, vp, vp, vp, vp]
     _L = L
     return L
 
@@ -138,6 +139,20 @@ class Oracle:
         self.L.oracle_integrate(self.h, nz, _p(X), X.shape[1], _p(t9_0), _p(t9_1), _p(rho_0), _p(rho_1), _p(ye),
                                 _p(dtwant), _p(ierr), stats, _p(bd), int(nthreads))
         return X, ye, ierr, stats, bd
+
+    def compute_nse(self, t9, rho, ye):
+        """compute_nse (nse_swj.F90:272-384) per zone from a fresh state: X, mu_p, mu_n, iterations, ierr."""
+        t9 = np.ascontiguousarray(np.atleast_1d(t9), dtype=np.float64)
+        nz = len(t9)
+        f = lambda a: np.ascontiguousarray(np.broadcast_to(np.asarray(a, float), (nz,)))
+        rho, ye = f(rho), f(ye)
+        X = np.zeros((nz, self.net.nsp))
+        mu_p, mu_n = np.zeros(nz), np.zeros(nz)
+        it, ierr = np.zeros(nz, np.int32), np.zeros(nz, np.int32)
+        if self.L.oracle_nse(self.h, nz, _p(t9), _p(rho), _p(ye), _p(X), self.net.nsp, _p(mu_p), _p(mu_n),
+                             _p(it), _p(ierr)) != 0:
+            raise ValueError("network has no protons or no Ni56 for NSE")
+        return X, mu_p, mu_n, it, ierr
 
     def calculate_ye(self, X):
         x = np.ascontiguousarray(X, dtype=np.float64)

@@ -205,6 +205,20 @@ def test_hot_heshell_zones_ill_conditioned(orc, abi, wl):
     assert spread > 1e-3
 
 
+def test_oracle_nse_satisfies_constraints(orc, abi, wl):
+    """compute_nse converges to theta = sum X - 1 = 0 and phi = sum (Z/A) X - Ye = 0 within the
+    reference's Newton tolerance (1e-9, nse_swj.F90:104), over T9 6..10 and rho 1e6..1e8."""
+    net = wl.network(1107)
+    ref = orc.Oracle(net, abi.default_knobs())
+    zb = wl.nse_batch(8, net=net)
+    X, mu_p, mu_n, it, ierr = ref.compute_nse(zb.t9_0, zb.rho_0, zb.ye)
+    assert (ierr == 0).all() and (it > 0).all()
+    zoa = np.where(net.anetw > 0, net.znetw / np.where(net.anetw > 0, net.anetw, 1.0), 0.0)
+    assert np.abs(X.sum(axis=1) - 1.0).max() < 2e-9
+    assert np.abs((X * zoa).sum(axis=1) - zb.ye).max() < 2e-9
+    assert np.isfinite(mu_p).all() and np.isfinite(mu_n).all()
+
+
 def test_library_exports_header_symbols(solver_mod):
     """Every function declared in include/nuppn.h is exported by the built library."""
     hdr = open(os.path.join(ROOT, "include", "nuppn.h")).read()

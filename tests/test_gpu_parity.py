@@ -189,3 +189,39 @@ def test_integrate_bd_hot_zones_within_reference_spread(solver_mod, abi, orc, wl
     assert max(s.nvar1_max for s in st) > 32
     assert np.abs(X.sum(axis=1) - 1.0).max() < 1e-10
     assert (rel(X) <= np.maximum(2.0 * spread, 1e-6)).all(), (rel(X), spread)
+
+
+def test_nse_matches_checker(solver_mod, abi, orc, wl):
+    """compute_nse on the device (nuppn_nse) against the checker: same outcome, X within 1e-9 relative
+    for X > 1e-12 and the chemical potentials within 1e-9 (isotope sums differ in rounding order)."""
+    net = wl.network(1107)
+    zb = wl.nse_batch(8, net=net)
+    dev = _dev(solver_mod, net, abi)
+    ref = orc.Oracle(net, abi.default_knobs())
+    X, mp, mn, it, ierr = dev.compute_nse(zb.t9_0, zb.rho_0, zb.ye)
+    Xr, mpr, mnr, itr, ierr_r = ref.compute_nse(zb.t9_0, zb.rho_0, zb.ye)
+    assert (ierr == 0).all() and (ierr_r == 0).all()
+    rel, ab = _compare_X(X, Xr)
+    assert rel <= 1e-9 and ab <= 1e-15, (rel, ab)
+    assert np.abs(mp - mpr).max() <= 1e-9 * np.abs(mpr).max()
+    assert np.abs(mn - mnr).max() <= 1e-9 * np.abs(mnr).max()
+
+
+@pytest.mark.parametrize("method", [1, 0], ids=["rk", "euler"])
+def test_integrate_nse_matches_checker(solver_mod, abi, orc, wl, method):
+    """integrate_network above nse_min_t9 with i_nse = 1: NSE abundances with Ye evolved by the weak
+    rates (Cash-Karp RK or Euler, nse_solver.F90). X within 1e-6 relative; the change of Ye within
+    1e-6 of the checker's change."""
+    net = wl.network(1107)
+    zb = wl.nse_batch(6, net=net, dtwant=100.0)
+    kw = dict(integration_method=1, i_nse=1, nse_weak_method=method)
+    dev = _dev(solver_mod, net, abi, **kw)
+    ref = orc.Oracle(net, abi.default_knobs(**kw))
+    args = (zb.X, zb.t9_0, zb.t9_1, zb.rho_0, zb.rho_1, zb.ye, zb.dtwant)
+    X, ye, ierr, st, _ = dev.integrate_network(*args)
+    Xr, yer, ierr_r, str_, _ = ref.integrate_network(*args)
+    assert (ierr == 0).all() and (ierr_r == 0).all()
+    assert [s.nsucc for s in st] == [s.nsucc for s in str_]
+    rel, ab = _compare_X(X, Xr)
+    assert rel <= 1e-6 and ab <= 1e-15, (rel, ab)
+    assert (np.abs((ye - zb.ye) - (yer - zb.ye)) <= 1e-6 * np.abs(yer - zb.ye) + 1e-15).all(), (ye - yer)
