@@ -86,6 +86,56 @@ def nse_batch(nz: int, net: sn.Network | None = None, seed: int = 5, dtwant: flo
                      dtwant=np.full(nz, dtwant))
 
 
+@dataclasses.dataclass
+class Trajectories:
+    """Explosive-burning trajectories T9(t) = T9_0 exp(-t / (3 tau)), rho(t) = rho_0 exp(-t / tau) on a
+    common time grid; X0 and Ye0 are the starting composition and electron fraction."""
+    t9_0: np.ndarray
+    rho_0: np.ndarray
+    tau: np.ndarray
+    X0: np.ndarray
+    ye0: np.ndarray
+    times: np.ndarray
+
+    @property
+    def nz(self):
+        return len(self.t9_0)
+
+    def t9(self, t):
+        return self.t9_0 * np.exp(-t / (3.0 * self.tau))
+
+    def rho(self, t):
+        return self.rho_0 * np.exp(-t / self.tau)
+
+    def interval(self, k, X, ye):
+        """ZoneBatch for grid interval k (times[k] .. times[k+1]) from the state X, ye."""
+        t0, t1 = self.times[k], self.times[k + 1]
+        return ZoneBatch(X=X, t9_0=self.t9(t0), t9_1=self.t9(t1), rho_0=self.rho(t0), rho_1=self.rho(t1), ye=ye,
+                         dtwant=np.full(self.nz, t1 - t0))
+
+
+def trajectory_batch(nz: int, net: sn.Network | None = None, seed: int = 7, t9_range=(2.0, 5.0),
+                     npts: int = 201, t_end: float = 10.0) -> Trajectories:
+    """tppnp-style trajectories: T9_0 ~ U[t9_range], rho_0 log-U[1e6, 1e8] g/cm^3, tau ~ U[0.1, 1] s,
+    Ye ~ U[0.48, 0.50], on npts points: t = 0 and npts-1 log-spaced times from 1e-6 s to t_end. The
+    seed is Si28 with the Fe56 admixture that gives the drawn Ye (Ye from the composition as
+    calculate_ye, utils.F90:537-553)."""
+    net = net or network(1107)
+    rng = np.random.default_rng(seed)
+    t9_0 = rng.uniform(t9_range[0], t9_range[1], nz)
+    rho_0 = 10.0 ** rng.uniform(6.0, 8.0, nz)
+    tau = rng.uniform(0.1, 1.0, nz)
+    ye = rng.uniform(0.48, 0.50, nz)
+    isi, ife = net.species_index("SI 28"), net.species_index("FE 56")
+    ye_fe = net.znetw[ife] / net.anetw[ife]
+    f = (ye - ye_fe) / (0.5 - ye_fe)
+    X = np.full((nz, net.nsp), 1.0e-99)
+    X[:, isi] = f
+    X[:, ife] = 1.0 - f
+    times = np.concatenate([[0.0], 10.0 ** np.linspace(-6.0, np.log10(t_end), npts - 1)])
+    return Trajectories(t9_0=t9_0, rho_0=rho_0, tau=tau, X0=X, ye0=_ye_of(net, X), times=times)
+
+
 def hburn_zone(net: sn.Network | None = None) -> tuple[ZoneBatch, np.ndarray]:
     """One H-burning zone and its 200 frame time steps (dt log-spaced 1e3 .. 1e13 s)."""
     net = net or network(300)

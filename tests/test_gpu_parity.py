@@ -225,3 +225,36 @@ def test_integrate_nse_matches_checker(solver_mod, abi, orc, wl, method):
     rel, ab = _compare_X(X, Xr)
     assert rel <= 1e-6 and ab <= 1e-15, (rel, ab)
     assert (np.abs((ye - zb.ye) - (yer - zb.ye)) <= 1e-6 * np.abs(yer - zb.ye) + 1e-15).all(), (ye - yer)
+
+
+def test_trajectories_within_reference_spread(solver_mod, abi, orc, wl):
+    """tppnp-style trajectories (T9 falling from 2..5 with rho, Si28/Fe56 seed), 35 consecutive
+    integrate_network intervals from 0 to ~1.2 s on the 1109-species network, each zone carrying its
+    state and Bader-Deuflhard column between calls. Some trajectories are ill-conditioned in the
+    reference's own algorithm (1-ulp input changes move their abundances by up to ~1e-5 here), so each
+    must lie within 2x the checker's spread under such changes, or within 1e-6."""
+    net = wl.network(1107)
+    tr = wl.trajectory_batch(4, net=net, npts=41)
+    kn = abi.default_knobs(integration_method=1)
+    dev = _dev(solver_mod, net, abi, integration_method=1)
+    ref = orc.Oracle(net, kn)
+
+    def run(integrate, X, ye, **kw):
+        bd = np.zeros(tr.nz, np.int32)
+        for k in range(35):
+            zb = tr.interval(k, X, ye)
+            X, ye, ierr, _, bd = integrate(zb.X, zb.t9_0, zb.t9_1, zb.rho_0, zb.rho_1, zb.ye, zb.dtwant,
+                                           bd_state=bd, **kw)
+            assert (ierr == 0).all(), (k, ierr)
+        return X
+
+    Xd = run(dev.integrate_network, tr.X0, tr.ye0)
+    Xr = run(ref.integrate_network, tr.X0, tr.ye0, nthreads=4)
+    big = Xr > 1e-12
+    rel = lambda X: (np.abs(X - Xr) * big / np.where(big, Xr, 1.0)).max(axis=1)
+    spread = np.zeros(tr.nz)
+    for trial in (1, 2):
+        Xp = tr.X0 * (1.0 + np.random.default_rng(trial).choice([-1.0, 0.0, 1.0], size=tr.X0.shape) * 2.2e-16)
+        spread = np.maximum(spread, rel(run(ref.integrate_network, Xp, tr.ye0, nthreads=4)))
+    assert (rel(Xd) <= np.maximum(2.0 * spread, 1e-6)).all(), (rel(Xd), spread)
+    assert np.abs(Xd.sum(axis=1) - 1.0).max() < 1e-10
