@@ -145,6 +145,114 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_traj(args, rank, world, local):
+    """Explosive-burning trajectories: args.nz per GPU, 201 points from 0 to 10 s (T9_0 in [2, 5],
+    rho_0 in [1e6, 1e8], tau in [0.1, 1] s, Si28/Fe56 seed), tppnp's trajectory loop for all of them
+    in one launch. A step integrates every trajectory over the whole grid."""
+    wl = importlib.import_module(PKG + ".workloads")
+    abi = importlib.import_module(PKG + ".abi")
+    net = wl.network(1107)
+    tr_all = wl.trajectory_batch(args.nz * world, net=net, npts=201)
+    sel = np.arange(rank * args.nz, (rank + 1) * args.nz)
+    tt, t9, rho = (g[sel] for g in tr_all.grids())
+    X0, ye0 = tr_all.X0[sel], tr_all.ye0[sel]
+    cfg = {"workload": "tppnp-traj-1107 201 points to 10 s", "trajectories": args.nz * world,
+           "trajectories_per_gpu": args.nz, "network_species": net.nsp, "integrator": "bader-deuflhard",
+           "lu": "fp64", "launches_per_step": 1}
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        cores = os.cpu_count() or 1
+        n = min(args.nz, max(cores, 16))
+        ref = orc.Oracle(net, abi.default_knobs(integration_method=1))
+        times, steps = [], []
+        for it in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            _, _, _, _, st = ref.integrate_trajectories(X0[:n], tt[:n], t9[:n], rho[:n], nthreads=cores)
+            dt = time.perf_counter() - t0
+            if it >= args.warmup:
+                times.append(dt)
+                steps.append(sum(s.nsucc for s in st))
+        v = sum(steps) / sum(times)
+        print(json.dumps({"impl": "reference", "metric": "zone-timesteps/s", "value": v, "unit": "zone-timesteps/s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+                          "cpu_baseline": {"value": v, "unit": "zone-timesteps/s", "cores": cores, "kind": "port",
+                                           "sample": f"{n} of {args.nz} trajectories per step"},
+                          "e2e": {"value": v, "unit": "zone-timesteps/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    solver = importlib.import_module(PKG + ".solver")
+    S = solver.NetworkSolver(net, abi.default_knobs(integration_method=1), device=torch.cuda.current_device())
+    nz = args.nz
+    cu = lambda a, dt=torch.float64: torch.tensor(np.ascontiguousarray(a), dtype=dt, device="cuda")
+    X0d, ye0d, ttd, t9d, rhod = cu(X0), cu(ye0), cu(tt), cu(t9), cu(rho)
+    X, ye = X0d.clone(), ye0d.clone()
+    ierr, fail = (torch.zeros(nz, dtype=torch.int32, device="cuda") for _ in range(2))
+    stats = torch.zeros((nz, 8), dtype=torch.int32, device="cuda")
+    bd = torch.zeros(nz, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def one_step():
+        X.copy_(X0d); ye.copy_(ye0d); bd.zero_()
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        S.integrate_trajectories_device(X, ttd, t9d, rhod, ye, ierr, fail, stats, bd, stream=stream)
+        e1.record()
+        return e0, e1
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = S.launches()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ev = [one_step() for _ in range(args.steps)]
+        torch.cuda.synchronize()
+    st_np = stats.cpu().numpy()
+    steps_done = int(st_np[:, 0].sum()) * args.steps
+    t_ms = float(sum(a.elapsed_time(b) for a, b in ev))
+    gpu_launches = S.launches() - launches0
+    t0 = time.perf_counter()
+    _, _, _, _, st_h = S.integrate_trajectories(X0, tt, t9, rho)
+    e2e_t, e2e_steps = time.perf_counter() - t0, sum(s.nsucc for s in st_h)
+    if world > 1:
+        red = torch.tensor([t_ms, e2e_t], device="cuda", dtype=torch.float64)
+        dist.all_reduce(red, op=dist.ReduceOp.MAX)
+        t_ms, e2e_t = float(red[0]), float(red[1])
+        red = torch.tensor([steps_done, e2e_steps], device="cuda", dtype=torch.float64)
+        dist.all_reduce(red, op=dist.ReduceOp.SUM)
+        steps_done, e2e_steps = int(red[0]), int(red[1])
+    if rank == 0:
+        cfg.update({"accepted_steps_per_call": int(st_np[:, 0].sum()), "rejected_steps_per_call": int(st_np[:, 1].sum()),
+                    "failed_trajectories": int((fail.cpu().numpy() >= 0).sum()),
+                    "l2": "flushed: 256 MiB written before each timed call"})
+        line = {"metric": "zone-timesteps/s", "value": steps_done / (t_ms * 1e-3), "unit": "zone-timesteps/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": cfg, "gpu_launches": int(gpu_launches),
+                "e2e": {"value": e2e_steps / e2e_t, "unit": "zone-timesteps/s",
+                        "h2d_bytes_per_step": int(X0.nbytes + 3 * tt.nbytes + 8 * nz),
+                        "d2h_bytes_per_step": int(X0.nbytes + 8 * nz + 8 * nz + 32 * nz)},
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -155,11 +263,16 @@ def main():
     ap.add_argument("--ref-zones", type=int, default=32)
     ap.add_argument("--cpu-zones", type=int, default=16)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="heshell", choices=["heshell", "traj"],
+                    help="heshell: 1024 He-shell zones (the headline); traj: tppnp-style trajectories")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "traj":
+        run_traj(args, rank, world, local)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

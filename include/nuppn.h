@@ -249,6 +249,26 @@ nuppn_status nuppn_integrate_device(nuppn_net *net, int32_t nz, double *d_X, int
                                     int32_t *d_ierr, nuppn_zone_stats *d_stats, int32_t *d_bd_state,
                                     void *stream);
 
+/* The trajectory loop of tppnp (frames/tppnp/source/tppnp.F90:131-168), batched: every zone z follows
+ * its own trajectory of npts points time[z*npts + i], t9[...], rho[...]. The starting composition is
+ * renormalised (Kahan sum) if |1 - sum X| > 1e-8; then for each interval i: Ye from the composition
+ * (calculate_ye), integrate_network from point i to i+1, stop at the first interval with a non-zero
+ * outcome (ierr[z] = that code, fail[z] = i; fail[z] = -1 when all succeed), and renormalise if
+ * |1 - sum X| > 5e-7. Each zone carries its Bader-Deuflhard column and first-call flag between its
+ * intervals (fresh for every trajectory). One launch for all intervals of all zones: zones with
+ * few and many sub-steps share the GPU instead of waiting for each other interval by interval.
+ * stats sum over the intervals (nvar1_max: maximum). fail and stats may be NULL. Host buffers. */
+nuppn_status nuppn_integrate_trajectories(nuppn_net *net, int32_t nz, int32_t npts, double *X, int32_t ldx,
+                                         const double *time, const double *t9, const double *rho, double *ye,
+                                         int32_t *ierr, int32_t *fail, nuppn_zone_stats *stats);
+
+/* Same on device-resident buffers, asynchronous on the given stream; bd_state as for
+ * nuppn_integrate_device (0 = fresh). */
+nuppn_status nuppn_integrate_trajectories_device(nuppn_net *net, int32_t nz, int32_t npts, double *d_X, int32_t ldx,
+                                                const double *d_time, const double *d_t9, const double *d_rho,
+                                                double *d_ye, int32_t *d_ierr, int32_t *d_fail,
+                                                nuppn_zone_stats *d_stats, int32_t *d_bd_state, void *stream);
+
 /* Same as nuppn_integrate_device, but this call allocates no device memory. It has no counterpart
  * in the reference (whose solver allocates through SuperLU on every call); it is for callers that
  * cannot call cudaMalloc while they step: programs that hand all of the GPU's memory to their own

@@ -24,7 +24,7 @@ constexpr int kSpinLimit = 1 << 22;  // per wait; a timeout marks the zone as fa
 
 // Sparse active subsystems up to this size are factored and solved by one warp, row after row,
 // with no inter-warp flags; larger ones by all warps with per-row ready flags.
-constexpr int kOneWarpMax = 192;
+constexpr int kOneWarpMax = 512;
 
 // Flags of a compact LU position (jflag): entry set, diagonal, fill (no Jacobian entry).
 enum : uint8_t { JF_SET = 1, JF_DIAG = 2, JF_FILL = 4 };

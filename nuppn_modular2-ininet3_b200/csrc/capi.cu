@@ -431,7 +431,7 @@ nuppn_status nuppn_integrate_device_noalloc(nuppn_net *net, int32_t nz, double *
   const int grid = std::min(std::min(nz, resident_slots(net)), slabs);
   cudaStream_t s = (cudaStream_t)stream;
   CK(cudaMemsetAsync(base, 0, sizeof(int), s));  // the zone counter starts at zero every call
-  IntegrateArgs A;
+  IntegrateArgs A = {};
   A.nz = nz; A.ldx = ldx; A.X = d_X; A.t9_0 = d_t9_0; A.t9_1 = d_t9_1; A.rho_0 = d_rho_0; A.rho_1 = d_rho_1;
   A.dtwant = d_dtwant; A.ye = d_ye; A.ierr = d_ierr; A.stats = d_stats; A.bd_state = d_bd_state;
   A.counter = (int *)base;
@@ -578,7 +578,7 @@ nuppn_status nuppn_integrate_device(nuppn_net *net, int32_t nz, double *d_X, int
   if (st != NUPPN_OK) return st;
   cudaStream_t s = (cudaStream_t)stream;
   CK(cudaMemsetAsync(net->counter.p, 0, sizeof(int), s));
-  IntegrateArgs A;
+  IntegrateArgs A = {};
   A.nz = nz; A.ldx = ldx; A.X = d_X; A.t9_0 = d_t9_0; A.t9_1 = d_t9_1; A.rho_0 = d_rho_0; A.rho_1 = d_rho_1;
   A.dtwant = d_dtwant; A.ye = d_ye; A.ierr = d_ierr; A.stats = d_stats; A.bd_state = d_bd_state;
   A.counter = (int *)net->counter.p;
@@ -623,6 +623,71 @@ nuppn_status nuppn_integrate(nuppn_net *net, int32_t nz, double *X, int32_t ldx,
   CK(cudaMemcpy(ierr, sb + oi, nz * 4, cudaMemcpyDeviceToHost));
   if (stats) CK(cudaMemcpy(stats, sb + os, (size_t)nz * sizeof(nuppn_zone_stats), cudaMemcpyDeviceToHost));
   if (bd_state) CK(cudaMemcpy(bd_state, sb + ob, nz * 4, cudaMemcpyDeviceToHost));
+  return NUPPN_OK;
+}
+
+nuppn_status nuppn_integrate_trajectories_device(nuppn_net *net, int32_t nz, int32_t npts, double *d_X, int32_t ldx,
+                                                const double *d_time, const double *d_t9, const double *d_rho,
+                                                double *d_ye, int32_t *d_ierr, int32_t *d_fail,
+                                                nuppn_zone_stats *d_stats, int32_t *d_bd_state, void *stream) {
+  nuppn_status st = check_zone_args(net, nz, ldx);
+  if (st != NUPPN_OK) return st;
+  if (npts < 2) { set_error("npts < 2"); return NUPPN_ERR_ARG; }
+  if (nz == 0) return NUPPN_OK;
+  if (!d_X || !d_time || !d_t9 || !d_rho || !d_ye || !d_ierr) {
+    set_error("null device argument");
+    return NUPPN_ERR_ARG;
+  }
+  CK(cudaSetDevice(net->device));
+  int grid = std::min(nz, resident_slots(net));
+  st = ensure_ws(net, grid);
+  if (st != NUPPN_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  CK(cudaMemsetAsync(net->counter.p, 0, sizeof(int), s));
+  IntegrateArgs A = {};
+  A.nz = nz; A.ldx = ldx; A.X = d_X; A.ye = d_ye; A.ierr = d_ierr; A.stats = d_stats; A.bd_state = d_bd_state;
+  A.counter = (int *)net->counter.p;
+  A.npts = npts; A.tr_time = d_time; A.tr_t9 = d_t9; A.tr_rho = d_rho; A.tr_fail = d_fail;
+  CK(launch_integrate(net->D, net->L, (char *)net->ws.p, grid, net->block, net->act_smem, A, s));
+  net->launches++;
+  return NUPPN_OK;
+}
+
+nuppn_status nuppn_integrate_trajectories(nuppn_net *net, int32_t nz, int32_t npts, double *X, int32_t ldx,
+                                         const double *time, const double *t9, const double *rho, double *ye,
+                                         int32_t *ierr, int32_t *fail, nuppn_zone_stats *stats) {
+  nuppn_status st = check_zone_args(net, nz, ldx);
+  if (st != NUPPN_OK) return st;
+  if (npts < 2) { set_error("npts < 2"); return NUPPN_ERR_ARG; }
+  if (nz == 0) return NUPPN_OK;
+  if (!X || !time || !t9 || !rho || !ye || !ierr) {
+    set_error("null argument");
+    return NUPPN_ERR_ARG;
+  }
+  CK(cudaSetDevice(net->device));
+  const size_t np = (size_t)nz * npts * 8;
+  Stager S;
+  size_t oX = S.add((size_t)nz * ldx * 8), ot = S.add(np), o9 = S.add(np), orh = S.add(np), oy = S.add(nz * 8);
+  size_t oi = S.add(nz * 4), of = S.add(nz * 4), os = S.add((size_t)nz * sizeof(nuppn_zone_stats)), ob = S.add(nz * 4);
+  CK(net->stage.ensure(S.total));
+  char *sb = (char *)net->stage.p;
+  CK(cudaMemcpy(sb + oX, X, (size_t)nz * ldx * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + ot, time, np, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + o9, t9, np, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + orh, rho, np, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + oy, ye, nz * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemset(sb + ob, 0, nz * 4));
+  st = nuppn_integrate_trajectories_device(net, nz, npts, (double *)(sb + oX), ldx, (double *)(sb + ot),
+                                           (double *)(sb + o9), (double *)(sb + orh), (double *)(sb + oy),
+                                           (int *)(sb + oi), (int *)(sb + of), (nuppn_zone_stats *)(sb + os),
+                                           (int *)(sb + ob), nullptr);
+  if (st != NUPPN_OK) return st;
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(X, sb + oX, (size_t)nz * ldx * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ye, sb + oy, nz * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ierr, sb + oi, nz * 4, cudaMemcpyDeviceToHost));
+  if (fail) CK(cudaMemcpy(fail, sb + of, nz * 4, cudaMemcpyDeviceToHost));
+  if (stats) CK(cudaMemcpy(stats, sb + os, (size_t)nz * sizeof(nuppn_zone_stats), cudaMemcpyDeviceToHost));
   return NUPPN_OK;
 }
 

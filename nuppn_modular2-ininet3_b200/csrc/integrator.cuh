@@ -55,6 +55,25 @@ __device__ void ypsplus(double *y, int n) {
   __syncthreads();
 }
 
+// renorm_1d (utils.F90:436-446): y / ksum(y), the Kahan sum (utils.F90:670-685) taken in order
+__device__ void dev_renorm_ksum(double *y, int n, double *sred) {
+  if (threadIdx.x == 0) {
+    double c = 0.0, s = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double yy = y[i] - c;
+      const double t = s + yy;
+      c = (t - s) - yy;
+      s = t;
+    }
+    sred[0] = s;
+  }
+  __syncthreads();
+  const double s = sred[0];
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = y[i] / s;
+  __syncthreads();
+}
+
 // calculate_ye (utils.F90:537-553)
 __device__ double dev_ye(const DevNet &N, const double *x, double *sred) {
   double s = 0.0;

@@ -163,6 +163,11 @@ struct IntegrateArgs {
   nuppn_zone_stats *stats;
   int *bd_state;
   int *counter;
+  // trajectory mode (npts > 0): per zone npts points of time, T9 and rho ([nz][npts]); tr_fail gets
+  // the index of the interval that failed, or -1
+  int npts;
+  const double *tr_time, *tr_t9, *tr_rho;
+  int *tr_fail;
 };
 
 // arguments of the single-phase parity kernel

@@ -583,13 +583,34 @@ __global__ void __launch_bounds__(256, 3) k_integrate(const __grid_constant__ De
     C.sint = sint;
     nse_reset(C.nse);
     double ye = A.ye[z];
-    int ierr = dev_integrate_zone(N, W, C, A.t9_0[z], A.t9_1[z], A.rho_0[z], A.rho_1[z], ye, A.dtwant[z], st <= 0, sred);
+    int ierr, fail = -1;
+    if (A.npts > 0) {
+      // the trajectory loop of tppnp (tppnp.F90:131-168) for this zone
+      const double *tt = A.tr_time + (size_t)z * A.npts, *tp = A.tr_t9 + (size_t)z * A.npts;
+      const double *tr = A.tr_rho + (size_t)z * A.npts;
+      if (fabs(1.0 - vsum(W.y, N.nsp, sred)) > 1.e-8) dev_renorm_ksum(W.y, N.nsp, sred);
+      bool frst = st <= 0;
+      ierr = 0;
+      for (int i = 1; i < A.npts; ++i) {
+        ye = dev_ye(N, W.y, sred);
+        ierr = dev_integrate_zone(N, W, C, tp[i - 1], tp[i], tr[i - 1], tr[i], ye, tt[i] - tt[i - 1], frst, sred);
+        frst = false;
+        if (ierr != 0) {
+          fail = i - 1;
+          break;
+        }
+        if (fabs(1.0 - vsum(W.y, N.nsp, sred)) > 5.e-7) dev_renorm_ksum(W.y, N.nsp, sred);
+      }
+    } else {
+      ierr = dev_integrate_zone(N, W, C, A.t9_0[z], A.t9_1[z], A.rho_0[z], A.rho_1[z], ye, A.dtwant[z], st <= 0, sred);
+    }
     for (int s = threadIdx.x; s < N.nsp; s += blockDim.x) A.X[(size_t)z * A.ldx + s] = W.y[s];
     if (threadIdx.x == 0) {
       A.ye[z] = ye;
       A.ierr[z] = ierr;
       if (A.stats) A.stats[z] = C.st;
       if (A.bd_state) A.bd_state[z] = C.kopt;
+      if (A.tr_fail) A.tr_fail[z] = fail;
     }
   }
 }

@@ -56,9 +56,12 @@ def load_library():
     L.nuppn_launch_count.argtypes = [vp]
     L.nuppn_launch_count.restype = i64
     L.nuppn_nse.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.nuppn_integrate_trajectories.argtypes = [vp, i32, i32, vp, i32, vp, vp, vp, vp, vp, vp, vp]
+    L.nuppn_integrate_trajectories_device.argtypes = [vp, i32, i32, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     for name in ("nuppn_net_create", "nuppn_net_destroy", "nuppn_net_info_get", "nuppn_set_knobs",
                  "nuppn_jac_pattern", "nuppn_eval_rates", "nuppn_dxdt", "nuppn_jacobian",
-                 "nuppn_solve_reduced", "nuppn_integrate", "nuppn_integrate_device", "nuppn_nse"):
+                 "nuppn_solve_reduced", "nuppn_integrate", "nuppn_integrate_device", "nuppn_nse",
+                 "nuppn_integrate_trajectories", "nuppn_integrate_trajectories_device"):
         getattr(L, name).restype = i32
     _LIB = L
     return L
@@ -167,6 +170,29 @@ class NetworkSolver:
         x = np.zeros((nz, self.nsp))
         self._check(self.L.nuppn_solve_reduced(self.h, nz, _p(jac), _p(es), _p(mk), _p(dt), _p(b), _p(x)))
         return x
+
+    def integrate_trajectories(self, X, time, t9, rho):
+        """tppnp's trajectory loop for every zone in one launch (nuppn_integrate_trajectories):
+        X[nz, nsp] starting compositions, per-zone time/t9/rho [nz, npts]. Returns (X, ye, ierr, fail,
+        stats)."""
+        X = np.array(np.atleast_2d(X), dtype=np.float64, order="C", copy=True)
+        nz = X.shape[0]
+        f = lambda a: np.ascontiguousarray(np.broadcast_to(np.asarray(a, np.float64), (nz, np.shape(a)[-1])))
+        time, t9, rho = f(time), f(t9), f(rho)
+        ye, ierr, fail = np.zeros(nz), np.zeros(nz, np.int32), np.zeros(nz, np.int32)
+        stats = (abi.ZoneStats * nz)()
+        p = lambda a: C.c_void_p(a.ctypes.data)
+        self._check(self.L.nuppn_integrate_trajectories(self.h, nz, time.shape[1], p(X), X.shape[1], p(time), p(t9),
+                                                        p(rho), p(ye), p(ierr), p(fail), stats))
+        return X, ye, ierr, fail, stats
+
+    def integrate_trajectories_device(self, X, time, t9, rho, ye, ierr, fail=None, stats=None, bd_state=None,
+                                      stream=0):
+        """Device-resident form (torch CUDA tensors); time/t9/rho are [nz, npts]."""
+        ptr = lambda t: None if t is None else C.c_void_p(t.data_ptr())
+        self._check(self.L.nuppn_integrate_trajectories_device(
+            self.h, X.shape[0], time.shape[1], ptr(X), X.shape[1], ptr(time), ptr(t9), ptr(rho), ptr(ye), ptr(ierr),
+            ptr(fail), ptr(stats), ptr(bd_state), C.c_void_p(stream)))
 
     def compute_nse(self, t9, rho, ye):
         """compute_nse per zone (nuppn_nse): X[nz, nsp], mu_p, mu_n, iterations, ierr."""

@@ -107,6 +107,11 @@ class Trajectories:
     def rho(self, t):
         return self.rho_0 * np.exp(-t / self.tau)
 
+    def grids(self):
+        """Per-zone time, T9 and rho at every grid point, [nz, npts] each."""
+        tt = np.broadcast_to(self.times, (self.nz, len(self.times))).copy()
+        return tt, self.t9(tt.T).T.copy(), self.rho(tt.T).T.copy()
+
     def interval(self, k, X, ye):
         """ZoneBatch for grid interval k (times[k] .. times[k+1]) from the state X, ye."""
         t0, t1 = self.times[k], self.times[k + 1]

@@ -1766,6 +1766,65 @@ int oracle_integrate(void *net, int32_t nz, double *X, int32_t ldx, const double
 
 double oracle_calculate_ye(void *net, const double *X) { return calculate_ye(*(Net *)net, X); }
 
+// The trajectory loop of tppnp (frames/tppnp/source/tppnp.F90:131-168) per zone.
+int oracle_integrate_trajectories(void *net, int32_t nz, int32_t npts, double *X, int32_t ldx, const double *time,
+                                  const double *t9, const double *rho, double *ye, int32_t *ierr, int32_t *fail,
+                                  nuppn_zone_stats *stats, int32_t nthreads) {
+  Net *N = (Net *)net;
+  if (!g_slu_solve) return -1;
+  auto ksum = [](const double *a, int n) {  // utils.F90:670-685
+    double c = 0.0, s = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double y = a[i] - c;
+      const double t = s + y;
+      c = (t - s) - y;
+      s = t;
+    }
+    return s;
+  };
+  std::atomic<int> next(0);
+  auto worker = [&]() {
+    for (;;) {
+      const int z = next.fetch_add(1);
+      if (z >= nz) break;
+      Zone Zn(N);
+      double *y = X + (size_t)z * ldx;
+      const double *tt = time + (size_t)z * npts, *tp = t9 + (size_t)z * npts, *tr = rho + (size_t)z * npts;
+      if (std::fabs(ONE - sortedsum(y, N->nsp)) > 1.e-8) {  // check_2d_mass_cons(.true.), renorm_2d
+        const double s = ksum(y, N->nsp);
+        for (int i = 0; i < N->nsp; ++i) y[i] = y[i] / s;
+      }
+      int32_t bd = 0;
+      int r = 0, f = -1;
+      double yez = ye[z];
+      for (int i = 1; i < npts; ++i) {
+        yez = calculate_ye(*N, y);
+        r = integrate_zone(Zn, y, tp[i - 1], tp[i], tr[i - 1], tr[i], yez, tt[i] - tt[i - 1], &bd);
+        if (r != 0) {
+          f = i - 1;
+          break;
+        }
+        double s = 0.0;  // check_1d_mass_cons(.false.)
+        for (int q = 0; q < N->nsp; ++q) s += y[q];
+        if (std::fabs(ONE - s) > 5.e-7) {
+          const double k = ksum(y, N->nsp);
+          for (int q = 0; q < N->nsp; ++q) y[q] = y[q] / k;
+        }
+      }
+      ye[z] = yez;
+      ierr[z] = r;
+      if (fail) fail[z] = f;
+      if (stats) stats[z] = Zn.st;
+    }
+  };
+  const int nt = std::max(1, (int)nthreads);
+  std::vector<std::thread> th;
+  for (int t = 1; t < nt; ++t) th.emplace_back(worker);
+  worker();
+  for (auto &t : th) t.join();
+  return 0;
+}
+
 int oracle_nse(void *net, int32_t nz, const double *t9, const double *rho, const double *ye, double *X,
                int32_t ldx, double *mu_p, double *mu_n, int32_t *iters, int32_t *ierr) {
   Net *N = (Net *)net;

@@ -49,6 +49,10 @@ int oracle_integrate(void *net, int32_t nz, double *X, int32_t ldx, const double
 
 /* Ye from composition, calculate_ye (utils.F90:537-553) */
 double oracle_calculate_ye(void *net, const double *X);
+// tppnp's trajectory loop (tppnp.F90:131-168) per zone over npts points ([nz][npts] arrays).
+int oracle_integrate_trajectories(void *net, int32_t nz, int32_t npts, double *X, int32_t ldx, const double *time,
+                                  const double *t9, const double *rho, double *ye, int32_t *ierr, int32_t *fail,
+                                  nuppn_zone_stats *stats, int32_t nthreads);
 // compute_nse (nse_swj.F90:272-384) per zone from a fresh state: X[z*ldx + i], chemical potentials,
 // Newton iterations and the outcome code. Returns -1 if the network has no protons or no Ni56.
 int oracle_nse(void *net, int32_t nz, const double *t9, const double *rho, const double *ye, double *X,

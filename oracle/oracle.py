@@ -47,6 +47,7 @@ def load():
     L.oracle_sortedsum.argtypes = [vp, i32]
     L.oracle_sortedsum.restype = d
     L.oracle_nse.argtypes = [vp, i32, vp, vp, vp, vp, i32, vp, vp, vp, vp]
+    L.oracle_integrate_trajectories.argtypes = [vp, i32, i32, vp, i32, vp, vp, vp, vp, vp, vp, vp, i32]
     _L = L
     return L
 
@@ -139,6 +140,18 @@ class Oracle:
         self.L.oracle_integrate(self.h, nz, _p(X), X.shape[1], _p(t9_0), _p(t9_1), _p(rho_0), _p(rho_1), _p(ye),
                                 _p(dtwant), _p(ierr), stats, _p(bd), int(nthreads))
         return X, ye, ierr, stats, bd
+
+    def integrate_trajectories(self, X, time, t9, rho, nthreads=1):
+        """tppnp's trajectory loop per zone: X[nz, nsp], per-zone time/t9/rho [nz, npts]."""
+        X = np.array(np.atleast_2d(X), dtype=np.float64, order="C", copy=True)
+        nz = X.shape[0]
+        f = lambda a: np.ascontiguousarray(np.broadcast_to(np.asarray(a, float), (nz, np.shape(a)[-1])))
+        time, t9, rho = f(time), f(t9), f(rho)
+        ye, ierr, fail = np.zeros(nz), np.zeros(nz, np.int32), np.zeros(nz, np.int32)
+        stats = (self._abi.ZoneStats * nz)()
+        self.L.oracle_integrate_trajectories(self.h, nz, time.shape[1], _p(X), X.shape[1], _p(time), _p(t9), _p(rho),
+                                             _p(ye), _p(ierr), _p(fail), stats, int(nthreads))
+        return X, ye, ierr, fail, stats
 
     def compute_nse(self, t9, rho, ye):
         """compute_nse (nse_swj.F90:272-384) per zone from a fresh state: X, mu_p, mu_n, iterations, ierr."""

@@ -258,3 +258,28 @@ def test_trajectories_within_reference_spread(solver_mod, abi, orc, wl):
         spread = np.maximum(spread, rel(run(ref.integrate_network, Xp, tr.ye0, nthreads=4)))
     assert (rel(Xd) <= np.maximum(2.0 * spread, 1e-6)).all(), (rel(Xd), spread)
     assert np.abs(Xd.sum(axis=1) - 1.0).max() < 1e-10
+
+
+def test_trajectory_entry_within_reference_spread(solver_mod, abi, orc, wl):
+    """nuppn_integrate_trajectories (tppnp's trajectory loop for all zones in one launch) against the
+    checker's restatement of the same loop, 4 trajectories of 36 points (0 to ~1.2 s): every
+    trajectory succeeds, and each lies within 2x the checker's spread under 1-ulp input changes, or
+    within 1e-6."""
+    net = wl.network(1107)
+    tr = wl.trajectory_batch(4, net=net, npts=41)
+    tt, t9, rho = (g[:, :36] for g in tr.grids())
+    kn = abi.default_knobs(integration_method=1)
+    dev = _dev(solver_mod, net, abi, integration_method=1)
+    ref = orc.Oracle(net, kn)
+    Xd, yed, ierr, fail, st = dev.integrate_trajectories(tr.X0, tt, t9, rho)
+    Xr, yer, ierr_r, fail_r, _ = ref.integrate_trajectories(tr.X0, tt, t9, rho, nthreads=4)
+    assert (ierr == 0).all() and (ierr_r == 0).all() and (fail == -1).all()
+    assert min(s.nsucc for s in st) >= 35
+    big = Xr > 1e-12
+    rel = lambda X: (np.abs(X - Xr) * big / np.where(big, Xr, 1.0)).max(axis=1)
+    spread = np.zeros(tr.nz)
+    for trial in (1, 2):
+        Xp = tr.X0 * (1.0 + np.random.default_rng(trial).choice([-1.0, 0.0, 1.0], size=tr.X0.shape) * 2.2e-16)
+        spread = np.maximum(spread, rel(ref.integrate_trajectories(Xp, tt, t9, rho, nthreads=4)[0]))
+    assert (rel(Xd) <= np.maximum(2.0 * spread, 1e-6)).all(), (rel(Xd), spread)
+    assert np.abs(yed - yer).max() < 1e-9
