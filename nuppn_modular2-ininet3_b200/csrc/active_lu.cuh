@@ -22,8 +22,11 @@ namespace nuppn {
 
 constexpr int kSpinLimit = 1 << 22;  // per wait; a timeout marks the zone as failed, never hangs
 
-// Sparse active subsystems up to this size are factored and solved by one warp, row after row,
-// with no inter-warp flags; larger ones by all warps with per-row ready flags.
+// Sparse active subsystems up to kOneWarpFactorMax rows are factored, and up to kOneWarpMax rows
+// solved, by one warp row after row with no inter-warp flags; larger ones by all warps with per-row
+// ready flags (for large systems the factorization has more independent work per row than the
+// solves, so it leaves one warp sooner).
+constexpr int kOneWarpFactorMax = 192;
 constexpr int kOneWarpMax = 512;
 
 // Flags of a compact LU position (jflag): entry set, diagonal, fill (no Jacobian entry).
@@ -32,10 +35,12 @@ enum : uint8_t { JF_SET = 1, JF_DIAG = 2, JF_FILL = 4 };
 struct Act {
   int na, nnz;
   int *crp, *cdiag, *arow, *flagF, *flagS, *ccol, *csrc;
-  bool onewarp;      // sparse factor/solve by one warp (small systems)
+  bool onewarp;      // sparse solve by one warp
+  bool onewarp_f;    // sparse factorization by one warp
   bool tile;         // tile_rows > 0
   int tile_rows;     // 0, 32 or 64: dense tile factorization, register-resident solve
   double *cval, *xs, *wbuf;  // sparse path only: L\U values in CSR order, multi-warp scratch
+  double *rdg;       // sparse path only: 1 / U(c, c) of each factored row
   double *jval;      // [nnz] Jacobian value of each position (the reference's 1e-99 + contributions)
   uint8_t *jflag;    // [nnz] JF_* flags; JF_SET is cleared when a level drops the entry
   double *anc;       // [na] mass number of active row c
@@ -69,9 +74,11 @@ __device__ __forceinline__ void act_bind(Act &A, char *base, int na, int nnz, in
   if (tile_rows == 0) {
     A.cval = (double *)p; p += a16((size_t)nnz * 8);
     A.wbuf = (double *)p; p += a16((size_t)nwarps * na * 8);
+    A.rdg = (double *)p; p += a16((size_t)na * 8);
   } else {
     A.cval = nullptr;
     A.wbuf = nullptr;
+    A.rdg = nullptr;
   }
   A.xs = (double *)p; p += a16((size_t)na * 8);
   A.jval = (double *)p; p += a16((size_t)nnz * 8);
@@ -200,6 +207,7 @@ __device__ void dev_compact(const DevNet &N, const Ws &W, Act &A, char *smem, si
   }
   __syncthreads();
   A.onewarp = na <= (N.kn.lu_onewarp_max > 0 ? N.kn.lu_onewarp_max : kOneWarpMax);
+  A.onewarp_f = na <= (N.kn.lu_onewarp_max > 0 ? N.kn.lu_onewarp_max : kOneWarpFactorMax);
 }
 
 // One reaction's contribution to Jacobian slot s (jac_rhs.F90:355-392) and whether it sets the
@@ -561,11 +569,11 @@ __device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h
   }
   for (int p = tid; p < A.nnz; p += nt) A.cval[p] = assemble_entry(A, p, h);
   __syncthreads();
-  if (A.onewarp) {  // one warp, rows in order
+  if (A.onewarp_f) {  // one warp, rows in order
     int bad = 0;
     if (w == 0) {
       const int *crp = A.crp, *cdiag = A.cdiag, *ccol = A.ccol;  // plain: rewritten per Jacobian
-      double *cval = A.cval, *wb = A.wbuf;
+      double *cval = A.cval, *wb = A.wbuf, *rdg = A.rdg;
       for (int c = 0; c < na; ++c) {
         const int rs = crp[c], re = crp[c + 1], dg = cdiag[c];
         for (int p = rs + lane; p < re; p += 32) wb[ccol[p]] = cval[p];
@@ -574,7 +582,7 @@ __device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h
           const int j = ccol[p];
           const double a = wb[j];
           if (a != 0.0) {
-            const double l = a * (1.0 / cval[cdiag[j]]);
+            const double l = a * rdg[j];
             const int qe = crp[j + 1];
             for (int q = cdiag[j] + 1 + lane; q < qe; q += 32) wb[ccol[q]] -= l * cval[q];
             __syncwarp();
@@ -585,6 +593,8 @@ __device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h
         for (int p = rs + lane; p < re; p += 32) cval[p] = wb[ccol[p]];
         __syncwarp();
         bad |= !pivot_ok(cval[dg]);
+        if (lane == 0) rdg[c] = 1.0 / cval[dg];
+        __syncwarp();
       }
     }
     return __syncthreads_or(bad) == 0;
@@ -602,7 +612,7 @@ __device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h
       __syncwarp();
       const double a = wb[j];
       if (a != 0.0) {
-        const double l = a * (1.0 / A.cval[A.cdiag[j]]);
+        const double l = a * A.rdg[j];
         const int qe = A.crp[j + 1];
         for (int q = A.cdiag[j] + 1 + lane; q < qe; q += 32) wb[A.ccol[q]] -= l * A.cval[q];
         __syncwarp();
@@ -613,6 +623,7 @@ __device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h
     for (int p = rs + lane; p < re; p += 32) A.cval[p] = wb[A.ccol[p]];
     __syncwarp();
     if (!pivot_ok(A.cval[dg])) ok = false;
+    if (lane == 0) A.rdg[c] = 1.0 / A.cval[dg];
     __threadfence_block();
     __syncwarp();
     if (lane == 0) *(volatile int *)&A.flagF[c] = gen;

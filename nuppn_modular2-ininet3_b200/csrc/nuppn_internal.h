@@ -127,12 +127,12 @@ NUPPN_HD inline int tile_rows_for(int na, int limit) {
 
 // Bytes of the active-subsystem LU for na rows, nnz entries, nwarps warps and a tile of tile_rows
 // rows (see active_lu.cuh): int crp[na+1], cdiag[na], arow[na], flagF[na], flagS[na], ccol[nnz],
-// csrc[nnz]; without a tile double cval[nnz], wbuf[nwarps*na]; double xs[na], jval[nnz], anc[na],
+// csrc[nnz]; without a tile double cval[nnz], wbuf[nwarps*na], rdg[na]; double xs[na], jval[nnz], anc[na],
 // xnc[na+1]; uint8 jflag[nnz]; with a tile double T[na * tile_rows] (na columns of tile_rows rows),
 // rinv[tile_rows]. Every array 16-byte aligned.
 NUPPN_HD inline size_t act_bytes(int na, int nnz, int nwarps, int tile_rows) {
   size_t b = a16((size_t)(na + 1) * 4) + 4 * a16((size_t)na * 4) + 2 * a16((size_t)nnz * 4);
-  if (tile_rows == 0) b += a16((size_t)nnz * 8) + a16((size_t)nwarps * na * 8);
+  if (tile_rows == 0) b += a16((size_t)nnz * 8) + a16((size_t)nwarps * na * 8) + a16((size_t)na * 8);
   b += a16((size_t)na * 8);
   b += a16((size_t)nnz * 8) + a16((size_t)na * 8) + a16((size_t)(na + 1) * 8) + a16((size_t)nnz);
   b += (size_t)na * tile_rows * 8 + (size_t)tile_rows * 8;
