@@ -557,6 +557,9 @@ namespace nuppn {
 // ---------------------------------------------------------------------------------------------
 // kernels: persistent CTAs, one zone at a time, workspace slab per CTA; dynamic shared memory holds
 // the active-subsystem LU when it fits (act_smem bytes).
+// kTraj: tppnp's trajectory loop per zone (IntegrateArgs::npts > 0); a separate instantiation so the
+// single-interval kernel keeps its own register allocation.
+template <bool kTraj>
 __global__ void __launch_bounds__(256, 3) k_integrate(const __grid_constant__ DevNet N, const __grid_constant__ WsLayout L,
                                                    char *ws, const __grid_constant__ IntegrateArgs A, int act_smem) {
   extern __shared__ __align__(16) char smem_dyn[];
@@ -584,7 +587,7 @@ __global__ void __launch_bounds__(256, 3) k_integrate(const __grid_constant__ De
     nse_reset(C.nse);
     double ye = A.ye[z];
     int ierr, fail = -1;
-    if (A.npts > 0) {
+    if (kTraj) {
       // the trajectory loop of tppnp (tppnp.F90:131-168) for this zone
       const double *tt = A.tr_time + (size_t)z * A.npts, *tp = A.tr_t9 + (size_t)z * A.npts;
       const double *tr = A.tr_rho + (size_t)z * A.npts;
@@ -677,7 +680,8 @@ __global__ void __launch_bounds__(256) k_phase(const __grid_constant__ DevNet N,
 
 cudaError_t launch_integrate(const DevNet &N, const WsLayout &L, char *ws, int grid, int block, int act_smem,
                              const IntegrateArgs &A, cudaStream_t st) {
-  k_integrate<<<grid, block, act_smem, st>>>(N, L, ws, A, act_smem);
+  if (A.npts > 0) k_integrate<true><<<grid, block, act_smem, st>>>(N, L, ws, A, act_smem);
+  else k_integrate<false><<<grid, block, act_smem, st>>>(N, L, ws, A, act_smem);
   return cudaGetLastError();
 }
 
@@ -688,13 +692,15 @@ cudaError_t launch_phase(const DevNet &N, const WsLayout &L, char *ws, int grid,
 }
 
 cudaError_t configure_kernels(int act_smem) {
-  cudaError_t e = cudaFuncSetAttribute(k_integrate, cudaFuncAttributeMaxDynamicSharedMemorySize, act_smem);
+  cudaError_t e = cudaFuncSetAttribute(k_integrate<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, act_smem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_integrate<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, act_smem);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_phase, cudaFuncAttributeMaxDynamicSharedMemorySize, act_smem);
 }
 
 cudaError_t occupancy_integrate(int block, int act_smem, int *per_sm) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_integrate, block, act_smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_integrate<false>, block, act_smem);
 }
 
 }  // namespace nuppn
