@@ -449,7 +449,7 @@ __device__ bool tile_factor_block(double *T, double *rinv, int na) {
 // depend on x), forms the block's four final values from four broadcasts (the small triangle solved
 // redundantly), then applies the four columns to its rows. Each row sees exactly the operations of
 // the column-by-column order (column-oriented, like SuperLU's dgstrs; a zero entry is skipped); the
-// diagonal is applied as the reciprocal computed by the factorization.
+// diagonal is divided out (div_piv, from the reciprocal the factorization stored).
 template <int R>
 __device__ __forceinline__ double tile_row(const double (&x)[R], int r) {
   return (R == 1 || r < 32) ? x[0] : x[R - 1];
@@ -458,6 +458,24 @@ __device__ __forceinline__ double tile_row(const double (&x)[R], int r) {
 __device__ __forceinline__ double sub_nz(double x, double a, double v) {  // x - a*v, skipped for a == 0
   const double t = x - a * v;
   return a != 0.0 ? t : x;
+}
+
+// a / d rounded to nearest, as SuperLU's triangular solve divides by U(c, c) (dgstrs.c:248,
+// dmyblas2.c:139), formed from r = 1 / d (itself a rounded division) by one correction step of
+// Markstein's method (P. Markstein, IBM J. Res. Develop. 34(1), 1990): q0 = a r is within an ulp of
+// a / d, the residual e = a - d q0 is exact under an FMA, and q0 + e r is the correctly rounded
+// quotient. The theorem needs every intermediate normal; outside that range this divides. Multiplying
+// by r alone differs from the quotient by an ulp now and then, which is enough to change the step
+// control of an ill-conditioned system (a 1e10-scale cancellation of rows holding U entries near
+// 1e109 against x near 1e-99).
+__device__ __forceinline__ double div_piv(double a, double d, double r) {
+  const double q0 = a * r;
+  const double m = fabs(q0), n = fabs(a);
+  if (m > 1e-250 && m < 1e250 && n > 1e-250 && n < 1e250 && fabs(d) < 1e250) {
+    const double e = fma(-d, q0, a);
+    return fma(e, r, q0);
+  }
+  return a / d;
 }
 
 template <int R>
@@ -510,10 +528,11 @@ __device__ __forceinline__ void tile_solve_regs(const double *T, const double *r
     const double u2 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c - 1), (c - 1) & 31);
     const double u1 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c - 2), (c - 2) & 31);
     const double u0 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c - 3), (c - 3) & 31);
-    const double w3 = u3 * r3;
-    const double w2 = sub_nz(u2, e23, w3) * r2;
-    const double w1 = sub_nz(sub_nz(u1, e13, w3), e12, w2) * r1;
-    const double w0 = sub_nz(sub_nz(sub_nz(u0, e03, w3), e02, w2), e01, w1) * r0;
+    const double d3 = T[c * (S + 1)], d2 = T[(c - 1) * (S + 1)], d1 = T[(c - 2) * (S + 1)], d0 = T[(c - 3) * (S + 1)];
+    const double w3 = div_piv(u3, d3, r3);
+    const double w2 = div_piv(sub_nz(u2, e23, w3), d2, r2);
+    const double w1 = div_piv(sub_nz(sub_nz(u1, e13, w3), e12, w2), d1, r1);
+    const double w0 = div_piv(sub_nz(sub_nz(sub_nz(u0, e03, w3), e02, w2), e01, w1), d0, r0);
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       const int r = lane + 32 * i;
@@ -526,7 +545,7 @@ __device__ __forceinline__ void tile_solve_regs(const double *T, const double *r
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       a[i] = T[c * S + lane + 32 * i];
-      if (lane + 32 * i == c) x[i] *= ri[i];
+      if (lane + 32 * i == c) x[i] = div_piv(x[i], a[i], ri[i]);
     }
     const double xc = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
 #pragma unroll

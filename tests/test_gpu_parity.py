@@ -84,6 +84,70 @@ def test_reduced_solve_matches_superlu(solver_mod, abi, orc, net300, batch, tile
     assert err.max() < 1e-9, err
 
 
+@pytest.mark.parametrize("na", [11, 60], ids=["tile32", "tile64"])
+def test_tile_solve_divides_like_superlu(solver_mod, abi, net300, na):
+    """SuperLU's triangular solve divides by U(c, c) (dgstrs.c:248, dmyblas2.c:139). On a diagonal
+    system (only the diagonal entries set, dt = 1 so that 1 - dt J_cc is formed exactly as numpy forms
+    it) the tile path must return b / (1 - J_cc) bit for bit: quotients over 1e-280..1e280 with
+    pivots over 1e-14..1e250 of either sign."""
+    dev = _dev(solver_mod, net300, abi)
+    r, c, _ = dev.jac_pattern()
+    nz, nsp = 256, net300.nsp
+    rng = np.random.default_rng(na)
+    diag = np.nonzero((r == c) & net300.considerisotope[r].astype(bool))[0]
+    sp_diag = r[diag]  # species of each diagonal entry (considered species only)
+    jac = np.zeros((nz, r.size))
+    es = np.zeros((nz, r.size), np.uint8)
+    es[:, diag] = 1
+    d = rng.choice([-1.0, 1.0], size=(nz, diag.size)) * 10.0 ** rng.uniform(-14, 250, size=(nz, diag.size))
+    jac[:, diag] = 1.0 - d
+    piv = -jac[:, diag] + 1.0  # assemble_entry: J * (-dt) + 1 with dt = 1
+    mk = np.zeros((nz, nsp), np.uint8)
+    act = np.argsort(rng.random((nz, diag.size)), axis=1)[:, :na]
+    mk[np.arange(nz)[:, None], sp_diag[act]] = 1
+    b = rng.choice([-1.0, 1.0], size=(nz, nsp)) * 10.0 ** rng.uniform(-280, 280, size=(nz, nsp))
+    x = dev.solve_reduced(jac, es, mk, 1.0, b)
+    want = np.zeros((nz, nsp))
+    on = mk[:, sp_diag].astype(bool)
+    want[:, sp_diag] = np.where(on, b[:, sp_diag] / piv, 0.0)
+    bad = np.nonzero(x != want)
+    assert bad[0].size == 0, (bad[0].size, x[bad][:4], want[bad][:4])
+
+
+def test_trajectory_cooling_through_min_t9_matches_checker(solver_mod, abi, orc, wl):
+    """A trajectory interval where T9 falls from 0.0131 to 0.0085 (crossing min_t9_for_slv) with a
+    rate near 1e109 in its active system: the dynamic network has 11 species and the Bader-Deuflhard
+    error test hinges on a 1e10-scale cancellation in the back substitution (a dX/dt term against
+    U(r, c) x(c), both rounded products of the same factors), so the step only succeeds when the solve
+    rounds as SuperLU built without FMA does: products rounded before they are subtracted, and x(c)
+    divided by U(c, c) rather than multiplied by its reciprocal. Both LU paths must take the checker's
+    steps and end within 1e-6 of its abundances."""
+    net = wl.network(1107)
+    tr = wl.trajectory_batch(1024, net=net, npts=201)
+    tt, t9, rho = tr.grids()
+    z, k1 = 244, 191
+    kn = abi.default_knobs(integration_method=1)
+    ref = orc.Oracle(net, kn)
+    X = tr.X0[[z]].copy()
+    bd = np.zeros(1, np.int32)
+    for k in range(k1 + 1):
+        ye = np.array([ref.calculate_ye(X[0])])
+        a = (X, t9[z, k], t9[z, k + 1], rho[z, k], rho[z, k + 1], ye, tt[z, k + 1] - tt[z, k])
+        if k == k1:
+            break
+        X, _, ierr, _, bd = ref.integrate_network(*a, bd_state=bd)
+        assert ierr[0] == 0, k
+    Xr, _, ierr_r, st_r, _ = ref.integrate_network(*a, bd_state=bd.copy())
+    assert ierr_r[0] == 0
+    for tile in (0, -1):
+        dev = _dev(solver_mod, net, abi, integration_method=1, lu_tile_max=tile)
+        Xd, _, ierr, st, _ = dev.integrate_network(*a, bd_state=bd.copy())
+        assert ierr[0] == 0, (tile, st[0].nsucc, st[0].nfail)
+        assert (st[0].nsucc, st[0].nfail) == (st_r[0].nsucc, st_r[0].nfail), tile
+        rel, ab = _compare_X(Xd, Xr)
+        assert rel <= 1e-6 and ab <= 1e-15, (tile, rel, ab)
+
+
 def _compare_X(X, Xr):
     big = Xr > 1e-12
     rel = np.abs(X - Xr)[big] / Xr[big]
