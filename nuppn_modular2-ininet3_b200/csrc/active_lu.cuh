@@ -464,23 +464,27 @@ __device__ __forceinline__ double sub_nz(double x, double a, double v) {  // x -
 // dmyblas2.c:139), formed from r = 1 / d (itself a rounded division) by one correction step of
 // Markstein's method (P. Markstein, IBM J. Res. Develop. 34(1), 1990): q0 = a r is within an ulp of
 // a / d, the residual e = a - d q0 is exact under an FMA, and q0 + e r is the correctly rounded
-// quotient. The theorem needs every intermediate normal; outside that range this divides. Multiplying
-// by r alone differs from the quotient by an ulp now and then, which is enough to change the step
-// control of an ill-conditioned system (a 1e10-scale cancellation of rows holding U entries near
-// 1e109 against x near 1e-99).
-__device__ __forceinline__ double div_piv(double a, double d, double r) {
+// quotient. The theorem needs the residual exact and every intermediate normal, which holds for a,
+// q0 and d within [1e-280, 1e280] (the residual is exact down to |a| ~ 1e-292); a = +0 gives the
+// right signed zero as well. Otherwise `bad` is raised (a test off the dependency chain) and the
+// caller repeats the solve with plain division; -0 goes that way too (the correction would return
+// +0 for -0 / d, d > 0). Multiplying by r alone differs from the quotient by an ulp now and then,
+// which is enough to change the step control of an ill-conditioned system (a 1e10-scale
+// cancellation of rows holding U entries near 1e109 against x near 1e-99).
+template <bool kPlain>
+__device__ __forceinline__ double div_piv(double a, double d, double r, int &bad) {
+  if (kPlain) return a / d;
   const double q0 = a * r;
-  const double m = fabs(q0), n = fabs(a);
-  if (m > 1e-250 && m < 1e250 && n > 1e-250 && n < 1e250 && fabs(d) < 1e250) {
-    const double e = fma(-d, q0, a);
-    return fma(e, r, q0);
-  }
-  return a / d;
+  const double e = fma(-d, q0, a);
+  const double m = fabs(q0), n = fabs(a), dd = fabs(d);
+  const bool ok = (m > 1e-280 && m < 1e280 && n > 1e-280 && n < 1e280) || (a == 0.0 && !signbit(a));
+  bad |= !(ok && dd > 1e-280 && dd < 1e280);
+  return fma(e, r, q0);
 }
 
-template <int R>
-__device__ __forceinline__ void tile_solve_regs(const double *T, const double *rinv, int na, double (&x)[R],
-                                                const double (&ri)[R], int lane) {
+template <int R, bool kPlain>
+__device__ __forceinline__ void tile_solve_core(const double *T, const double *rinv, int na, double (&x)[R],
+                                                const double (&ri)[R], int lane, int &bad) {
   constexpr int S = 32 * R;
   int c = 0;
   for (; c + 4 < na; c += 4) {  // forward, columns c .. c+3 (the last column has no entries below)
@@ -529,10 +533,10 @@ __device__ __forceinline__ void tile_solve_regs(const double *T, const double *r
     const double u1 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c - 2), (c - 2) & 31);
     const double u0 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c - 3), (c - 3) & 31);
     const double d3 = T[c * (S + 1)], d2 = T[(c - 1) * (S + 1)], d1 = T[(c - 2) * (S + 1)], d0 = T[(c - 3) * (S + 1)];
-    const double w3 = div_piv(u3, d3, r3);
-    const double w2 = div_piv(sub_nz(u2, e23, w3), d2, r2);
-    const double w1 = div_piv(sub_nz(sub_nz(u1, e13, w3), e12, w2), d1, r1);
-    const double w0 = div_piv(sub_nz(sub_nz(sub_nz(u0, e03, w3), e02, w2), e01, w1), d0, r0);
+    const double w3 = div_piv<kPlain>(u3, d3, r3, bad);
+    const double w2 = div_piv<kPlain>(sub_nz(u2, e23, w3), d2, r2, bad);
+    const double w1 = div_piv<kPlain>(sub_nz(sub_nz(u1, e13, w3), e12, w2), d1, r1, bad);
+    const double w0 = div_piv<kPlain>(sub_nz(sub_nz(sub_nz(u0, e03, w3), e02, w2), e01, w1), d0, r0, bad);
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       const int r = lane + 32 * i;
@@ -545,12 +549,27 @@ __device__ __forceinline__ void tile_solve_regs(const double *T, const double *r
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       a[i] = T[c * S + lane + 32 * i];
-      if (lane + 32 * i == c) x[i] = div_piv(x[i], a[i], ri[i]);
+      if (lane + 32 * i == c) x[i] = div_piv<kPlain>(x[i], a[i], ri[i], bad);
     }
     const double xc = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
 #pragma unroll
     for (int i = 0; i < R; ++i)
       if (lane + 32 * i < c) x[i] = sub_nz(x[i], a[i], xc);
+  }
+}
+
+template <int R>
+__device__ __forceinline__ void tile_solve_regs(const double *T, const double *rinv, int na, double (&x)[R],
+                                                const double (&ri)[R], int lane) {
+  double x0[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) x0[i] = x[i];
+  int bad = 0;
+  tile_solve_core<R, false>(T, rinv, na, x, ri, lane, bad);
+  if (__any_sync(NUPPN_FULL, bad)) {  // an operand outside div_piv's range: divide
+#pragma unroll
+    for (int i = 0; i < R; ++i) x[i] = x0[i];
+    tile_solve_core<R, true>(T, rinv, na, x, ri, lane, bad);
   }
 }
 

@@ -88,8 +88,9 @@ def test_reduced_solve_matches_superlu(solver_mod, abi, orc, net300, batch, tile
 def test_tile_solve_divides_like_superlu(solver_mod, abi, net300, na):
     """SuperLU's triangular solve divides by U(c, c) (dgstrs.c:248, dmyblas2.c:139). On a diagonal
     system (only the diagonal entries set, dt = 1 so that 1 - dt J_cc is formed exactly as numpy forms
-    it) the tile path must return b / (1 - J_cc) bit for bit: quotients over 1e-280..1e280 with
-    pivots over 1e-14..1e250 of either sign."""
+    it) the tile path must return b / (1 - J_cc) bit for bit, signed zeros included: right-hand sides
+    of 0, -0 and 1e-300..1e300 with pivots over 1e-14..1e250 of either sign (inside and outside the
+    range of the reciprocal-based quotient)."""
     dev = _dev(solver_mod, net300, abi)
     r, c, _ = dev.jac_pattern()
     nz, nsp = 256, net300.nsp
@@ -105,12 +106,14 @@ def test_tile_solve_divides_like_superlu(solver_mod, abi, net300, na):
     mk = np.zeros((nz, nsp), np.uint8)
     act = np.argsort(rng.random((nz, diag.size)), axis=1)[:, :na]
     mk[np.arange(nz)[:, None], sp_diag[act]] = 1
-    b = rng.choice([-1.0, 1.0], size=(nz, nsp)) * 10.0 ** rng.uniform(-280, 280, size=(nz, nsp))
+    b = rng.choice([-1.0, 1.0], size=(nz, nsp)) * 10.0 ** rng.uniform(-300, 300, size=(nz, nsp))
+    b[:, ::7] = 0.0
+    b[:, 3::11] = -0.0
     x = dev.solve_reduced(jac, es, mk, 1.0, b)
     want = np.zeros((nz, nsp))
     on = mk[:, sp_diag].astype(bool)
     want[:, sp_diag] = np.where(on, b[:, sp_diag] / piv, 0.0)
-    bad = np.nonzero(x != want)
+    bad = np.nonzero(x.view(np.int64) != want.view(np.int64))  # signed zeros included
     assert bad[0].size == 0, (bad[0].size, x[bad][:4], want[bad][:4])
 
 
