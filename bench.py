@@ -158,7 +158,7 @@ def run_traj(args, rank, world, local):
     X0, ye0 = tr_all.X0[sel], tr_all.ye0[sel]
     cfg = {"workload": "tppnp-traj-1107 201 points to 10 s", "trajectories": args.nz * world,
            "trajectories_per_gpu": args.nz, "network_species": net.nsp, "integrator": "bader-deuflhard",
-           "lu": "fp64", "launches_per_step": 1}
+           "lu": "fp64", "launches_per_step": 2}
     if args.impl == "reference":
         if rank != 0:
             return

@@ -22,6 +22,8 @@ cudaError_t launch_integrate(const DevNet &N, const WsLayout &L, char *ws, int g
 cudaError_t launch_phase(const DevNet &N, const WsLayout &L, char *ws, int grid, int block, int act_smem,
                          const PhaseArgs &A, cudaStream_t st);
 cudaError_t configure_kernels(int act_smem);
+cudaError_t launch_zone_order(const double *key, const double *key_b, int stride, int nz, int *order,
+                              cudaStream_t st);
 cudaError_t occupancy_integrate(int block, int act_smem, int *per_sm);
 }  // namespace nuppn
 
@@ -64,7 +66,7 @@ struct nuppn_net {
   void *arena = nullptr;
   size_t arena_bytes = 0;
   WsLayout L;
-  DevBuf ws, stage, counter;
+  DevBuf ws, stage, counter, order;  // order: the zone schedule of the allocating entry points
   int ws_slots = 0;
   int block = 256;
   int act_smem = 72 * 1024;  // shared-memory budget per CTA for the active subsystem (3 CTAs per SM)
@@ -358,6 +360,7 @@ nuppn_status nuppn_net_destroy(nuppn_net *net) {
   net->ws.release();
   net->stage.release();
   net->counter.release();
+  net->order.release();
   delete net;
   return NUPPN_OK;
 }
@@ -369,7 +372,7 @@ nuppn_status nuppn_net_info_get(const nuppn_net *net, nuppn_net_info *info) {
   info->nnz_jac = H.nnzJ; info->nnz_lu = H.nnzLU; info->n_solve = H.nsys;
   info->levels_lower = (int)H.lvL_ptr.size() - 1; info->levels_upper = (int)H.lvU_ptr.size() - 1;
   info->lu_flops = H.lu_flops;
-  info->device_bytes = (int64_t)(net->arena_bytes + net->ws.n + net->stage.n + net->counter.n);
+  info->device_bytes = (int64_t)(net->arena_bytes + net->ws.n + net->stage.n + net->counter.n + net->order.n);
   return NUPPN_OK;
 }
 
@@ -577,13 +580,16 @@ nuppn_status nuppn_integrate_device(nuppn_net *net, int32_t nz, double *d_X, int
   st = ensure_ws(net, grid);
   if (st != NUPPN_OK) return st;
   cudaStream_t s = (cudaStream_t)stream;
+  CK(net->order.ensure((size_t)nz * 4));
   CK(cudaMemsetAsync(net->counter.p, 0, sizeof(int), s));
+  CK(launch_zone_order(d_t9_0, d_t9_1, 1, nz, (int *)net->order.p, s));
   IntegrateArgs A = {};
   A.nz = nz; A.ldx = ldx; A.X = d_X; A.t9_0 = d_t9_0; A.t9_1 = d_t9_1; A.rho_0 = d_rho_0; A.rho_1 = d_rho_1;
   A.dtwant = d_dtwant; A.ye = d_ye; A.ierr = d_ierr; A.stats = d_stats; A.bd_state = d_bd_state;
   A.counter = (int *)net->counter.p;
+  A.order = (const int *)net->order.p;
   CK(launch_integrate(net->D, net->L, (char *)net->ws.p, grid, net->block, net->act_smem, A, s));
-  net->launches++;
+  net->launches += 2;  // k_zone_order, k_integrate
   return NUPPN_OK;
 }
 
@@ -643,13 +649,16 @@ nuppn_status nuppn_integrate_trajectories_device(nuppn_net *net, int32_t nz, int
   st = ensure_ws(net, grid);
   if (st != NUPPN_OK) return st;
   cudaStream_t s = (cudaStream_t)stream;
+  CK(net->order.ensure((size_t)nz * 4));
   CK(cudaMemsetAsync(net->counter.p, 0, sizeof(int), s));
+  CK(launch_zone_order(d_t9, nullptr, npts, nz, (int *)net->order.p, s));
   IntegrateArgs A = {};
   A.nz = nz; A.ldx = ldx; A.X = d_X; A.ye = d_ye; A.ierr = d_ierr; A.stats = d_stats; A.bd_state = d_bd_state;
   A.counter = (int *)net->counter.p;
+  A.order = (const int *)net->order.p;
   A.npts = npts; A.tr_time = d_time; A.tr_t9 = d_t9; A.tr_rho = d_rho; A.tr_fail = d_fail;
   CK(launch_integrate(net->D, net->L, (char *)net->ws.p, grid, net->block, net->act_smem, A, s));
-  net->launches++;
+  net->launches += 2;  // k_zone_order, k_integrate
   return NUPPN_OK;
 }
 

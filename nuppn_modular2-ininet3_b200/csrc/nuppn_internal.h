@@ -163,6 +163,8 @@ struct IntegrateArgs {
   nuppn_zone_stats *stats;
   int *bd_state;
   int *counter;
+  // zone schedule: the k-th zone taken is order[k] (costliest first, see k_zone_order), or k if null
+  const int *order;
   // trajectory mode (npts > 0): per zone npts points of time, T9 and rho ([nz][npts]); tr_fail gets
   // the index of the interval that failed, or -1
   int npts;

@@ -569,7 +569,10 @@ __global__ void __launch_bounds__(256, 3) k_integrate(const __grid_constant__ De
   const Ws W = ws_bind(ws + (size_t)blockIdx.x * L.bytes, L);
   for (;;) {
     __syncthreads();
-    if (threadIdx.x == 0) zsh = atomicAdd(A.counter, 1);
+    if (threadIdx.x == 0) {
+      const int k = atomicAdd(A.counter, 1);
+      zsh = (k < A.nz && A.order) ? A.order[k] : k;
+    }
     __syncthreads();
     const int z = zsh;
     if (z >= A.nz) break;
@@ -676,6 +679,47 @@ __global__ void __launch_bounds__(256) k_phase(const __grid_constant__ DevNet N,
     }
     __syncthreads();
   }
+}
+
+// Zone schedule for k_integrate: a counting sort of the zones on log2 T9 (64 bins per octave over
+// 2^-12 .. 2^4), hottest first. Hot zones have the largest dynamic networks and the most rejected
+// steps, and a persistent kernel ends when its last zone does: starting the costliest zones first
+// keeps one of them from starting late and running alone at the end. key[z * stride] (and, if
+// key_b is given, the larger of it and key_b[z * stride]) is the zone's temperature. One CTA; the
+// order within a bin follows the atomics, which is harmless: a zone's result does not depend on
+// which CTA integrates it or when.
+constexpr int kOrderBins = 1024;
+__global__ void __launch_bounds__(1024) k_zone_order(const double *key, const double *key_b, int stride, int nz,
+                                                     int *order) {
+  __shared__ int cnt[kOrderBins];
+  for (int b = threadIdx.x; b < kOrderBins; b += blockDim.x) cnt[b] = 0;
+  __syncthreads();
+  auto bin_of = [&](int z) {
+    double t = key[(size_t)z * stride];
+    if (key_b) t = fmax(t, key_b[(size_t)z * stride]);
+    if (!(t > 0.0) || !isfinite(t)) return kOrderBins - 1;  // rejected by the kernel at once: last
+    const double u = (log2(t) + 12.0) * 64.0;
+    const int b = u <= 0.0 ? 0 : (u >= kOrderBins - 1 ? kOrderBins - 1 : (int)u);
+    return kOrderBins - 1 - b;  // hottest first
+  };
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) atomicAdd(&cnt[bin_of(z)], 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {  // exclusive offsets (1024 bins: a serial pass is a few microseconds)
+    int acc = 0;
+    for (int b = 0; b < kOrderBins; ++b) {
+      const int c = cnt[b];
+      cnt[b] = acc;
+      acc += c;
+    }
+  }
+  __syncthreads();
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) order[atomicAdd(&cnt[bin_of(z)], 1)] = z;
+}
+
+cudaError_t launch_zone_order(const double *key, const double *key_b, int stride, int nz, int *order,
+                              cudaStream_t st) {
+  k_zone_order<<<1, 1024, 0, st>>>(key, key_b, stride, nz, order);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_integrate(const DevNet &N, const WsLayout &L, char *ws, int grid, int block, int act_smem,
