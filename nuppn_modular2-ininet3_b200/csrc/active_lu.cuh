@@ -46,6 +46,14 @@ struct Act {
   double *anc;       // [na] mass number of active row c
   double *xnc;       // [na+1] molar abundances of the active rows; xnc[na] = 1 (gamma)
   double *T, *rinv;  // tile: T[c*tile_rows + r] = entry (r, c) of L\U; rinv[r] = 1 / U(r, r)
+  // mixed precision (lu_precision = 1, tile systems): T keeps I - hJ unfactored in FP64 for the
+  // refinement residuals; T32 / rinv32 hold the FP32 factor of diag(srow) (I - hJ) diag(scol)
+  bool mixed;        // the tile has the mixed-precision arrays
+  bool mixed_now;    // the current factorization is the FP32 one (false after an FP32 pivot failure)
+  float *T32, *rinv32;
+  double *srow, *scol;
+  int ir_max;        // knobs ir_max_iters, ir_rtol
+  double ir_rtol;
   int genF, genS;
   bool in_smem;
   // reactions of the step (see dev_active_reactions), in the CTA's workspace
@@ -62,7 +70,7 @@ struct Act {
   bool rhs_in_smem;
 };
 
-__device__ __forceinline__ void act_bind(Act &A, char *base, int na, int nnz, int nwarps, int tile_rows) {
+__device__ __forceinline__ void act_bind(Act &A, char *base, int na, int nnz, int nwarps, int tile_rows, bool mixed) {
   char *p = base;
   A.crp = (int *)p; p += a16((size_t)(na + 1) * 4);
   A.cdiag = (int *)p; p += a16((size_t)na * 4);
@@ -89,10 +97,22 @@ __device__ __forceinline__ void act_bind(Act &A, char *base, int na, int nnz, in
   A.tile = tile_rows > 0;
   if (A.tile) {
     A.T = (double *)p; p += (size_t)na * tile_rows * 8;
-    A.rinv = (double *)p;
+    A.rinv = (double *)p; p += (size_t)tile_rows * 8;
   } else {
     A.T = nullptr;
     A.rinv = nullptr;
+  }
+  A.mixed = mixed && A.tile;
+  A.mixed_now = false;
+  if (A.mixed) {
+    A.T32 = (float *)p; p += (size_t)na * tile_rows * 4;
+    A.rinv32 = (float *)p; p += a16((size_t)tile_rows * 4);
+    A.srow = (double *)p; p += (size_t)tile_rows * 8;
+    A.scol = (double *)p;
+  } else {
+    A.T32 = nullptr;
+    A.rinv32 = nullptr;
+    A.srow = A.scol = nullptr;
   }
 }
 
@@ -171,11 +191,14 @@ __device__ void dev_compact(const DevNet &N, const Ws &W, Act &A, char *smem, si
   __syncthreads();
   const int nnz = block_scan_excl(cnt, na, sint);
   const int trows = tile_rows_for(na, N.kn.lu_tile_max);
-  const size_t need = act_bytes(na, nnz, nw, trows);
+  const bool mixed = N.kn.lu_precision == 1 && trows > 0;
+  const size_t need = act_bytes(na, nnz, nw, trows, mixed);
   A.na = na;
   A.nnz = nnz;
   A.in_smem = need <= smem_bytes;
-  act_bind(A, A.in_smem ? smem : W.act, na, nnz, nw, trows);
+  act_bind(A, A.in_smem ? smem : W.act, na, nnz, nw, trows, mixed);
+  A.ir_max = N.kn.ir_max_iters;
+  A.ir_rtol = N.kn.ir_rtol;
   A.genF = 0;
   A.genS = 0;
   for (int c = tid; c < na; c += nt) {
@@ -394,6 +417,7 @@ __device__ __forceinline__ double assemble_entry(Act &A, int p, double h) {
 }
 
 __device__ __forceinline__ bool pivot_ok(double d) { return d != 0.0 && isfinite(d); }
+__device__ __forceinline__ bool pivot_ok(float d) { return d != 0.0f && isfinite(d); }
 
 // Right-looking elimination of a dense tile by all warps of the CTA. At pivot k every warp forms
 // the multipliers l_r = a_rk / a_kk of the rows below in registers (lane l owns rows l + 32 i) and
@@ -401,35 +425,36 @@ __device__ __forceinline__ bool pivot_ok(double d) { return d != 0.0 && isfinite
 // left unscaled during the elimination and scaled at the end by the stored reciprocal, the same
 // product a_rk * (1 / a_kk) that SuperLU forms (dpivotL.c:178-180). Returns false on a zero or
 // non-finite pivot.
-template <int R>
-__device__ bool tile_factor_block(double *T, double *rinv, int na) {
+// F = double for the FP64 factor; F = float for the FP32 factor of the mixed-precision mode.
+template <int R, typename F = double>
+__device__ bool tile_factor_block(F *T, F *rinv, int na) {
   constexpr int S = 32 * R;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   int bad = 0;
   for (int k = 0; k < na; ++k) {
-    const double piv = T[k * (S + 1)];
+    const F piv = T[k * (S + 1)];
     bad |= !pivot_ok(piv);
-    const double rp = 1.0 / piv;
+    const F rp = F(1) / piv;
     if (threadIdx.x == 0) rinv[k] = rp;
-    double l[R];
+    F l[R];
     bool any = false;
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       const int r = lane + 32 * i;
-      l[i] = 0.0;
+      l[i] = F(0);
       if (r > k && r < na) {
-        const double a = T[k * S + r];
-        l[i] = a != 0.0 ? a * rp : 0.0;
+        const F a = T[k * S + r];
+        l[i] = a != F(0) ? a * rp : F(0);
       }
-      any |= l[i] != 0.0;
+      any |= l[i] != F(0);
     }
     if (__any_sync(NUPPN_FULL, any)) {
 #pragma unroll 2
       for (int m = k + 1 + w; m < na; m += nw) {
-        const double u = T[m * S + k];
+        const F u = T[m * S + k];
 #pragma unroll
         for (int i = 0; i < R; ++i)
-          if (l[i] != 0.0) T[m * S + lane + 32 * i] -= l[i] * u;
+          if (l[i] != F(0)) T[m * S + lane + 32 * i] -= l[i] * u;
       }
     }
     __syncthreads();
@@ -437,11 +462,47 @@ __device__ bool tile_factor_block(double *T, double *rinv, int na) {
   for (int i = threadIdx.x; i < na * S; i += blockDim.x) {  // L columns: a_rk * (1 / a_kk)
     const int c = i / S, r = i - c * S;
     if (r > c && r < na) {
-      const double a = T[i];
-      if (a != 0.0) T[i] = a * rinv[c];
+      const F a = T[i];
+      if (a != F(0)) T[i] = a * rinv[c];
     }
   }
   return __syncthreads_or(bad) == 0;
+}
+
+// Power of two that brings |m| into [1, 2) (1 for 0 or non-finite m).
+__device__ __forceinline__ double pow2_scale(double m) {
+  return (m > 0.0 && isfinite(m)) ? ldexp(1.0, -ilogb(m)) : 1.0;
+}
+
+// Mixed-precision factorization of the assembled tile T (I - hJ, FP64, left unfactored): columns,
+// then rows, are scaled by powers of two to a largest entry in [1, 2) (exact in FP64; active
+// systems hold entries from ~1e-99 to ~1e110, beyond FP32's range), the scaled matrix is rounded to
+// FP32 and factored there. Entries that underflow FP32 become zeros of the FP32 factor only; the
+// FP64 residuals of the refinement still see them. Returns false on a zero or non-finite FP32 pivot.
+template <int R>
+__device__ bool tile_factor_mixed(Act &A, int na) {
+  constexpr int S = 32 * R;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
+  const double *T = A.T;
+  for (int c = w; c < na; c += nw) {  // column scales (columns are contiguous)
+    double m = 0.0;
+    for (int r = lane; r < na; r += 32) m = fmax(m, fabs(T[c * S + r]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(NUPPN_FULL, m, o));
+    if (lane == 0) A.scol[c] = pow2_scale(m);
+  }
+  __syncthreads();
+  for (int r = tid; r < na; r += nt) {  // row scales of the column-scaled matrix
+    double m = 0.0;
+    for (int c = 0; c < na; ++c) m = fmax(m, fabs(T[c * S + r]) * A.scol[c]);
+    A.srow[r] = pow2_scale(m);
+  }
+  __syncthreads();
+  for (int i = tid; i < na * S; i += nt) {
+    const int c = i / S, r = i - c * S;
+    A.T32[i] = r < na ? (float)(T[i] * A.scol[c] * A.srow[r]) : 0.0f;
+  }
+  __syncthreads();
+  return tile_factor_block<R, float>(A.T32, A.rinv32, na);
 }
 
 // Forward and backward substitution of a factored tile by one warp, x[i] holding row lane + 32 i.
@@ -450,14 +511,18 @@ __device__ bool tile_factor_block(double *T, double *rinv, int na) {
 // redundantly), then applies the four columns to its rows. Each row sees exactly the operations of
 // the column-by-column order (column-oriented, like SuperLU's dgstrs; a zero entry is skipped); the
 // diagonal is divided out (div_piv, from the reciprocal the factorization stored).
-template <int R>
-__device__ __forceinline__ double tile_row(const double (&x)[R], int r) {
+template <int R, typename F>
+__device__ __forceinline__ F tile_row(const F (&x)[R], int r) {
   return (R == 1 || r < 32) ? x[0] : x[R - 1];
 }
 
 __device__ __forceinline__ double sub_nz(double x, double a, double v) {  // x - a*v, skipped for a == 0
   const double t = x - a * v;
   return a != 0.0 ? t : x;
+}
+__device__ __forceinline__ float sub_nz(float x, float a, float v) {
+  const float t = x - a * v;
+  return a != 0.0f ? t : x;
 }
 
 // a / d rounded to nearest, as SuperLU's triangular solve divides by U(c, c) (dgstrs.c:248,
@@ -472,6 +537,10 @@ __device__ __forceinline__ double sub_nz(double x, double a, double v) {  // x -
 // which is enough to change the step control of an ill-conditioned system (a 1e10-scale
 // cancellation of rows holding U entries near 1e109 against x near 1e-99).
 template <bool kPlain>
+__device__ __forceinline__ float div_piv(float a, float d, float r, int &) {  // FP32 factor: refined
+  return a * r;
+}
+template <bool kPlain>
 __device__ __forceinline__ double div_piv(double a, double d, double r, int &bad) {
   if (kPlain) return a / d;
   const double q0 = a * r;
@@ -482,76 +551,76 @@ __device__ __forceinline__ double div_piv(double a, double d, double r, int &bad
   return fma(e, r, q0);
 }
 
-template <int R, bool kPlain>
-__device__ __forceinline__ void tile_solve_core(const double *T, const double *rinv, int na, double (&x)[R],
-                                                const double (&ri)[R], int lane, int &bad) {
+template <int R, bool kPlain, typename F = double>
+__device__ __forceinline__ void tile_solve_core(const F *T, const F *rinv, int na, F (&x)[R], const F (&ri)[R],
+                                                int lane, int &bad) {
   constexpr int S = 32 * R;
   int c = 0;
   for (; c + 4 < na; c += 4) {  // forward, columns c .. c+3 (the last column has no entries below)
-    double a[R][4];
+    F a[R][4];
 #pragma unroll
     for (int i = 0; i < R; ++i)
 #pragma unroll
       for (int k = 0; k < 4; ++k) a[i][k] = T[(c + k) * S + lane + 32 * i];
-    const double l10 = T[c * S + c + 1], l20 = T[c * S + c + 2], l30 = T[c * S + c + 3];
-    const double l21 = T[(c + 1) * S + c + 2], l31 = T[(c + 1) * S + c + 3], l32 = T[(c + 2) * S + c + 3];
-    const double v0 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
-    const double u1 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c + 1), (c + 1) & 31);
-    const double u2 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c + 2), (c + 2) & 31);
-    const double u3 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c + 3), (c + 3) & 31);
-    const double v1 = sub_nz(u1, l10, v0);
-    const double v2 = sub_nz(sub_nz(u2, l20, v0), l21, v1);
-    const double v3 = sub_nz(sub_nz(sub_nz(u3, l30, v0), l31, v1), l32, v2);
+    const F l10 = T[c * S + c + 1], l20 = T[c * S + c + 2], l30 = T[c * S + c + 3];
+    const F l21 = T[(c + 1) * S + c + 2], l31 = T[(c + 1) * S + c + 3], l32 = T[(c + 2) * S + c + 3];
+    const F v0 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
+    const F u1 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c + 1), (c + 1) & 31);
+    const F u2 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c + 2), (c + 2) & 31);
+    const F u3 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c + 3), (c + 3) & 31);
+    const F v1 = sub_nz(u1, l10, v0);
+    const F v2 = sub_nz(sub_nz(u2, l20, v0), l21, v1);
+    const F v3 = sub_nz(sub_nz(sub_nz(u3, l30, v0), l31, v1), l32, v2);
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       const int r = lane + 32 * i;
-      const double t = sub_nz(sub_nz(sub_nz(sub_nz(x[i], a[i][0], v0), a[i][1], v1), a[i][2], v2), a[i][3], v3);
+      const F t = sub_nz(sub_nz(sub_nz(sub_nz(x[i], a[i][0], v0), a[i][1], v1), a[i][2], v2), a[i][3], v3);
       x[i] = r == c + 1 ? v1 : r == c + 2 ? v2 : r == c + 3 ? v3 : (r > c + 3 ? t : x[i]);
     }
   }
   for (; c < na - 1; ++c) {
-    double a[R];
+    F a[R];
 #pragma unroll
     for (int i = 0; i < R; ++i) a[i] = T[c * S + lane + 32 * i];
-    const double xc = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
+    const F xc = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
 #pragma unroll
     for (int i = 0; i < R; ++i)
       if (lane + 32 * i > c) x[i] = sub_nz(x[i], a[i], xc);
   }
   c = na - 1;
   for (; c >= 3; c -= 4) {  // backward, columns c, c-1, c-2, c-3
-    double a[R][4];
+    F a[R][4];
 #pragma unroll
     for (int i = 0; i < R; ++i)
 #pragma unroll
       for (int k = 0; k < 4; ++k) a[i][k] = T[(c - k) * S + lane + 32 * i];
-    const double r3 = rinv[c], r2 = rinv[c - 1], r1 = rinv[c - 2], r0 = rinv[c - 3];
-    const double e23 = T[c * S + c - 1], e13 = T[c * S + c - 2], e03 = T[c * S + c - 3];
-    const double e12 = T[(c - 1) * S + c - 2], e02 = T[(c - 1) * S + c - 3], e01 = T[(c - 2) * S + c - 3];
-    const double u3 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
-    const double u2 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c - 1), (c - 1) & 31);
-    const double u1 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c - 2), (c - 2) & 31);
-    const double u0 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c - 3), (c - 3) & 31);
-    const double d3 = T[c * (S + 1)], d2 = T[(c - 1) * (S + 1)], d1 = T[(c - 2) * (S + 1)], d0 = T[(c - 3) * (S + 1)];
-    const double w3 = div_piv<kPlain>(u3, d3, r3, bad);
-    const double w2 = div_piv<kPlain>(sub_nz(u2, e23, w3), d2, r2, bad);
-    const double w1 = div_piv<kPlain>(sub_nz(sub_nz(u1, e13, w3), e12, w2), d1, r1, bad);
-    const double w0 = div_piv<kPlain>(sub_nz(sub_nz(sub_nz(u0, e03, w3), e02, w2), e01, w1), d0, r0, bad);
+    const F r3 = rinv[c], r2 = rinv[c - 1], r1 = rinv[c - 2], r0 = rinv[c - 3];
+    const F e23 = T[c * S + c - 1], e13 = T[c * S + c - 2], e03 = T[c * S + c - 3];
+    const F e12 = T[(c - 1) * S + c - 2], e02 = T[(c - 1) * S + c - 3], e01 = T[(c - 2) * S + c - 3];
+    const F u3 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
+    const F u2 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c - 1), (c - 1) & 31);
+    const F u1 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c - 2), (c - 2) & 31);
+    const F u0 = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c - 3), (c - 3) & 31);
+    const F d3 = T[c * (S + 1)], d2 = T[(c - 1) * (S + 1)], d1 = T[(c - 2) * (S + 1)], d0 = T[(c - 3) * (S + 1)];
+    const F w3 = div_piv<kPlain>(u3, d3, r3, bad);
+    const F w2 = div_piv<kPlain>(sub_nz(u2, e23, w3), d2, r2, bad);
+    const F w1 = div_piv<kPlain>(sub_nz(sub_nz(u1, e13, w3), e12, w2), d1, r1, bad);
+    const F w0 = div_piv<kPlain>(sub_nz(sub_nz(sub_nz(u0, e03, w3), e02, w2), e01, w1), d0, r0, bad);
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       const int r = lane + 32 * i;
-      const double t = sub_nz(sub_nz(sub_nz(sub_nz(x[i], a[i][0], w3), a[i][1], w2), a[i][2], w1), a[i][3], w0);
+      const F t = sub_nz(sub_nz(sub_nz(sub_nz(x[i], a[i][0], w3), a[i][1], w2), a[i][2], w1), a[i][3], w0);
       x[i] = r == c ? w3 : r == c - 1 ? w2 : r == c - 2 ? w1 : r == c - 3 ? w0 : (r < c - 3 ? t : x[i]);
     }
   }
   for (; c >= 0; --c) {
-    double a[R];
+    F a[R];
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       a[i] = T[c * S + lane + 32 * i];
       if (lane + 32 * i == c) x[i] = div_piv<kPlain>(x[i], a[i], ri[i], bad);
     }
-    const double xc = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
+    const F xc = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
 #pragma unroll
     for (int i = 0; i < R; ++i)
       if (lane + 32 * i < c) x[i] = sub_nz(x[i], a[i], xc);
@@ -573,6 +642,67 @@ __device__ __forceinline__ void tile_solve_regs(const double *T, const double *r
   }
 }
 
+// Mixed-precision solve of (I - hJ) x = b by the calling warp, b in x on entry (rows lane + 32 i):
+// x = 0, r = b; repeat: dx = scol * FP32-solve(srow * r * 2^-e) * 2^e (2^-e brings the scaled
+// residual's largest entry into [1, 2), so it stays in FP32's range), x += dx, stop after
+// ir_max_iters corrections or when max|dx| <= ir_rtol * max|x|, else r = b - (I - hJ) x in FP64 from
+// the unfactored tile. Returns the number of FP64 residuals formed (the refinement sweeps).
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(NUPPN_FULL, v, o));
+  return v;
+}
+template <int R>
+__device__ int tile_solve_mixed(const Act &A, double (&x)[R], int lane) {
+  constexpr int S = 32 * R;
+  const int na = A.na;
+  double b[R], sr[R], sc[R], r[R];
+  float ri[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int row = lane + 32 * i;
+    const bool on = row < na;
+    b[i] = on ? x[i] : 0.0;
+    r[i] = b[i];
+    sr[i] = on ? A.srow[row] : 0.0;
+    sc[i] = on ? A.scol[row] : 0.0;
+    ri[i] = on ? A.rinv32[row] : 0.0f;
+    x[i] = 0.0;
+  }
+  int sweeps = 0;
+  for (int it = 0;; ++it) {
+    double m = 0.0;
+#pragma unroll
+    for (int i = 0; i < R; ++i) m = fmax(m, fabs(r[i] * sr[i]));
+    m = warp_max(m);
+    if (!(m > 0.0) || !isfinite(m)) break;  // exact (r = 0), or nothing left to refine
+    const int e = ilogb(m);
+    float f[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) f[i] = (float)ldexp(r[i] * sr[i], -e);
+    int bad = 0;
+    tile_solve_core<R, false, float>(A.T32, A.rinv32, na, f, ri, lane, bad);
+    double dm = 0.0, xm = 0.0;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const double dx = ldexp((double)f[i], e) * sc[i];
+      x[i] += dx;
+      dm = fmax(dm, fabs(dx));
+      xm = fmax(xm, fabs(x[i]));
+    }
+    if (it >= A.ir_max || warp_max(dm) <= A.ir_rtol * warp_max(xm)) break;
+    // r = b - (I - hJ) x, row-oriented over the unfactored FP64 tile
+#pragma unroll
+    for (int i = 0; i < R; ++i) r[i] = b[i];
+    for (int c = 0; c < na; ++c) {
+      const double xc = __shfl_sync(NUPPN_FULL, tile_row<R>(x, c), c & 31);
+#pragma unroll
+      for (int i = 0; i < R; ++i) r[i] = sub_nz(r[i], A.T[c * S + lane + 32 * i], xc);
+    }
+    ++sweeps;
+  }
+  return sweeps;
+}
+
 // Tile solve in place on A.xs by the calling warp.
 template <int R>
 __device__ void tile_solve_xs(const Act &A, int lane) {
@@ -583,7 +713,8 @@ __device__ void tile_solve_xs(const Act &A, int lane) {
     x[i] = r < A.na ? A.xs[r] : 0.0;
     ri[i] = r < A.na ? A.rinv[r] : 0.0;
   }
-  tile_solve_regs<R>(A.T, A.rinv, A.na, x, ri, lane);
+  if (A.mixed_now) tile_solve_mixed<R>(A, x, lane);
+  else tile_solve_regs<R>(A.T, A.rinv, A.na, x, ri, lane);
 #pragma unroll
   for (int i = 0; i < R; ++i)
     if (lane + 32 * i < A.na) A.xs[lane + 32 * i] = x[i];
@@ -603,6 +734,10 @@ __device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h
     for (int c = w; c < na; c += nw)
       for (int p = A.crp[c] + lane; p < A.crp[c + 1]; p += 32) T[A.ccol[p] * S + c] = assemble_entry(A, p, h);
     __syncthreads();
+    if (A.mixed) {
+      A.mixed_now = S == 32 ? tile_factor_mixed<1>(A, na) : tile_factor_mixed<2>(A, na);
+      if (A.mixed_now) return true;  // otherwise factor in FP64 (T is still unfactored)
+    }
     return S == 32 ? tile_factor_block<1>(T, A.rinv, na) : tile_factor_block<2>(T, A.rinv, na);
   }
   for (int p = tid; p < A.nnz; p += nt) A.cval[p] = assemble_entry(A, p, h);
@@ -820,7 +955,7 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
   }
   __syncthreads();
   const int ngi = block_scan_excl(cnt, na, sint);
-  const size_t lu_need = act_bytes(na, A.nnz, nw, A.tile_rows), need = rhs_bytes(na, ngi);
+  const size_t lu_need = act_bytes(na, A.nnz, nw, A.tile_rows, A.mixed), need = rhs_bytes(na, ngi);
   char *base;
   if (A.in_smem && lu_need + need <= smem_bytes) {
     base = smem + lu_need;

@@ -335,9 +335,9 @@ nuppn_status nuppn_net_create(const nuppn_net_desc *desc, const nuppn_knobs *kno
   net->nsm = prop.multiProcessorCount;
   net->block = kn.threads_per_zone > 0 ? kn.threads_per_zone : 256;
   if (net->block % 32 || net->block > 256) { delete net; set_error("threads_per_zone must be a multiple of 32, <= 256"); return NUPPN_ERR_ARG; }
-  if (kn.lu_precision != 0) {
+  if (kn.lu_precision != 0 && kn.lu_precision != 1) {
     delete net;
-    set_error("lu_precision: only 0 (FP64 factorization) is available in this build");
+    set_error("lu_precision must be 0 (FP64) or 1 (FP32 factor + FP64 refinement)");
     return NUPPN_ERR_ARG;
   }
   nuppn_status st = upload(net);
@@ -378,8 +378,8 @@ nuppn_status nuppn_net_info_get(const nuppn_net *net, nuppn_net_info *info) {
 
 nuppn_status nuppn_set_knobs(nuppn_net *net, const nuppn_knobs *knobs) {
   if (!net || !knobs) return NUPPN_ERR_ARG;
-  if (knobs->lu_precision != 0) {
-    set_error("lu_precision 1 is not available in this build");
+  if (knobs->lu_precision != 0 && knobs->lu_precision != 1) {
+    set_error("lu_precision must be 0 (FP64) or 1 (FP32 factor + FP64 refinement)");
     return NUPPN_ERR_ARG;
   }
   if (knobs->i_nse == 1 && (net->H.nse_iprot < 0 || net->H.nse_ini56 < 0)) {

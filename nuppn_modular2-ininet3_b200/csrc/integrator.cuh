@@ -196,9 +196,10 @@ __device__ int dev_bd_substep(const DevNet &N, const Ws &W, ZoneCtl &C, const Bd
 // dev_bd_substep. Leaves y_k / delta_k in B.yk / B.dk; returns 0 or HUGE_ABUNDS.
 template <int R>
 __device__ int bd_level_tile(const Act &A, const BdVec &B, double h, int nseq, bool huge_frozen, int &nsolve,
-                             int *sflag) {
+                             int &ir_sweeps, int *sflag) {
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, na = A.na;
   double y[R], d[R], ri[R], an[R];
+  int sweeps = 0;  // refinement sweeps (mixed precision), counted by warp 0
   if (w == 0) {
 #pragma unroll
     for (int i = 0; i < R; ++i) {
@@ -213,6 +214,7 @@ __device__ int bd_level_tile(const Act &A, const BdVec &B, double h, int nseq, b
     if (lane == 0) {
       sflag[0] = 0;  // stop: HUGE_ABUNDS
       sflag[1] = 0;  // solves done
+      sflag[2] = 0;  // refinement sweeps
     }
   }
   for (int j = 0;; ++j) {
@@ -233,7 +235,8 @@ __device__ int bd_level_tile(const Act &A, const BdVec &B, double h, int nseq, b
           x[i] = stage == 1 ? h * dx : h * dx - d[i];
         }
       }
-      tile_solve_regs<R>(A.T, A.rinv, na, x, ri, lane);
+      if (A.mixed_now) sweeps += tile_solve_mixed<R>(A, x, lane);
+      else tile_solve_regs<R>(A.T, A.rinv, na, x, ri, lane);
       bool huge = false;
 #pragma unroll
       for (int i = 0; i < R; ++i) {
@@ -257,17 +260,20 @@ __device__ int bd_level_tile(const Act &A, const BdVec &B, double h, int nseq, b
         B.yk[lane + 32 * i] = y[i];
         B.dk[lane + 32 * i] = d[i];
       }
+    if (lane == 0) sflag[2] = sweeps;
   }
+  __syncthreads();
   const int err = sflag[0];
   nsolve += sflag[1];
+  ir_sweeps += sflag[2];
   __syncthreads();
   return err;
 }
 
 __device__ int dev_bd_level_tile(const Act &A, const BdVec &B, double h, int nseq, bool huge_frozen, int &nsolve,
-                                 int *sflag) {
-  return A.tile_rows == 32 ? bd_level_tile<1>(A, B, h, nseq, huge_frozen, nsolve, sflag)
-                           : bd_level_tile<2>(A, B, h, nseq, huge_frozen, nsolve, sflag);
+                                 int &ir_sweeps, int *sflag) {
+  return A.tile_rows == 32 ? bd_level_tile<1>(A, B, h, nseq, huge_frozen, nsolve, ir_sweeps, sflag)
+                           : bd_level_tile<2>(A, B, h, nseq, huge_frozen, nsolve, ir_sweeps, sflag);
 }
 
 // extrapolate (bader_deuflhard.F90:371-407): Neville tableau, column k, on the active rows
@@ -338,7 +344,7 @@ __device__ int dev_bader_deuflhard(const DevNet &N, const Ws &W, ZoneCtl &C, dou
     C.st.nfact++;
     int ierr;
     if (A.tile) {
-      ierr = dev_bd_level_tile(A, B, h, N.nseq[k], huge_fz, C.st.nsolve, C.sint);
+      ierr = dev_bd_level_tile(A, B, h, N.nseq[k], huge_fz, C.st.nsolve, C.st.ir_sweeps, C.sint);
     } else {
       ierr = dev_bd_substep(N, W, C, B, h, 1, huge_fz);
       for (int i = 1; ierr == 0 && i <= N.nseq[k] - 1; ++i) ierr = dev_bd_substep(N, W, C, B, h, 2, huge_fz);

@@ -151,6 +151,37 @@ def test_trajectory_cooling_through_min_t9_matches_checker(solver_mod, abi, orc,
         assert rel <= 1e-6 and ab <= 1e-15, (tile, rel, ab)
 
 
+@pytest.mark.parametrize("dt", [1.0e2, 1.0e8])
+def test_reduced_solve_mixed_matches_superlu(solver_mod, abi, orc, net300, batch, dt):
+    """lu_precision = 1: FP32 factor of the equilibrated tile, FP64 iterative refinement to
+    ir_rtol = 1e-14; the solution must match SuperLU's FP64 one like the FP64 tile does (1e-9)."""
+    dev = _dev(solver_mod, net300, abi, lu_precision=1)
+    ref = orc.Oracle(net300, abi.default_knobs())
+    vr = ref.evaluate_all_rates(batch.t9_0, batch.rho_0, batch.ye, batch.X)
+    jr, esr, mkr = ref.calculate_jacobian(vr, batch.X, dt)
+    b = np.random.default_rng(5).normal(size=(batch.nz, net300.nsp)) * 1e-3
+    x = dev.solve_reduced(jr, esr, mkr, dt, b)
+    xr, ierr = ref.solve_reduced(jr, esr, mkr, dt, b)
+    assert (ierr == 0).all()
+    err = np.abs(x - xr).max(axis=1) / np.abs(xr).max(axis=1)
+    assert err.max() < 1e-9, err
+
+
+def test_integrate_bd_mixed_matches_checker(solver_mod, abi, orc, net300, batch):
+    """Bader-Deuflhard with lu_precision = 1 against the FP64 checker: the workload's tolerance
+    (1e-6 relative for X > 1e-12, 1e-15 absolute below), mass conserved, refinement sweeps made."""
+    dev = _dev(solver_mod, net300, abi, integration_method=1, lu_precision=1)
+    ref = orc.Oracle(net300, abi.default_knobs(integration_method=1))
+    args = (batch.X, batch.t9_0, batch.t9_1, batch.rho_0, batch.rho_1, batch.ye, batch.dtwant)
+    X, ye, ierr, st, _ = dev.integrate_network(*args)
+    Xr, yer, ierr_r, str_, _ = ref.integrate_network(*args)
+    assert (ierr == 0).all() and (ierr_r == 0).all()
+    assert sum(s.ir_sweeps for s in st) > 0
+    rel, ab = _compare_X(X, Xr)
+    assert rel <= 1e-6 and ab <= 1e-15, (rel, ab)
+    assert np.abs(X.sum(axis=1) - 1.0).max() < 1e-10
+
+
 def _compare_X(X, Xr):
     big = Xr > 1e-12
     rel = np.abs(X - Xr)[big] / Xr[big]
@@ -213,7 +244,7 @@ def hot1107(wl, orc, abi):
     return net, zb, X, ref
 
 
-@pytest.mark.parametrize("tile", [0, -1], ids=["tile", "sparse"])
+@pytest.mark.parametrize("tile", [0, -1, "mixed"], ids=["tile", "sparse", "mixed"])
 @pytest.mark.parametrize("dt", [1.0e2, 1.0e8, 1.0e10])
 def test_reduced_solve_wide_matches_superlu(solver_mod, abi, hot1107, tile, dt):
     net, zb, X, ref = hot1107
@@ -222,7 +253,8 @@ def test_reduced_solve_wide_matches_superlu(solver_mod, abi, hot1107, tile, dt):
     na = mkr.sum(axis=1)
     if dt >= 1.0e8:
         assert ((na > 32) & (na <= 64)).all(), na
-    dev = _dev(solver_mod, net, abi, lu_tile_max=tile)
+    kw = dict(lu_precision=1) if tile == "mixed" else dict(lu_tile_max=tile)
+    dev = _dev(solver_mod, net, abi, **kw)
     b = np.random.default_rng(7).normal(size=(zb.nz, net.nsp)) * 1e-3
     x = dev.solve_reduced(jr, esr, mkr, dt, b)
     xr, ierr = ref.solve_reduced(jr, esr, mkr, dt, b)
