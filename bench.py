@@ -40,12 +40,19 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """nvidia-smi clocks and throttle reasons during the timed region. The sampler is started before
+    the warm-up (nvidia-smi takes a few hundred ms to start) and samples every 50 ms; only the rows
+    that arrive between mark() and the end of the `with` block are summarised."""
 
     def __init__(self, index=0):
         self.index = index
         self.rows = []
         self.proc = None
+        self.t0 = None
+        self.t1 = None
+
+    def mark(self):
+        self.t0 = time.time()
 
     def __enter__(self):
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
@@ -53,7 +60,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -65,9 +72,10 @@ class ClockSampler:
         for line in self.proc.stdout:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) == 7:
-                self.rows.append(parts)
+                self.rows.append((time.time(), parts))
 
     def __exit__(self, *a):
+        self.t1 = time.time()
         if self.proc:
             self.proc.terminate()
             try:
@@ -76,14 +84,17 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.rows:
+        t0 = self.t0 if self.t0 is not None else 0.0
+        t1 = self.t1 if self.t1 is not None else time.time()
+        rows = [r for t, r in self.rows if t0 <= t <= t1]
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[3 + k].lower() == "active"})
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[3 + k].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(rows)}
 
 
 def measured_traffic_per_zone():
@@ -211,14 +222,15 @@ def run_traj(args, rank, world, local):
         e1.record()
         return e0, e1
 
-    for _ in range(args.warmup):
-        one_step()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    launches0 = S.launches()
     with ClockSampler(torch.cuda.current_device()) as clk:
+        for _ in range(args.warmup):
+            one_step()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        launches0 = S.launches()
+        clk.mark()
         ev = [one_step() for _ in range(args.steps)]
         torch.cuda.synchronize()
     st_np = stats.cpu().numpy()
@@ -261,7 +273,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nz", type=int, default=1024)
     ap.add_argument("--ref-zones", type=int, default=32)
-    ap.add_argument("--cpu-zones", type=int, default=16)
+    ap.add_argument("--cpu-zones", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="heshell", choices=["heshell", "traj"],
                     help="heshell: 1024 He-shell zones (the headline); traj: tppnp-style trajectories")
@@ -313,16 +325,17 @@ def main():
         e1.record()
         return e0, e1
 
-    for _ in range(args.warmup):
-        one_step()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    launches0 = S.launches()
     ev = []
     steps_done = 0
     with ClockSampler(dev_id) as clk:
+        for _ in range(args.warmup):
+            one_step()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        launches0 = S.launches()
+        clk.mark()
         for _ in range(args.steps):
             ev.append(one_step())
         torch.cuda.synchronize()
