@@ -265,6 +265,103 @@ def run_traj(args, rank, world, local):
         dist.destroy_process_group()
 
 
+def run_serve(args, rank, world):
+    """Serving: a seeded Poisson stream (args.rate requests/s over args.serve_seconds) of one-zone and
+    one-trajectory requests, 40 % He-shell zones (1109 species, BD over 1e10 s), 40 % H-burning zones
+    on the 300-species network (T9 U[0.015, 0.08], rho log-U[1, 1e3], BD over 1e10 s), 20 % tppnp
+    trajectories (1109 species, 21 points to 10 s), submitted as they arrive to two servers (one per
+    network) on one GPU and polled from this thread. value = accepted zone sub-steps of all requests
+    / (last completion - first arrival); latency = completion - arrival, from the polling loop."""
+    if rank != 0:
+        return
+    if args.impl == "reference":
+        print(json.dumps({"impl": "reference", "unavailable": "the serving workload has no reference counterpart "
+                          "(the reference integrates one zone per call on the host)"}), flush=True)
+        return
+    import torch
+    wl = importlib.import_module(PKG + ".workloads")
+    abi = importlib.import_module(PKG + ".abi")
+    solver = importlib.import_module(PKG + ".solver")
+    n1107, n300 = wl.network(1107), wl.network(300)
+    he = wl.heshell_batch(1024, net=n1107, seed=2)
+    hb0, _ = wl.hburn_zone(n300)
+    tr = wl.trajectory_batch(256, net=n1107, npts=21)
+    tt, t9g, rhog = tr.grids()
+    rng = np.random.default_rng(11)
+    gaps = rng.exponential(1.0 / args.rate, size=int(args.rate * args.serve_seconds * 1.5) + 16)
+    arrive = np.cumsum(gaps)
+    arrive = arrive[arrive < args.serve_seconds]
+    kinds = rng.choice(3, size=arrive.size, p=[0.4, 0.4, 0.2])
+    pick = rng.integers(0, 1 << 30, size=arrive.size)
+    hb_t9 = rng.uniform(0.015, 0.08, size=arrive.size)
+    hb_rho = 10.0 ** rng.uniform(0.0, 3.0, size=arrive.size)
+    kn = abi.default_knobs(integration_method=1)
+    d1107 = solver.NetworkSolver(n1107, kn, device=torch.cuda.current_device())
+    d300 = solver.NetworkSolver(n300, kn, device=torch.cuda.current_device())
+    s1107, s300 = solver.Server(d1107, lanes=4), solver.Server(d300, lanes=2)
+
+    def submit(i):
+        k = kinds[i]
+        if k == 0:
+            z = pick[i] % he.nz
+            return s1107, s1107.submit(he.X[z], he.t9_0[z], he.t9_1[z], he.rho_0[z], he.rho_1[z], he.ye[z], he.dtwant[z])
+        if k == 1:
+            return s300, s300.submit(hb0.X[0], hb_t9[i], hb_t9[i], hb_rho[i], hb_rho[i], hb0.ye[0], 1.0e10)
+        j = pick[i] % tr.nz
+        return s1107, s1107.submit_trajectory(tr.X0[j], tt[j], t9g[j], rhog[j])
+
+    for i in range(min(args.warmup, arrive.size) * 8):  # warm-up: a few requests of each kind, waited for
+        srv, rid = submit(i % arrive.size)
+        srv.wait(rid)
+    lat = [[], [], []]
+    steps = 0
+    fails = [{}, {}, {}]  # per kind: ierr code -> count
+    out = {}
+    t0 = time.perf_counter()
+    nxt = 0
+    last_done = t0
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        clk.mark()
+        while nxt < arrive.size or out:
+            now = time.perf_counter() - t0
+            while nxt < arrive.size and arrive[nxt] <= now:
+                out[nxt] = submit(nxt)
+                nxt += 1
+            for i in list(out):
+                srv, rid = out[i]
+                r = srv.poll(rid)
+                if r is None:
+                    continue
+                tdone = time.perf_counter()
+                last_done = tdone
+                lat[kinds[i]].append((tdone - t0 - arrive[i]) * 1e3)
+                steps += r[3].nsucc
+                if r[2] != 0:
+                    fails[kinds[i]][str(r[2])] = fails[kinds[i]].get(str(r[2]), 0) + 1
+                del out[i]
+            time.sleep(2e-4)
+    elapsed = last_done - t0 - (arrive[0] if arrive.size else 0.0)
+    launches = s1107.info().launches + s300.info().launches
+    s1107.close()
+    s300.close()
+    allv = np.concatenate([np.array(v) for v in lat if v]) if arrive.size else np.zeros(1)
+    pct = lambda v: {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99))} if len(v) else None
+    value = steps / elapsed
+    print(json.dumps({"metric": "zone-timesteps/s", "value": value, "unit": "zone-timesteps/s", "n_gpus": 1,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                      "config": {"workload": "serve: Poisson stream, 40% heshell-1107 zones, 40% hburn-300 zones, "
+                                             "20% tppnp-1107 trajectories (21 points)",
+                                 "rate_req_per_s": args.rate, "arrival_window_s": args.serve_seconds,
+                                 "requests": int(arrive.size), "lanes": {"1107": 4, "300": 2}},
+                      "latency_ms": {"all": pct(allv), "heshell_zone": pct(lat[0]), "hburn_zone": pct(lat[1]),
+                                     "trajectory": pct(lat[2])},
+                      "requests_failed": {"heshell_zone": fails[0], "hburn_zone": fails[1], "trajectory": fails[2]}, "drain_s": float(elapsed - args.serve_seconds),
+                      "e2e": {"value": value, "unit": "zone-timesteps/s",
+                              "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+                      "gpu_launches": int(launches), "clocks": clk.summary()}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -275,8 +372,11 @@ def main():
     ap.add_argument("--ref-zones", type=int, default=32)
     ap.add_argument("--cpu-zones", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="heshell", choices=["heshell", "traj"],
-                    help="heshell: 1024 He-shell zones (the headline); traj: tppnp-style trajectories")
+    ap.add_argument("--workload", default="heshell", choices=["heshell", "traj", "serve"],
+                    help="heshell: 1024 He-shell zones (the headline); traj: tppnp-style trajectories; "
+                         "serve: Poisson request stream through nuppn_serve_*")
+    ap.add_argument("--rate", type=float, default=2000.0, help="serve: mean requests per second")
+    ap.add_argument("--serve-seconds", type=float, default=5.0, help="serve: arrival window (s)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -284,6 +384,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload == "traj":
         run_traj(args, rank, world, local)
+        return
+    if args.workload == "serve":
+        run_serve(args, rank, world)
         return
     if args.impl == "reference":
         run_reference(args, rank, world)

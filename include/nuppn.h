@@ -292,8 +292,58 @@ nuppn_status nuppn_integrate_device_noalloc(nuppn_net *net, int32_t nz, double *
                                             const double *d_dtwant, int32_t *d_ierr,
                                             nuppn_zone_stats *d_stats, int32_t *d_bd_state, void *stream);
 
-/* Number of kernel launches issued by the library since the handle was created. */
+/* Number of kernel launches issued by the library since the handle was created (server launches
+ * are counted by nuppn_serve_info). */
 int64_t nuppn_launch_count(const nuppn_net *net);
+
+/* ---- Serving: continuous batching of independent requests ------------------------------------
+ * Each request is one call of integrate_network (solver.F90:53) for one zone, or one tppnp
+ * trajectory (tppnp.F90:131-168), as the frames issue them one at a time; the server runs them on
+ * the GPU as they arrive. It owns `lanes` CUDA streams, each with its own workspace slabs and device
+ * buffers. A host worker thread, whenever a lane is idle, takes up to `max_batch` pending requests of
+ * one kind (zones, or trajectories with the same number of points) in submission order and launches
+ * them there, so batches admitted while others are on the GPU run beside them. A request's result
+ * is the one nuppn_integrate / nuppn_integrate_trajectories gives for it alone: zones never read one
+ * another's state. The knobs are those of `net` when the server is opened; do not call
+ * nuppn_set_knobs or destroy `net` while a server on it is open. Submit, poll and close from one
+ * host thread. */
+typedef struct nuppn_server nuppn_server;
+
+/* lanes: 0 = 4. max_batch: requests per launch, 0 = the GPU's resident CTA slots. Each lane holds
+ * a workspace slab per resident CTA; lanes that do not fit in half of the free device memory are
+ * not opened (NUPPN_ERR_NOMEM if not even one fits). */
+nuppn_status nuppn_serve_open(nuppn_net *net, int32_t lanes, int32_t max_batch, nuppn_server **out);
+
+/* One zone: X[nsp] (copied at submit), interval T9/rho end points, Ye, dtwant, bd_state (0 = fresh,
+ * as for nuppn_integrate). *id identifies the request in nuppn_serve_poll. */
+nuppn_status nuppn_serve_submit(nuppn_server *srv, const double *X, double t9_0, double t9_1, double rho_0,
+                                double rho_1, double ye, double dtwant, int32_t bd_state, int64_t *id);
+
+/* One trajectory of npts points (time, t9, rho copied at submit), as for
+ * nuppn_integrate_trajectories. */
+nuppn_status nuppn_serve_submit_trajectory(nuppn_server *srv, const double *X, int32_t npts, const double *time,
+                                           const double *t9, const double *rho, int64_t *id);
+
+/* *done = 1 and the outputs filled (X[nsp], Ye, ierr, stats, bd_state, fail = failed interval or -1
+ * for a trajectory) once the request has finished, after which its id is released; *done = 0 while
+ * it is pending or on the GPU. Output pointers may be NULL. NUPPN_ERR_ARG for an unknown id;
+ * NUPPN_ERR_CUDA if the launch that carried the request failed. */
+nuppn_status nuppn_serve_poll(nuppn_server *srv, int64_t id, int32_t *done, double *X, double *ye, int32_t *ierr,
+                              nuppn_zone_stats *stats, int32_t *bd_state, int32_t *fail);
+
+typedef struct {
+  int32_t lanes, max_batch, slots_per_lane;
+  int32_t pending;          /* submitted, not yet on the GPU */
+  int32_t in_flight;        /* on the GPU */
+  int64_t launches;         /* kernel launches by the server */
+  int64_t batches;          /* batches launched */
+  int64_t completed;        /* requests finished */
+  int64_t device_bytes;     /* device memory held by the server */
+} nuppn_serve_stats;
+nuppn_status nuppn_serve_info(nuppn_server *srv, nuppn_serve_stats *out);
+
+/* Waits for the batches on the GPU, drops requests not yet launched, frees everything. */
+nuppn_status nuppn_serve_close(nuppn_server *srv);
 
 #ifdef __cplusplus
 }

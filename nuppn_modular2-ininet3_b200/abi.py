@@ -98,6 +98,13 @@ class ZoneStats(C.Structure):
                 ("ir_sweeps", C.c_int32), ("nvar1_max", C.c_int32)]
 
 
+class ServeStats(C.Structure):
+    """nuppn_serve_stats (include/nuppn.h)."""
+    _fields_ = [("lanes", C.c_int32), ("max_batch", C.c_int32), ("slots_per_lane", C.c_int32),
+                ("pending", C.c_int32), ("in_flight", C.c_int32), ("launches", C.c_int64),
+                ("batches", C.c_int64), ("completed", C.c_int64), ("device_bytes", C.c_int64)]
+
+
 class NetInfo(C.Structure):
     _fields_ = [("nsp", C.c_int32), ("nre", C.c_int32), ("nspec_active", C.c_int32),
                 ("nreac_active", C.c_int32), ("nnz_jac", C.c_int32), ("nnz_lu", C.c_int32),

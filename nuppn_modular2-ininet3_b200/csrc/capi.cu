@@ -6,11 +6,17 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "net_host.h"
@@ -697,6 +703,384 @@ nuppn_status nuppn_integrate_trajectories(nuppn_net *net, int32_t nz, int32_t np
   CK(cudaMemcpy(ierr, sb + oi, nz * 4, cudaMemcpyDeviceToHost));
   if (fail) CK(cudaMemcpy(fail, sb + of, nz * 4, cudaMemcpyDeviceToHost));
   if (stats) CK(cudaMemcpy(stats, sb + os, (size_t)nz * sizeof(nuppn_zone_stats), cudaMemcpyDeviceToHost));
+  return NUPPN_OK;
+}
+
+}  // extern "C"
+
+// ---- serving: continuous batching of independent requests --------------------------------------
+// A server owns lanes (stream, event, workspace slabs, a device "packet" of per-request arrays and
+// its pinned host twin). The worker thread launches a batch on every idle lane that finds pending
+// requests, and completes a lane's requests when its event has fired; batches on different lanes
+// run on the GPU at the same time.
+namespace {
+
+struct ServeReq {
+  int64_t id = 0;
+  int kind = 0;  // 0: one zone, 1: one trajectory
+  int npts = 0;
+  std::vector<double> X, time, t9, rho;
+  double t9_0 = 0, t9_1 = 0, rho_0 = 0, rho_1 = 0, ye = 0, dtwant = 0;
+  int bd = 0, ierr = 0, fail = -1;
+  nuppn_zone_stats st{};
+  int status = 0;  // 0 pending or on the GPU, 1 done, 2 its launch failed
+  std::string err;
+};
+
+struct ServeLane {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  DevBuf ws, dev;
+  char *host = nullptr;
+  size_t bytes = 0;
+  int cap = 0, cap_npts = 0;  // requests and trajectory points the packet holds
+  bool busy = false;
+  std::vector<ServeReq *> batch;
+  // packet offsets (identical in the device and the pinned host packet)
+  size_t oX = 0, oye = 0, obd = 0, oierr = 0, ofail = 0, ost = 0, ot90 = 0, ot91 = 0, orh0 = 0, orh1 = 0,
+         odt = 0, oord = 0, ocnt = 0, otime = 0, ot9 = 0, orho = 0;
+
+  size_t layout(int B, int nsp, int npts) {
+    size_t t = 0;
+    auto take = [&](size_t b) { size_t o = t; t = align256(t + std::max<size_t>(b, 8)); return o; };
+    oX = take((size_t)B * nsp * 8); oye = take(B * 8); obd = take(B * 4); oierr = take(B * 4); ofail = take(B * 4);
+    ost = take((size_t)B * sizeof(nuppn_zone_stats)); ot90 = take(B * 8); ot91 = take(B * 8); orh0 = take(B * 8);
+    orh1 = take(B * 8); odt = take(B * 8); oord = take(B * 4); ocnt = take(4);
+    otime = take((size_t)B * npts * 8); ot9 = take((size_t)B * npts * 8); orho = take((size_t)B * npts * 8);
+    return t;
+  }
+};
+
+}  // namespace
+
+struct nuppn_server {
+  nuppn_net *net = nullptr;
+  int max_batch = 0, slots = 0;
+  std::vector<ServeLane> lanes;
+  std::thread worker;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<ServeReq *> pending;
+  std::unordered_map<int64_t, ServeReq *> reqs;
+  int64_t next_id = 1;
+  std::atomic<bool> stop{false};
+  std::atomic<int64_t> launches{0}, batches{0}, completed{0};
+  std::atomic<int> in_flight{0};
+  int64_t device_bytes = 0;
+};
+
+namespace {
+
+cudaError_t lane_alloc(ServeLane &L, const nuppn_net *net, int B, int npts) {
+  L.cap = B;
+  L.cap_npts = npts;
+  L.bytes = L.layout(B, net->H.nsp, npts);
+  cudaError_t e = L.dev.ensure(L.bytes);
+  if (e != cudaSuccess) return e;
+  if (L.host) cudaFreeHost(L.host);
+  L.host = nullptr;
+  return cudaMallocHost((void **)&L.host, L.bytes);
+}
+
+void lane_free(ServeLane &L) {
+  if (L.stream) cudaStreamSynchronize(L.stream);
+  L.ws.release();
+  L.dev.release();
+  if (L.host) cudaFreeHost(L.host);
+  L.host = nullptr;
+  if (L.done) cudaEventDestroy(L.done);
+  if (L.stream) cudaStreamDestroy(L.stream);
+  L.done = nullptr;
+  L.stream = nullptr;
+}
+
+// Pending requests of the oldest one's kind (and point count), oldest first, at most max_batch.
+std::vector<ServeReq *> take_batch(nuppn_server *S) {
+  std::vector<ServeReq *> b;
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (S->pending.empty()) return b;
+  const int kind = S->pending.front()->kind, npts = S->pending.front()->npts;
+  std::deque<ServeReq *> keep;
+  for (ServeReq *r : S->pending) {
+    if ((int)b.size() < S->max_batch && r->kind == kind && r->npts == npts) b.push_back(r);
+    else keep.push_back(r);
+  }
+  S->pending.swap(keep);
+  S->in_flight += (int)b.size();
+  return b;
+}
+
+void fail_batch(nuppn_server *S, std::vector<ServeReq *> &b, const std::string &why) {
+  std::lock_guard<std::mutex> lk(S->mu);
+  for (ServeReq *r : b) { r->status = 2; r->err = why; }
+  S->in_flight -= (int)b.size();
+  S->completed += (int64_t)b.size();
+  b.clear();
+}
+
+#define SK(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess) return std::string(#call) + ": " + cudaGetErrorString(e_);  \
+  } while (0)
+
+// Stage and launch one batch on an idle lane. Returns "" or what failed.
+std::string lane_launch(nuppn_server *S, ServeLane &L, std::vector<ServeReq *> &b) {
+  nuppn_net *net = S->net;
+  const int n = (int)b.size(), nsp = net->H.nsp, kind = b[0]->kind, npts = b[0]->npts;
+  if (kind == 1 && npts > L.cap_npts) {  // rare: grow the packet (frees synchronise the device)
+    SK(lane_alloc(L, net, L.cap, std::max(npts, 2 * L.cap_npts)));
+  }
+  char *h = L.host, *d = (char *)L.dev.p;
+  for (int i = 0; i < n; ++i) {
+    const ServeReq *r = b[i];
+    memcpy(h + L.oX + (size_t)i * nsp * 8, r->X.data(), (size_t)nsp * 8);
+    ((double *)(h + L.oye))[i] = r->ye;
+    ((int *)(h + L.obd))[i] = r->bd;
+    if (kind == 0) {
+      ((double *)(h + L.ot90))[i] = r->t9_0; ((double *)(h + L.ot91))[i] = r->t9_1;
+      ((double *)(h + L.orh0))[i] = r->rho_0; ((double *)(h + L.orh1))[i] = r->rho_1;
+      ((double *)(h + L.odt))[i] = r->dtwant;
+    } else {
+      memcpy(h + L.otime + (size_t)i * npts * 8, r->time.data(), (size_t)npts * 8);
+      memcpy(h + L.ot9 + (size_t)i * npts * 8, r->t9.data(), (size_t)npts * 8);
+      memcpy(h + L.orho + (size_t)i * npts * 8, r->rho.data(), (size_t)npts * 8);
+    }
+  }
+  L.batch = b;
+  cudaStream_t s = L.stream;
+  auto h2d = [&](size_t off, size_t bytes) { return cudaMemcpyAsync(d + off, h + off, bytes, cudaMemcpyHostToDevice, s); };
+  auto d2h = [&](size_t off, size_t bytes) { return cudaMemcpyAsync(h + off, d + off, bytes, cudaMemcpyDeviceToHost, s); };
+  SK(h2d(L.oX, (size_t)n * nsp * 8));
+  SK(h2d(L.oye, (size_t)n * 8));
+  SK(h2d(L.obd, (size_t)n * 4));
+  IntegrateArgs A = {};
+  A.nz = n; A.ldx = nsp; A.X = (double *)(d + L.oX); A.ye = (double *)(d + L.oye);
+  A.ierr = (int *)(d + L.oierr); A.stats = (nuppn_zone_stats *)(d + L.ost); A.bd_state = (int *)(d + L.obd);
+  A.counter = (int *)(d + L.ocnt); A.order = (const int *)(d + L.oord);
+  if (kind == 0) {
+    SK(h2d(L.ot90, (size_t)n * 8)); SK(h2d(L.ot91, (size_t)n * 8));
+    SK(h2d(L.orh0, (size_t)n * 8)); SK(h2d(L.orh1, (size_t)n * 8)); SK(h2d(L.odt, (size_t)n * 8));
+    A.t9_0 = (double *)(d + L.ot90); A.t9_1 = (double *)(d + L.ot91);
+    A.rho_0 = (double *)(d + L.orh0); A.rho_1 = (double *)(d + L.orh1); A.dtwant = (double *)(d + L.odt);
+    SK(launch_zone_order(A.t9_0, A.t9_1, 1, n, (int *)(d + L.oord), s));
+  } else {
+    const size_t np = (size_t)n * npts * 8;
+    SK(h2d(L.otime, np)); SK(h2d(L.ot9, np)); SK(h2d(L.orho, np));
+    A.npts = npts; A.tr_time = (double *)(d + L.otime); A.tr_t9 = (double *)(d + L.ot9);
+    A.tr_rho = (double *)(d + L.orho); A.tr_fail = (int *)(d + L.ofail);
+    SK(launch_zone_order(A.tr_t9, nullptr, npts, n, (int *)(d + L.oord), s));
+  }
+  SK(cudaMemsetAsync(d + L.ocnt, 0, sizeof(int), s));
+  SK(launch_integrate(net->D, net->L, (char *)L.ws.p, std::min(n, S->slots), net->block, net->act_smem, A, s));
+  S->launches += 2;
+  S->batches += 1;
+  SK(d2h(L.oX, (size_t)n * nsp * 8));
+  SK(d2h(L.oye, (size_t)n * 8));
+  SK(d2h(L.obd, (size_t)n * 4));
+  SK(d2h(L.oierr, (size_t)n * 4));
+  SK(d2h(L.ost, (size_t)n * sizeof(nuppn_zone_stats)));
+  if (kind == 1) SK(d2h(L.ofail, (size_t)n * 4));
+  SK(cudaEventRecord(L.done, s));
+  L.busy = true;
+  return "";
+}
+
+void lane_finish(nuppn_server *S, ServeLane &L, cudaError_t e) {
+  const int nsp = S->net->H.nsp, n = (int)L.batch.size();
+  const char *h = L.host;
+  std::lock_guard<std::mutex> lk(S->mu);
+  for (int i = 0; i < n; ++i) {
+    ServeReq *r = L.batch[i];
+    if (e != cudaSuccess) {
+      r->status = 2;
+      r->err = std::string("batch failed: ") + cudaGetErrorString(e);
+      continue;
+    }
+    memcpy(r->X.data(), h + L.oX + (size_t)i * nsp * 8, (size_t)nsp * 8);
+    r->ye = ((const double *)(h + L.oye))[i];
+    r->bd = ((const int *)(h + L.obd))[i];
+    r->ierr = ((const int *)(h + L.oierr))[i];
+    r->st = ((const nuppn_zone_stats *)(h + L.ost))[i];
+    r->fail = r->kind == 1 ? ((const int *)(h + L.ofail))[i] : -1;
+    r->status = 1;
+  }
+  S->in_flight -= n;
+  S->completed += n;
+  L.batch.clear();
+  L.busy = false;
+}
+
+void serve_loop(nuppn_server *S) {
+  cudaSetDevice(S->net->device);
+  for (;;) {
+    bool did = false, busy = false;
+    for (ServeLane &L : S->lanes) {
+      if (!L.busy) continue;
+      const cudaError_t q = cudaEventQuery(L.done);
+      if (q == cudaErrorNotReady) { busy = true; continue; }
+      lane_finish(S, L, q);
+      did = true;
+    }
+    if (S->stop.load() && !busy) break;  // finished what was on the GPU; pending requests are dropped
+    if (!S->stop.load()) {
+      for (ServeLane &L : S->lanes) {
+        if (L.busy) continue;
+        std::vector<ServeReq *> b = take_batch(S);
+        if (b.empty()) break;
+        const std::string err = lane_launch(S, L, b);
+        if (!err.empty()) {
+          cudaStreamSynchronize(L.stream);  // copies of the failed batch may still be queued
+          L.batch.clear();
+          L.busy = false;
+          fail_batch(S, b, err);
+        }
+        did = true;
+      }
+    }
+    if (!did) {
+      std::unique_lock<std::mutex> lk(S->mu);
+      S->cv.wait_for(lk, std::chrono::microseconds(100));
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+nuppn_status nuppn_serve_open(nuppn_net *net, int32_t lanes, int32_t max_batch, nuppn_server **out) {
+  if (!net || !out) { set_error("null argument"); return NUPPN_ERR_ARG; }
+  if (lanes < 0 || max_batch < 0) { set_error("lanes and max_batch must be >= 0"); return NUPPN_ERR_ARG; }
+  *out = nullptr;
+  CK(cudaSetDevice(net->device));
+  size_t free_b = 0, total_b = 0;
+  CK(cudaMemGetInfo(&free_b, &total_b));
+  nuppn_server *S = new (std::nothrow) nuppn_server();
+  if (!S) return NUPPN_ERR_NOMEM;
+  S->net = net;
+  S->slots = resident_slots(net);
+  S->max_batch = max_batch > 0 ? max_batch : S->slots;
+  const int want = lanes > 0 ? lanes : 4;
+  ServeLane probe;
+  const size_t per_lane = (size_t)S->slots * net->L.bytes + probe.layout(S->max_batch, net->H.nsp, 256);
+  const int fit = (int)std::min<size_t>((size_t)want, (free_b / 2) / std::max<size_t>(per_lane, 1));
+  if (fit < 1) {
+    delete S;
+    set_error("nuppn_serve_open: one lane needs " + std::to_string(per_lane) + " bytes, more than half of the " +
+              std::to_string(free_b) + " bytes free");
+    return NUPPN_ERR_NOMEM;
+  }
+  S->lanes.resize(fit);
+  for (ServeLane &L : S->lanes) {
+    cudaError_t e = cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = L.ws.ensure((size_t)S->slots * net->L.bytes);
+    if (e == cudaSuccess) e = lane_alloc(L, net, S->max_batch, 256);
+    if (e != cudaSuccess) {
+      for (ServeLane &M : S->lanes) lane_free(M);
+      delete S;
+      set_error(std::string("nuppn_serve_open: ") + cudaGetErrorString(e));
+      return NUPPN_ERR_NOMEM;
+    }
+    S->device_bytes += (int64_t)(L.ws.n + L.dev.n);
+  }
+  S->worker = std::thread(serve_loop, S);
+  *out = S;
+  return NUPPN_OK;
+}
+
+static nuppn_status serve_enqueue(nuppn_server *S, ServeReq *r, int64_t *id) {
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    r->id = S->next_id++;
+    S->reqs[r->id] = r;
+    S->pending.push_back(r);
+  }
+  S->cv.notify_one();
+  *id = r->id;
+  return NUPPN_OK;
+}
+
+nuppn_status nuppn_serve_submit(nuppn_server *srv, const double *X, double t9_0, double t9_1, double rho_0,
+                                double rho_1, double ye, double dtwant, int32_t bd_state, int64_t *id) {
+  if (!srv || !X || !id) { set_error("null argument"); return NUPPN_ERR_ARG; }
+  ServeReq *r = new (std::nothrow) ServeReq();
+  if (!r) return NUPPN_ERR_NOMEM;
+  r->kind = 0;
+  r->X.assign(X, X + srv->net->H.nsp);
+  r->t9_0 = t9_0; r->t9_1 = t9_1; r->rho_0 = rho_0; r->rho_1 = rho_1; r->ye = ye; r->dtwant = dtwant;
+  r->bd = bd_state;
+  return serve_enqueue(srv, r, id);
+}
+
+nuppn_status nuppn_serve_submit_trajectory(nuppn_server *srv, const double *X, int32_t npts, const double *time,
+                                           const double *t9, const double *rho, int64_t *id) {
+  if (!srv || !X || !time || !t9 || !rho || !id) { set_error("null argument"); return NUPPN_ERR_ARG; }
+  if (npts < 2) { set_error("npts < 2"); return NUPPN_ERR_ARG; }
+  ServeReq *r = new (std::nothrow) ServeReq();
+  if (!r) return NUPPN_ERR_NOMEM;
+  r->kind = 1;
+  r->npts = npts;
+  r->X.assign(X, X + srv->net->H.nsp);
+  r->time.assign(time, time + npts);
+  r->t9.assign(t9, t9 + npts);
+  r->rho.assign(rho, rho + npts);
+  return serve_enqueue(srv, r, id);
+}
+
+nuppn_status nuppn_serve_poll(nuppn_server *srv, int64_t id, int32_t *done, double *X, double *ye, int32_t *ierr,
+                              nuppn_zone_stats *stats, int32_t *bd_state, int32_t *fail) {
+  if (!srv || !done) { set_error("null argument"); return NUPPN_ERR_ARG; }
+  ServeReq *r = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    auto it = srv->reqs.find(id);
+    if (it == srv->reqs.end()) { set_error("unknown request id"); return NUPPN_ERR_ARG; }
+    if (it->second->status == 0) { *done = 0; return NUPPN_OK; }
+    r = it->second;
+    srv->reqs.erase(it);
+  }
+  *done = 1;
+  const int st = r->status;
+  const std::string err = r->err;
+  if (st == 1) {
+    if (X) memcpy(X, r->X.data(), r->X.size() * 8);
+    if (ye) *ye = r->ye;
+    if (ierr) *ierr = r->ierr;
+    if (stats) *stats = r->st;
+    if (bd_state) *bd_state = r->bd;
+    if (fail) *fail = r->fail;
+  }
+  delete r;
+  if (st != 1) { set_error(err); return NUPPN_ERR_CUDA; }
+  return NUPPN_OK;
+}
+
+nuppn_status nuppn_serve_info(nuppn_server *srv, nuppn_serve_stats *out) {
+  if (!srv || !out) { set_error("null argument"); return NUPPN_ERR_ARG; }
+  std::lock_guard<std::mutex> lk(srv->mu);
+  out->lanes = (int32_t)srv->lanes.size();
+  out->max_batch = srv->max_batch;
+  out->slots_per_lane = srv->slots;
+  out->pending = (int32_t)srv->pending.size();
+  out->in_flight = srv->in_flight.load();
+  out->launches = srv->launches.load();
+  out->batches = srv->batches.load();
+  out->completed = srv->completed.load();
+  out->device_bytes = srv->device_bytes;
+  return NUPPN_OK;
+}
+
+nuppn_status nuppn_serve_close(nuppn_server *srv) {
+  if (!srv) return NUPPN_OK;
+  srv->stop = true;
+  srv->cv.notify_all();
+  if (srv->worker.joinable()) srv->worker.join();
+  cudaSetDevice(srv->net->device);
+  for (ServeLane &L : srv->lanes) lane_free(L);
+  for (auto &kv : srv->reqs) delete kv.second;
+  delete srv;
   return NUPPN_OK;
 }
 

@@ -58,10 +58,19 @@ def load_library():
     L.nuppn_nse.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp]
     L.nuppn_integrate_trajectories.argtypes = [vp, i32, i32, vp, i32, vp, vp, vp, vp, vp, vp, vp]
     L.nuppn_integrate_trajectories_device.argtypes = [vp, i32, i32, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    f64, i64 = C.c_double, C.c_int64
+    L.nuppn_serve_open.argtypes = [vp, i32, i32, C.POINTER(vp)]
+    L.nuppn_serve_submit.argtypes = [vp, vp, f64, f64, f64, f64, f64, f64, i32, C.POINTER(i64)]
+    L.nuppn_serve_submit_trajectory.argtypes = [vp, vp, i32, vp, vp, vp, C.POINTER(i64)]
+    L.nuppn_serve_poll.argtypes = [vp, i64, C.POINTER(i32), vp, vp, vp, vp, vp, vp]
+    L.nuppn_serve_info.argtypes = [vp, vp]
+    L.nuppn_serve_close.argtypes = [vp]
     for name in ("nuppn_net_create", "nuppn_net_destroy", "nuppn_net_info_get", "nuppn_set_knobs",
                  "nuppn_jac_pattern", "nuppn_eval_rates", "nuppn_dxdt", "nuppn_jacobian",
                  "nuppn_solve_reduced", "nuppn_integrate", "nuppn_integrate_device", "nuppn_nse",
-                 "nuppn_integrate_trajectories", "nuppn_integrate_trajectories_device"):
+                 "nuppn_integrate_trajectories", "nuppn_integrate_trajectories_device",
+                 "nuppn_serve_open", "nuppn_serve_submit", "nuppn_serve_submit_trajectory", "nuppn_serve_poll",
+                 "nuppn_serve_info", "nuppn_serve_close"):
         getattr(L, name).restype = i32
     _LIB = L
     return L
@@ -227,3 +236,72 @@ class NetworkSolver:
         self._check(self.L.nuppn_integrate_device(
             self.h, X.shape[0], ptr(X), X.shape[1], ptr(t9_0), ptr(t9_1), ptr(rho_0), ptr(rho_1), ptr(ye),
             ptr(dtwant), ptr(ierr), ptr(stats), ptr(bd_state), C.c_void_p(stream)))
+
+
+class Server:
+    """Continuous batching of independent requests (nuppn_serve_*): each request is one zone
+    (integrate_network's arguments) or one trajectory; the library's worker thread launches pending
+    requests on any idle lane while other lanes' batches run. Submit, poll and close from one thread;
+    do not change the solver's knobs while the server is open."""
+
+    def __init__(self, solver: NetworkSolver, lanes: int = 0, max_batch: int = 0):
+        self.solver, self.L = solver, solver.L
+        h = C.c_void_p()
+        solver._check(self.L.nuppn_serve_open(solver.h, lanes, max_batch, C.byref(h)))
+        self.h = h
+
+    def submit(self, X, t9_0, t9_1, rho_0, rho_1, ye, dtwant, bd_state=0) -> int:
+        x = np.ascontiguousarray(X, dtype=np.float64)
+        rid = C.c_int64()
+        self.solver._check(self.L.nuppn_serve_submit(self.h, _p(x), float(t9_0), float(t9_1), float(rho_0),
+                                                     float(rho_1), float(ye), float(dtwant), int(bd_state),
+                                                     C.byref(rid)))
+        return rid.value
+
+    def submit_trajectory(self, X, time, t9, rho) -> int:
+        x = np.ascontiguousarray(X, dtype=np.float64)
+        tt, tp, tr = (np.ascontiguousarray(a, dtype=np.float64) for a in (time, t9, rho))
+        rid = C.c_int64()
+        self.solver._check(self.L.nuppn_serve_submit_trajectory(self.h, _p(x), tt.size, _p(tt), _p(tp), _p(tr),
+                                                                C.byref(rid)))
+        return rid.value
+
+    def poll(self, rid: int):
+        """None while the request runs, else (X, ye, ierr, stats, bd_state, fail)."""
+        if getattr(self, "_xbuf", None) is None:
+            self._xbuf = np.zeros(self.solver.nsp)
+        done = C.c_int32()
+        ye, ierr, bd, fail = C.c_double(), C.c_int32(), C.c_int32(), C.c_int32()
+        st = abi.ZoneStats()
+        self.solver._check(self.L.nuppn_serve_poll(self.h, rid, C.byref(done), _p(self._xbuf), C.byref(ye),
+                                                   C.byref(ierr), C.byref(st), C.byref(bd), C.byref(fail)))
+        if not done.value:
+            return None
+        return self._xbuf.copy(), ye.value, ierr.value, st, bd.value, fail.value
+
+    def wait(self, rid: int, timeout: float = 300.0):
+        import time as _time
+        t_end = _time.monotonic() + timeout
+        while True:
+            r = self.poll(rid)
+            if r is not None:
+                return r
+            if _time.monotonic() > t_end:
+                raise TimeoutError(f"request {rid} not finished after {timeout} s")
+            _time.sleep(2e-4)
+
+    def info(self) -> abi.ServeStats:
+        s = abi.ServeStats()
+        self.solver._check(self.L.nuppn_serve_info(self.h, C.byref(s)))
+        return s
+
+    def close(self):
+        if self.h:
+            self.L.nuppn_serve_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
