@@ -298,7 +298,9 @@ def run_serve(args, rank, world):
     kn = abi.default_knobs(integration_method=1)
     d1107 = solver.NetworkSolver(n1107, kn, device=torch.cuda.current_device())
     d300 = solver.NetworkSolver(n300, kn, device=torch.cuda.current_device())
-    s1107, s300 = solver.Server(d1107, lanes=4), solver.Server(d300, lanes=2)
+    lanes = args.serve_lanes or 4
+    s1107 = solver.Server(d1107, lanes=lanes, max_batch=args.serve_batch)
+    s300 = solver.Server(d300, lanes=max(1, lanes // 2), max_batch=args.serve_batch)
 
     def submit(i):
         k = kinds[i]
@@ -341,7 +343,8 @@ def run_serve(args, rank, world):
                 del out[i]
             time.sleep(2e-4)
     elapsed = last_done - t0 - (arrive[0] if arrive.size else 0.0)
-    launches = s1107.info().launches + s300.info().launches
+    s_info = (s1107.info(), s300.info())
+    launches = s_info[0].launches + s_info[1].launches
     s1107.close()
     s300.close()
     allv = np.concatenate([np.array(v) for v in lat if v]) if arrive.size else np.zeros(1)
@@ -353,7 +356,9 @@ def run_serve(args, rank, world):
                       "config": {"workload": "serve: Poisson stream, 40% heshell-1107 zones, 40% hburn-300 zones, "
                                              "20% tppnp-1107 trajectories (21 points)",
                                  "rate_req_per_s": args.rate, "arrival_window_s": args.serve_seconds,
-                                 "requests": int(arrive.size), "lanes": {"1107": 4, "300": 2}},
+                                 "requests": int(arrive.size),
+                                 "lanes": {"1107": s_info[0].lanes, "300": s_info[1].lanes},
+                                 "max_batch": {"1107": s_info[0].max_batch, "300": s_info[1].max_batch}},
                       "latency_ms": {"all": pct(allv), "heshell_zone": pct(lat[0]), "hburn_zone": pct(lat[1]),
                                      "trajectory": pct(lat[2])},
                       "requests_failed": {"heshell_zone": fails[0], "hburn_zone": fails[1], "trajectory": fails[2]}, "drain_s": float(elapsed - args.serve_seconds),
@@ -377,6 +382,8 @@ def main():
                          "serve: Poisson request stream through nuppn_serve_*")
     ap.add_argument("--rate", type=float, default=2000.0, help="serve: mean requests per second")
     ap.add_argument("--serve-seconds", type=float, default=5.0, help="serve: arrival window (s)")
+    ap.add_argument("--serve-lanes", type=int, default=0, help="serve: lanes of the 1109-species server (0: 4)")
+    ap.add_argument("--serve-batch", type=int, default=0, help="serve: max requests per launch (0: library)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

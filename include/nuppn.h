@@ -309,7 +309,9 @@ int64_t nuppn_launch_count(const nuppn_net *net);
  * host thread. */
 typedef struct nuppn_server nuppn_server;
 
-/* lanes: 0 = 4. max_batch: requests per launch, 0 = the GPU's resident CTA slots. Each lane holds
+/* lanes: 0 = 4. max_batch: requests per launch, 0 = the GPU's resident CTA slots (large batches
+ * measured faster than more lanes with smaller batches: a launch's throughput grows with its batch).
+ * Each lane holds
  * a workspace slab per resident CTA; lanes that do not fit in half of the free device memory are
  * not opened (NUPPN_ERR_NOMEM if not even one fits). */
 nuppn_status nuppn_serve_open(nuppn_net *net, int32_t lanes, int32_t max_batch, nuppn_server **out);

@@ -960,8 +960,8 @@ nuppn_status nuppn_serve_open(nuppn_net *net, int32_t lanes, int32_t max_batch, 
   if (!S) return NUPPN_ERR_NOMEM;
   S->net = net;
   S->slots = resident_slots(net);
-  S->max_batch = max_batch > 0 ? max_batch : S->slots;
   const int want = lanes > 0 ? lanes : 4;
+  S->max_batch = max_batch > 0 ? max_batch : S->slots;
   ServeLane probe;
   const size_t per_lane = (size_t)S->slots * net->L.bytes + probe.layout(S->max_batch, net->H.nsp, 256);
   const int fit = (int)std::min<size_t>((size_t)want, (free_b / 2) / std::max<size_t>(per_lane, 1));
