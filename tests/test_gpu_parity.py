@@ -359,6 +359,46 @@ def test_trajectories_within_reference_spread(solver_mod, abi, orc, wl):
     assert np.abs(Xd.sum(axis=1) - 1.0).max() < 1e-10
 
 
+def test_trajectory_from_nse_within_reference_spread(solver_mod, abi, orc, wl):
+    """Explosive trajectories that start in NSE (T9_0 in [6.2, 8], X_0 from the NSE solve, i_nse = 1)
+    and cool through nse_min_t9 = 6 into network integration, 21 points to 1 s, through
+    nuppn_integrate_trajectories. While the trajectories are in NSE (the first 16 points) device and
+    checker agree to 1e-9. After the exit the network integration starts from an NSE composition at
+    T9 just below 6, where the reference's own result is not determined to better than O(1): 1-ulp
+    changes of the T9 grid move its final abundances by up to ~4x. (Changes of X_0 do not probe this:
+    NSE sub-steps recompute X from T, rho and Ye.) So for the whole trajectory every one must succeed,
+    conserve mass, and lie (X and Ye) within 4x the largest deviation of three 1-ulp T9 perturbations
+    of the checker, or 1e-6 (X) / 1e-8 (Ye)."""
+    net = wl.network(1107)
+    tr = wl.trajectory_batch(4, net=net, npts=21, t9_range=(6.2, 8.0), t_end=1.0)
+    tt, t9, rho = tr.grids()
+    kn = abi.default_knobs(integration_method=1, i_nse=1)
+    dev = _dev(solver_mod, net, abi, integration_method=1, i_nse=1)
+    ref = orc.Oracle(net, kn)
+    X0, _, _, _, ierr0 = ref.compute_nse(t9[:, 0], rho[:, 0], np.linspace(0.48, 0.495, tr.nz))
+    assert (ierr0 == 0).all()
+    assert (t9[:, 15] >= 6.0).all() and (t9[:, -1] < 6.0).all()
+    nse = slice(0, 16)
+    Xd16 = dev.integrate_trajectories(X0, tt[:, nse], t9[:, nse], rho[:, nse])[0]
+    Xr16 = ref.integrate_trajectories(X0, tt[:, nse], t9[:, nse], rho[:, nse], nthreads=4)[0]
+    rel16, ab16 = _compare_X(Xd16, Xr16)
+    assert rel16 <= 1e-9 and ab16 <= 1e-15, (rel16, ab16)
+    Xd, yed, ierr, fail, st = dev.integrate_trajectories(X0, tt, t9, rho)
+    Xr, yer, ierr_r, fail_r, _ = ref.integrate_trajectories(X0, tt, t9, rho, nthreads=4)
+    assert (ierr == 0).all() and (ierr_r == 0).all() and (fail == -1).all()
+    assert np.abs(Xd.sum(axis=1) - 1.0).max() < 1e-10
+    big = Xr > 1e-12
+    rel = lambda X: (np.abs(X - Xr) * big / np.where(big, Xr, 1.0)).max(axis=1)
+    spread, ye_spread = np.zeros(tr.nz), np.zeros(tr.nz)
+    for trial in (1, 2, 3):
+        t9p = t9 * (1.0 + np.random.default_rng(trial).choice([-1.0, 1.0], size=t9.shape) * 2.2e-16)
+        Xp, yep = ref.integrate_trajectories(X0, tt, t9p, rho, nthreads=4)[:2]
+        spread = np.maximum(spread, rel(Xp))
+        ye_spread = np.maximum(ye_spread, np.abs(yep - yer))
+    assert (rel(Xd) <= np.maximum(4.0 * spread, 1e-6)).all(), (rel(Xd), spread)
+    assert (np.abs(yed - yer) <= np.maximum(4.0 * ye_spread, 1e-8)).all(), (yed - yer, ye_spread)
+
+
 def test_trajectory_entry_within_reference_spread(solver_mod, abi, orc, wl):
     """nuppn_integrate_trajectories (tppnp's trajectory loop for all zones in one launch) against the
     checker's restatement of the same loop, 4 trajectories of 36 points (0 to ~1.2 s): every
