@@ -164,7 +164,7 @@ def run_traj(args, rank, world, local):
     abi = importlib.import_module(PKG + ".abi")
     net = wl.network(1107)
     tr_all = wl.trajectory_batch(args.nz * world, net=net, npts=201)
-    sel = np.arange(rank * args.nz, (rank + 1) * args.nz)
+    sel = importlib.import_module(PKG + ".sharding").zone_shard(args.nz, rank)
     tt, t9, rho = (g[sel] for g in tr_all.grids())
     X0, ye0 = tr_all.X0[sel], tr_all.ye0[sel]
     cfg = {"workload": "tppnp-traj-1107 201 points to 10 s", "trajectories": args.nz * world,
@@ -240,13 +240,9 @@ def run_traj(args, rank, world, local):
     t0 = time.perf_counter()
     _, _, _, _, st_h = S.integrate_trajectories(X0, tt, t9, rho)
     e2e_t, e2e_steps = time.perf_counter() - t0, sum(s.nsucc for s in st_h)
-    if world > 1:
-        red = torch.tensor([t_ms, e2e_t], device="cuda", dtype=torch.float64)
-        dist.all_reduce(red, op=dist.ReduceOp.MAX)
-        t_ms, e2e_t = float(red[0]), float(red[1])
-        red = torch.tensor([steps_done, e2e_steps], device="cuda", dtype=torch.float64)
-        dist.all_reduce(red, op=dist.ReduceOp.SUM)
-        steps_done, e2e_steps = int(red[0]), int(red[1])
+    sharding = importlib.import_module(PKG + ".sharding")
+    t_ms, steps_done = sharding.reduce_time_and_steps(t_ms, steps_done, "cuda", dist if world > 1 else None)
+    e2e_t, e2e_steps = sharding.reduce_time_and_steps(e2e_t, e2e_steps, "cuda", dist if world > 1 else None)
     if rank == 0:
         cfg.update({"accepted_steps_per_call": int(st_np[:, 0].sum()), "rejected_steps_per_call": int(st_np[:, 1].sum()),
                     "failed_trajectories": int((fail.cpu().numpy() >= 0).sum()),
@@ -411,7 +407,7 @@ def main():
     solver = importlib.import_module(PKG + ".solver")
     net = wl.network(1107)
     zb_all = wl.heshell_batch(args.nz * world, net=net, seed=2)
-    zb = zb_all.take(np.arange(rank * args.nz, (rank + 1) * args.nz))  # weak scaling: shard of zones
+    zb = zb_all.take(importlib.import_module(PKG + ".sharding").zone_shard(args.nz, rank))  # weak scaling
     knobs = abi.default_knobs(integration_method=1)
     S = solver.NetworkSolver(net, knobs, device=dev_id)
     nz = zb.nz
@@ -454,13 +450,8 @@ def main():
     kernel_ms = [a.elapsed_time(b) for a, b in ev]
     t_ms = float(sum(kernel_ms))
     gpu_launches = S.launches() - launches0
-    if world > 1:
-        t = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t.item())
-        s = torch.tensor([steps_done], device="cuda", dtype=torch.float64)
-        dist.all_reduce(s, op=dist.ReduceOp.SUM)
-        steps_done = int(s.item())
+    sharding = importlib.import_module(PKG + ".sharding")
+    t_ms, steps_done = sharding.reduce_time_and_steps(t_ms, steps_done, "cuda", dist if world > 1 else None)
     value = steps_done / (t_ms * 1e-3)
 
     # end to end through the host-buffer entry point (host <-> device copies inside)
@@ -476,13 +467,7 @@ def main():
             e2e_steps += sum(s.nsucc for s in st)
     h2d = Xh.nbytes + 6 * 8 * nz + 4 * nz
     d2h = Xh.nbytes + 8 * nz + 4 * nz + 32 * nz + 4 * nz
-    if world > 1:
-        t = torch.tensor([e2e_t], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
-        s = torch.tensor([e2e_steps], device="cuda", dtype=torch.float64)
-        dist.all_reduce(s, op=dist.ReduceOp.SUM)
-        e2e_steps = int(s.item())
+    e2e_t, e2e_steps = sharding.reduce_time_and_steps(e2e_t, e2e_steps, "cuda", dist if world > 1 else None)
     e2e = e2e_steps / e2e_t
 
     if rank == 0:
