@@ -261,6 +261,107 @@ def run_traj(args, rank, world, local):
         dist.destroy_process_group()
 
 
+def run_hburn(args, rank, world):
+    """The ppn frame of one H-burning zone (300-species network, T9 = 0.020, rho = 100, X(H) = 0.70,
+    X(He4) = 0.28, Z = 0.02 solar-scaled): 200 backward-Euler frame steps, dt log-spaced 1e3 .. 1e13 s,
+    each one integrate_network call carrying X, Ye and bd_state. A step is the whole frame; value =
+    accepted sub-steps / time. One zone is one CTA: this measures latency, not throughput."""
+    if rank != 0:
+        return
+    wl = importlib.import_module(PKG + ".workloads")
+    abi = importlib.import_module(PKG + ".abi")
+    net = wl.network(300)
+    zb, dts = wl.hburn_zone(net)
+    kn = abi.default_knobs(integration_method=0)
+    cfg = {"workload": "ppn hburn-300 BE frame: 200 steps, dt 1e3..1e13 s", "zones": 1, "network_species": net.nsp,
+           "integrator": "backward-euler", "lu": "fp64", "launches_per_step": 2 * len(dts)}
+    args_zone = (zb.t9_0, zb.t9_1, zb.rho_0, zb.rho_1)
+    if args.impl == "reference":
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        ref = orc.Oracle(net, kn)
+        times, steps = [], []
+        for it in range(args.warmup + args.steps):
+            X, ye, n = zb.X.copy(), zb.ye.copy(), 0
+            t0 = time.perf_counter()
+            for dt in dts:
+                X, ye, ierr, st, _ = ref.integrate_network(X, *args_zone, ye, dt)
+                n += st[0].nsucc
+            if it >= args.warmup:
+                times.append(time.perf_counter() - t0)
+                steps.append(n)
+        v = sum(steps) / sum(times)
+        print(json.dumps({"impl": "reference", "metric": "zone-timesteps/s", "value": v, "unit": "zone-timesteps/s",
+                          "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+                          "cpu_baseline": {"value": v, "unit": "zone-timesteps/s", "cores": 1, "kind": "port",
+                                           "sample": "the whole frame (one zone: one core)"},
+                          "e2e": {"value": v, "unit": "zone-timesteps/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import torch
+    solver = importlib.import_module(PKG + ".solver")
+    S = solver.NetworkSolver(net, kn, device=torch.cuda.current_device())
+    cu = lambda a, dt=torch.float64: torch.tensor(np.ascontiguousarray(a), dtype=dt, device="cuda")
+    X0d, ye0d = cu(zb.X), cu(zb.ye)
+    zone_d = [cu(a) for a in args_zone]
+    dts_d = cu(dts)
+    X, ye = X0d.clone(), ye0d.clone()
+    n = len(dts)
+    ierr = torch.zeros(n, dtype=torch.int32, device="cuda")
+    stats = torch.zeros((n, 8), dtype=torch.int32, device="cuda")
+    bd = torch.zeros(1, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def one_step():
+        X.copy_(X0d); ye.copy_(ye0d); bd.zero_()
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for i in range(n):
+            S.integrate_device(X, *zone_d, ye, dts_d[i:i + 1], ierr[i:i + 1], stats[i], bd, stream=stream)
+        e1.record()
+        return e0, e1
+
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        for _ in range(args.warmup):
+            one_step()
+        torch.cuda.synchronize()
+        launches0 = S.launches()
+        clk.mark()
+        ev = [one_step() for _ in range(args.steps)]
+        torch.cuda.synchronize()
+    gpu_launches = S.launches() - launches0
+    st_np = stats.cpu().numpy()
+    steps_done = int(st_np[:, 0].sum()) * args.steps
+    t_ms = float(sum(a.elapsed_time(b) for a, b in ev))
+    failed = int(np.count_nonzero(ierr.cpu().numpy()))
+    # end to end: the same frame through nuppn_integrate with host buffers
+    e2e_t, e2e_steps = 0.0, 0
+    for it in range(1 + args.steps):
+        Xh, yeh, m = zb.X.copy(), zb.ye.copy(), 0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for dt in dts:
+            Xh, yeh, ie, st, _ = S.integrate_network(Xh, *args_zone, yeh, dt)
+            m += st[0].nsucc
+        if it >= 1:
+            e2e_t += time.perf_counter() - t0
+            e2e_steps += m
+    print(json.dumps({"metric": "zone-timesteps/s", "value": steps_done / (t_ms * 1e-3), "unit": "zone-timesteps/s",
+                      "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                      "data": "synthetic", "config": dict(cfg, frame_steps_failed=failed,
+                                                          accepted_steps_per_frame=int(st_np[:, 0].sum()),
+                                                          l2="flushed: 256 MiB written before each timed frame"),
+                      "e2e": {"value": e2e_steps / e2e_t, "unit": "zone-timesteps/s",
+                              "h2d_bytes_per_step": int(n * (zb.X.nbytes + 7 * 8)),
+                              "d2h_bytes_per_step": int(n * (zb.X.nbytes + 8 + 4 + 32 + 4))},
+                      "gpu_launches": int(gpu_launches), "clocks": clk.summary()}), flush=True)
+
+
 def run_serve(args, rank, world):
     """Serving: a seeded Poisson stream (args.rate requests/s over args.serve_seconds) of one-zone and
     one-trajectory requests, 40 % He-shell zones (1109 species, BD over 1e10 s), 40 % H-burning zones
@@ -373,9 +474,10 @@ def main():
     ap.add_argument("--ref-zones", type=int, default=32)
     ap.add_argument("--cpu-zones", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="heshell", choices=["heshell", "traj", "serve"],
+    ap.add_argument("--workload", default="heshell", choices=["heshell", "traj", "serve", "hburn"],
                     help="heshell: 1024 He-shell zones (the headline); traj: tppnp-style trajectories; "
-                         "serve: Poisson request stream through nuppn_serve_*")
+                         "serve: Poisson request stream through nuppn_serve_*; hburn: the ppn frame of one "
+                         "H-burning zone (200 backward-Euler frame steps)")
     ap.add_argument("--rate", type=float, default=2000.0, help="serve: mean requests per second")
     ap.add_argument("--serve-seconds", type=float, default=5.0, help="serve: arrival window (s)")
     ap.add_argument("--serve-lanes", type=int, default=0, help="serve: lanes of the 1109-species server (0: 4)")
@@ -390,6 +492,9 @@ def main():
         return
     if args.workload == "serve":
         run_serve(args, rank, world)
+        return
+    if args.workload == "hburn":
+        run_hburn(args, rank, world)
         return
     if args.impl == "reference":
         run_reference(args, rank, world)
