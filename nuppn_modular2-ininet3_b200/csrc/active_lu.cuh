@@ -342,28 +342,54 @@ __device__ void dev_jacobian_active(const DevNet &N, const Ws &W, Act &A, int *s
     sf[t] = set ? 1 : 0;
   }
   __syncthreads();
-  for (int p = w; p < A.nnz; p += nw) {
+  // Short entries: one thread each, summed in the static list's order from 1e-99 (the reference's
+  // accumulation: jac = 1e-99, then += each contribution in reaction order, jac_rhs.F90:309-392).
+  // Long entries (a few: among n, p, alpha) are listed and summed by a warp each from P.
+  constexpr int kMaxLong = 128;
+  __shared__ int s_nlong;
+  __shared__ int s_longp[kMaxLong];
+  if (tid == 0) s_nlong = 0;
+  __syncthreads();
+  for (int p = tid; p < A.nnz; p += nt) {
     const int e = N.lu_src[A.csrc[p]];
     if (e < 0) {
-      if (lane == 0) {
-        A.jval[p] = 0.0;
-        A.jflag[p] = JF_FILL;
-      }
+      A.jval[p] = 0.0;
+      A.jflag[p] = JF_FILL;
       continue;
     }
+    if (N.jg_ptr[e + 1] - N.jg_ptr[e] > kLongList) {
+      const int k = atomicAdd(&s_nlong, 1);
+      if (k < kMaxLong) s_longp[k] = p;
+      continue;
+    }
+    double acc = 1.e-99;
+    int set = 0;
+    for (int t = off[p]; t < off[p + 1]; ++t) {
+      acc = acc + dv[t];
+      set |= sf[t];
+    }
+    A.jval[p] = acc;
+    A.jflag[p] = (uint8_t)((set ? JF_SET : 0) | (N.jdiag[N.jrow[e]] == e ? JF_DIAG : 0));
+  }
+  __syncthreads();
+  const int nlong = s_nlong;
+  const int nwork = nlong <= kMaxLong ? nlong : A.nnz;  // more than kMaxLong: scan every position
+  for (int k = w; k < nwork; k += nw) {
+    const int p = nlong <= kMaxLong ? s_longp[k] : k;
+    const int e = N.lu_src[A.csrc[p]];
+    if (e < 0 || N.jg_ptr[e + 1] - N.jg_ptr[e] <= kLongList) continue;
     double acc = 0.0;
     int set = 0;
-    if (N.jg_ptr[e + 1] - N.jg_ptr[e] <= kLongList) {
-      for (int t = off[p] + lane; t < off[p + 1]; t += 32) {
-        acc += dv[t];
-        set |= sf[t];
-      }
-    } else {
-      for (int i = lane; i < A.nP * 8; i += 32) {
-        const int a = A.Plist[i >> 3], s = i & 7;
-        if (N.act_ice[(size_t)a * 8 + s] == e) {
+    for (int i = lane; i < A.nP; i += 32) {  // a lane takes whole reactions: their 8 targets in 2 loads
+      const int a = A.Plist[i];
+      const int4 *ice = reinterpret_cast<const int4 *>(N.act_ice + (size_t)a * 8);
+      const int4 u = ice[0], v = ice[1];
+      const int tg[8] = {u.x, u.y, u.z, u.w, v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int sl = 0; sl < 8; ++sl) {
+        if (tg[sl] == e) {
           bool st;
-          acc += jac_contrib(N, W, a, s, st);
+          acc += jac_contrib(N, W, a, sl, st);
           set |= st ? 1 : 0;
         }
       }
