@@ -97,30 +97,86 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def measured_traffic_per_zone():
-    """DRAM bytes per zone of k_integrate from the committed ncu summary (None if absent)."""
-    p = os.path.join(ROOT, "profiles", "k_integrate_heshell1107_256_memory.md")
+def profile_value(name, key):
+    """A `key = value` line of a committed ncu summary under profiles/ (None if absent)."""
+    p = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(p):
-            if line.startswith("traffic_bytes_per_zone"):
-                return int(line.split("=")[1])
+            if line.startswith(key + " ="):
+                return float(line.split("=")[1])
     except OSError:
         pass
     return None
 
 
-def algorithmic_bytes(info, stats_np, nre_active, nsp):
-    """Bytes a zone-step must move at minimum (per-zone arrays, each read/written once per use):
-    8 * [ rates (R+3) + per Jacobian nnzJ + per factorization (nnzJ + nnzLU)
-          + per RHS+solve (R + 3N + nnzLU) ]."""
-    R, N, nnzJ, nnzLU = nre_active, nsp, info.nnz_jac, info.nnz_lu
-    nsucc, nfail, nfact, nsolve = (stats_np[:, i].astype(np.int64) for i in (0, 1, 3, 4))
-    per_zone = (R + 3) + (nsucc + nfail) * nnzJ + nfact * (nnzJ + nnzLU) + nsolve * (R + 3 * N + nnzLU)
-    return 8 * int(per_zone.sum())
+HESHELL_PROFILE = "k_integrate_heshell1107_256_memory.md"
+
+
+def measured_traffic_per_zone():
+    """DRAM bytes per zone of k_integrate from the committed ncu summary (None if absent)."""
+    v = profile_value(HESHELL_PROFILE, "traffic_bytes_per_zone")
+    return int(v) if v is not None else None
+
+
+def model_bytes(nz, nsp, arena_bytes):
+    """Bytes the integration must move between HBM and the SMs per launch, at minimum: each zone's
+    abundances in and out (2 * nsp doubles), its six input scalars (T9 and rho at both ends, Ye,
+    dtwant), its outputs (Ye, ierr, 8 counters, the Bader-Deuflhard state) and the zone-shared network
+    arena once. Everything else a zone touches (rates, Jacobian, LU, extrapolation tableau) is
+    per-zone working state that an ideal kernel keeps on chip."""
+    per_zone = 2 * nsp * 8 + 6 * 8 + 8 + 4 + 8 * 4 + 2 * 4
+    return nz * per_zone + arena_bytes
+
+
+def roofline(nz, nsp, arena_bytes, per_launch_s, peak_gbs, peak_kind, sm_mhz, n_sm=148):
+    """The `roofline` object of the bench line. bound "hbm": achieved = model bytes per launch /
+    launch time, against the measured HBM copy bandwidth. traffic = ncu DRAM bytes per zone (a 256-zone
+    capture) times the zones. The kernel is bound by per-zone dependency chains, not by either
+    peak; fp64_pipe_frac = FP64-pipe warp instructions (ncu, per zone, times the zones) / (SMs x the
+    pipe's peak per SM cycle x SM clock x launch time) shows how much of the FP64 pipe it uses."""
+    model = model_bytes(nz, nsp, arena_bytes)
+    achieved = model / per_launch_s / 1e9
+    tpz = measured_traffic_per_zone()
+    traffic = tpz * nz if tpz else None
+    out = {"bound": "hbm", "achieved": achieved, "peak": peak_gbs, "unit": "GB/s", "frac": achieved / peak_gbs,
+           "traffic": traffic, "peak_source": peak_kind, "kernel": "k_integrate",
+           "algorithmic_bytes_per_launch": model,
+           "model": "per zone 2*nsp*8 (X in, out) + 100 B of scalars; network arena once per launch",
+           "dram_achieved_gbs": (traffic / per_launch_s / 1e9) if traffic else None,
+           "dram_frac": (traffic / per_launch_s / 1e9 / peak_gbs) if traffic else None,
+           "traffic_source": "ncu dram__bytes_read+write per zone at 256 zones, x zones"}
+    fp64 = profile_value(HESHELL_PROFILE, "fp64_inst_per_zone")
+    fp64_peak = profile_value(HESHELL_PROFILE, "fp64_inst_peak_per_sm_cycle")
+    if fp64 and fp64_peak and sm_mhz:
+        out["fp64_pipe_frac"] = fp64 * nz / (n_sm * fp64_peak * sm_mhz * 1e6 * per_launch_s)
+        out["fp64_source"] = "ncu sm__inst_executed_pipe_fp64 per zone at 256 zones, x zones"
+    return out
+
+
+def heshell_config(nz_total, nsp):
+    """The workload both arms print in `config` (the same dict, so the arms are the same config)."""
+    return {"workload": "heshell-1107 BD 1e10 s", "zones": int(nz_total), "network_species": int(nsp),
+            "integrator": "bader-deuflhard", "arithmetic": "fp64"}
+
+
+def parity_sample(zb, n):
+    """A fixed sample of n zones for the checker: the 8 hottest (the costliest and least well-conditioned
+    zones) and the rest evenly spaced over the batch, in batch order."""
+    n = min(n, zb.nz)
+    hot = np.argsort(-np.maximum(zb.t9_0, zb.t9_1), kind="stable")[:min(8, n)]
+    rest = np.setdiff1d(np.arange(zb.nz), hot)
+    pick = rest[np.linspace(0, rest.size - 1, max(n - hot.size, 0)).astype(int)] if n > hot.size else rest[:0]
+    return np.sort(np.concatenate([hot, pick]))
+
+
+# The reference arm integrates the whole batch every step when it has at most this many zones (about
+# 4 s a step on 16 host cores for the 1024-zone batch), else this many zones of it.
+REF_MAX_ZONES = 1024
 
 
 def run_reference(args, rank, world):
-    """CPU reference arm: the checker (restated FP64 path + reference SuperLU), all host threads."""
+    """CPU reference arm: the checker (restated FP64 path + reference SuperLU), all host threads, on the
+    same batch as the GPU arm (the whole batch up to REF_MAX_ZONES zones per step)."""
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -128,10 +184,14 @@ def run_reference(args, rank, world):
     wl = importlib.import_module(PKG + ".workloads")
     abi = importlib.import_module(PKG + ".abi")
     net = wl.network(1107)
-    zb = wl.heshell_batch(args.nz, net=net, seed=2)
+    nz_total = args.nz * world
+    zb = wl.heshell_batch(nz_total, net=net, seed=2)
     cores = os.cpu_count() or 1
-    sample = min(args.nz, max(cores, args.ref_zones))
-    sub = zb.take(np.arange(sample))
+    sample = min(nz_total, REF_MAX_ZONES)
+    idx = np.arange(nz_total) if sample == nz_total else parity_sample(zb, sample)
+    # hottest first: the checker's threads take zones from a shared counter, so the costliest start first
+    idx = idx[np.argsort(-zb.t9_0[idx], kind="stable")]
+    sub = zb.take(idx)
     ref = orc.Oracle(net, abi.default_knobs(integration_method=1))
     times, steps = [], []
     for it in range(args.warmup + args.steps):
@@ -143,15 +203,15 @@ def run_reference(args, rank, world):
             times.append(dt)
             steps.append(sum(s.nsucc for s in st))
     v = sum(steps) / sum(times)
+    what = "all" if sample == nz_total else f"{sample} (the 8 hottest and evenly spaced others) of"
     line = {"impl": "reference", "metric": "zone-timesteps/s", "value": v, "unit": "zone-timesteps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "heshell-1107 BD 1e10 s", "zones": args.nz, "sample_zones": sample,
-                       "network_species": net.nsp, "integrator": "bader-deuflhard"},
+            "config": heshell_config(nz_total, net.nsp),
             "cpu_baseline": {"value": v, "unit": "zone-timesteps/s", "cores": cores, "kind": "port",
-                             "sample": f"{sample} of {args.nz} zones per step, restated FP64 path + "
-                                       f"reference SuperLU 5.0"},
+                             "sample": f"{what} {nz_total} zones per step, restated FP64 path + "
+                                       f"reference SuperLU 5.0, one zone per thread"},
             "e2e": {"value": v, "unit": "zone-timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -471,7 +531,6 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nz", type=int, default=1024)
-    ap.add_argument("--ref-zones", type=int, default=32)
     ap.add_argument("--cpu-zones", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="heshell", choices=["heshell", "traj", "serve", "hburn"],
@@ -577,63 +636,67 @@ def main():
 
     if rank == 0:
         peak, peak_kind = load_peaks()
-        nre_active = int(net.considerreaction.sum())
-        bytes_per_launch = algorithmic_bytes(S.info, st_np, nre_active, net.nsp)
         per_launch_s = (sum(kernel_ms) / len(kernel_ms)) * 1e-3
-        achieved = bytes_per_launch / per_launch_s / 1e9
-        tpz = measured_traffic_per_zone()
-        traffic = tpz * nz if tpz else None
+        clocks = clk.summary()
         line = {
             "metric": "zone-timesteps/s", "value": value, "unit": "zone-timesteps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "heshell-1107 BD 1e10 s", "zones": nz * world, "zones_per_gpu": nz,
-                       "network_species": net.nsp, "nnz_jac": S.info.nnz_jac, "nnz_lu": S.info.nnz_lu,
-                       "integrator": "bader-deuflhard", "lu": "fp64",
-                       "l2": "flushed: 256 MiB written before each timed call",
-                       "accepted_steps_per_call": int(st_np[:, 0].sum()),
-                       "rejected_steps_per_call": int(st_np[:, 1].sum())},
+            "config": heshell_config(nz * world, net.nsp),
+            "run": {"zones_per_gpu": nz, "nnz_jac": S.info.nnz_jac, "nnz_lu": S.info.nnz_lu, "lu": "fp64",
+                    "l2": "flushed: 256 MiB written before each timed call",
+                    "accepted_steps_per_call": int(st_np[:, 0].sum()),
+                    "rejected_steps_per_call": int(st_np[:, 1].sum())},
             "gpu_launches": int(gpu_launches),
             "e2e": {"value": e2e, "unit": "zone-timesteps/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": peak_kind, "kernel": "k_integrate",
-                         "algorithmic_bytes_per_launch": bytes_per_launch,
-                         "dram_achieved_gbs": (traffic / per_launch_s / 1e9) if traffic else None,
-                         "traffic_source": "ncu dram__bytes_read+write per zone at 256 zones, x zones",
-                         "note": "algorithmic bytes count the full-network sweeps (R + 3N + nnzLU per "
-                                 "substep) of the reference formulation; the kernel keeps each zone's "
-                                 "active subsystem on chip, so traffic is far below them and the "
-                                 "kernel is latency-bound"},
-            "clocks": clk.summary(),
+            "roofline": roofline(nz, net.nsp, S.arena_bytes, per_launch_s, peak, peak_kind, clocks.get("sm_mhz")),
+            "clocks": clocks,
         }
         if not args.no_cpu:
-            line["cpu_baseline"] = cpu_baseline(net, zb, args.cpu_zones)
+            dev_out = (X.cpu().numpy(), ierr.cpu().numpy(), st_np[:, 0])
+            line["cpu_baseline"], line["error_vs_oracle"] = cpu_baseline(net, zb, args.cpu_zones, dev_out)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
 
 
-def cpu_baseline(net, zb, nzones):
-    """The checker on the host cores, a bounded sample of the same workload."""
+def cpu_baseline(net, zb, nzones, dev_out):
+    """The checker on the host cores, on a fixed sample of the same workload (the 8 hottest zones and
+    evenly spaced others): its throughput, and the device results of those zones against it
+    (dev_out = final X, ierr and accepted steps of every zone from the last timed call). Zones beyond
+    1e-6 are also measured against the checker's own spread under 1-ulp changes of their input."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
+    import parity
     abi = importlib.import_module(PKG + ".abi")
     if not orc.available():
-        return {"value": None, "unit": "zone-timesteps/s", "cores": 0, "kind": "port", "sample": "unavailable"}
+        return ({"value": None, "unit": "zone-timesteps/s", "cores": 0, "kind": "port", "sample": "unavailable"},
+                None)
     cores = os.cpu_count() or 1
-    n = min(zb.nz, max(nzones, cores))
-    sub = zb.take(np.arange(n))
+    idx = parity_sample(zb, max(nzones, cores))
+    sub = zb.take(idx)
     ref = orc.Oracle(net, abi.default_knobs(integration_method=1))
     t0 = time.perf_counter()
-    X, ye, ierr, st, _ = ref.integrate_network(sub.X, sub.t9_0, sub.t9_1, sub.rho_0, sub.rho_1, sub.ye,
-                                               sub.dtwant, nthreads=cores)
+    Xr, ye, ierr_r, st, _ = ref.integrate_network(sub.X, sub.t9_0, sub.t9_1, sub.rho_0, sub.rho_1, sub.ye,
+                                                  sub.dtwant, nthreads=cores)
     dt = time.perf_counter() - t0
-    return {"value": sum(s.nsucc for s in st) / dt, "unit": "zone-timesteps/s", "cores": cores, "kind": "port",
-            "sample": f"{n} zones of the same batch (restated FP64 path + reference SuperLU), {dt:.1f} s"}
+    nsucc_r = np.array([s.nsucc for s in st])
+    base = {"value": int(nsucc_r.sum()) / dt, "unit": "zone-timesteps/s", "cores": cores, "kind": "port",
+            "sample": f"{len(idx)} zones of the batch (the 8 hottest and evenly spaced others; restated FP64 "
+                      f"path + reference SuperLU), {dt:.1f} s"}
+    X, ierr, nsucc = (a[idx] for a in dev_out)
+    rel, ab = parity.zone_errors(X, Xr)
+    off = np.nonzero((rel > parity.REL_TOL) | (ab > parity.ABS_TOL))[0]
+    spread = np.zeros(len(idx))
+    if off.size:
+        spread[off] = parity.checker_spread(ref, sub.take(off), Xr[off], nthreads=cores)
+    err = parity.summary(X, ierr, nsucc, Xr, ierr_r, nsucc_r, spread)
+    err["sample"] = f"{len(idx)} zones: the 8 hottest and evenly spaced others"
+    err["spread"] = "per zone beyond 1e-6: max relative change of the checker under +-1-ulp input changes, 2 draws"
+    return base, err
 
 
 if __name__ == "__main__":

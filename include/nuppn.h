@@ -194,6 +194,8 @@ nuppn_status nuppn_net_create(const nuppn_net_desc *desc, const nuppn_knobs *kno
                               nuppn_net **out);
 nuppn_status nuppn_net_destroy(nuppn_net *net);
 nuppn_status nuppn_net_info_get(const nuppn_net *net, nuppn_net_info *info);
+/* Replaces the knobs for later calls. threads_per_zone sets the CTA size and the workspace layout at
+ * nuppn_net_create and cannot change afterwards (NUPPN_ERR_ARG if it differs from the handle's). */
 nuppn_status nuppn_set_knobs(nuppn_net *net, const nuppn_knobs *knobs);
 
 /* Static Jacobian pattern of makemap (jac_rhs.F90:461-540): row/col (0-based) of each COO entry in
@@ -284,7 +286,9 @@ nuppn_status nuppn_integrate_trajectories_device(nuppn_net *net, int32_t nz, int
  * on a device shares the array, so calls whose kernels overlap on the GPU (other streams, other
  * handles, other host threads) race: order them on one stream or synchronize between them.
  * The first call on a device looks up the array's address on that device (which may load the
- * library's device code); make that first call before any stream capture. */
+ * library's device code); make that first call before any stream capture. The address is kept for
+ * the life of the process: after cudaDeviceReset (which also frees every handle's device memory, so
+ * the handles themselves are no longer usable) create new handles in a new process, not this one. */
 #define NUPPN_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
 nuppn_status nuppn_integrate_device_noalloc(nuppn_net *net, int32_t nz, double *d_X, int32_t ldx,
                                             const double *d_t9_0, const double *d_t9_1,

@@ -392,6 +392,10 @@ nuppn_status nuppn_set_knobs(nuppn_net *net, const nuppn_knobs *knobs) {
     set_error("i_nse = 1 needs protons and Ni56 among the considered species");
     return NUPPN_ERR_NET;
   }
+  if (knobs->threads_per_zone != net->H.kn.threads_per_zone) {  // fixes the CTA size and workspace
+    set_error("threads_per_zone takes effect only at nuppn_net_create");
+    return NUPPN_ERR_ARG;
+  }
   double old_dgrd = net->H.kn.dgrd;
   net->H.kn = *knobs;
   if (knobs->dgrd != old_dgrd) bd_constants(net->H);

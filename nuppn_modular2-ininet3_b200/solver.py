@@ -105,6 +105,9 @@ class NetworkSolver:
         info = abi.NetInfo()
         self._check(self.L.nuppn_net_info_get(self.h, C.byref(info)))
         self.info = info
+        # right after creation the handle holds only the zone-shared network arena (and a 256-byte
+        # zone counter): the workspace and staging buffers are allocated by the first call
+        self.arena_bytes = int(info.device_bytes)
 
     def _check(self, st):
         if st != 0:

@@ -36,3 +36,19 @@ def test_clock_summary_uses_timed_rows_only():
     assert s["samples"] == 3 and s["sm_mhz"] == 1965.0 and s["sm_max_mhz"] == 1965.0 and s["reasons"] == []
     c.t0, c.t1 = now + 20.0, now + 30.0
     assert c.summary()["reasons"] == ["unsampled"]
+
+
+def test_roofline_model_is_below_measured_traffic():
+    """The roofline's algorithmic bytes are the compulsory HBM traffic of the integration (abundances in
+    and out, scalars, the network arena once): they cannot exceed what ncu measured the kernel moving,
+    so at any launch time the model's fraction of HBM peak stays below the measured DRAM fraction and
+    below 1."""
+    b = _bench()
+    nz, nsp, arena = 1024, 1109, 8 << 20
+    tpz = b.measured_traffic_per_zone()
+    assert b.model_bytes(nz, nsp, arena) <= tpz * nz
+    for per_launch_s in (1e-4, 1e-3, 0.034):
+        r = b.roofline(nz, nsp, arena, per_launch_s, 6542.0, "measured", 1965.0)
+        assert r["bound"] == "hbm" and r["unit"] == "GB/s"
+        assert abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-12
+        assert r["frac"] <= r["dram_frac"] and r["frac"] <= 1.0

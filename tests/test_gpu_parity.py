@@ -290,6 +290,42 @@ def test_integrate_bd_hot_zones_within_reference_spread(solver_mod, abi, orc, wl
     assert (rel(X) <= np.maximum(2.0 * spread, 1e-6)).all(), (rel(X), spread)
 
 
+def _heshell_sample(zb, n):
+    """The 8 hottest zones of the batch and n - 8 evenly spaced others (bench.py's checker sample)."""
+    hot = np.argsort(-zb.t9_0, kind="stable")[:8]
+    rest = np.setdiff1d(np.arange(zb.nz), hot)
+    return np.sort(np.concatenate([hot, rest[np.linspace(0, rest.size - 1, n - 8).astype(int)]]))
+
+
+def test_heshell_batch_error_vs_checker(solver_mod, abi, orc, wl):
+    """64 zones of the benchmarked He-shell batch (1109 species, Bader-Deuflhard over 1e10 s): the 8
+    hottest and 56 evenly spaced others. Every zone succeeds on both sides and conserves mass. A zone
+    whose checker result moves by less than 1e-6 under 1-ulp input changes must be within 1e-6
+    relative (X > 1e-12) and 1e-15 absolute of the checker; a zone that the checker itself cannot pin
+    to 1e-6 must lie within twice that spread (on the checker's side 26 of these 64 zones, nearly all
+    with T9 > 0.24, move by more than 1e-6 under 1-ulp changes, by up to 72 %)."""
+    import parity
+
+    net = wl.network(1107)
+    full = wl.heshell_batch(1024, net=net, seed=2)
+    zb = full.take(_heshell_sample(full, 64))
+    args = (zb.t9_0, zb.t9_1, zb.rho_0, zb.rho_1, zb.ye, zb.dtwant)
+    ref = orc.Oracle(net, abi.default_knobs(integration_method=1))
+    Xr, _, ierr_r, st_r, _ = ref.integrate_network(zb.X, *args, nthreads=8)
+    dev = _dev(solver_mod, net, abi, integration_method=1)
+    X, _, ierr, st, _ = dev.integrate_network(zb.X, *args)
+    assert (ierr == 0).all() and (ierr_r == 0).all(), (ierr, ierr_r)
+    assert np.abs(X.sum(axis=1) - 1.0).max() < 1e-10
+    rel, ab = parity.zone_errors(X, Xr)
+    off = np.nonzero((rel > 1e-6) | (ab > 1e-15))[0]
+    spread = np.zeros(zb.nz)
+    if off.size:
+        spread[off] = parity.checker_spread(ref, zb.take(off), Xr[off], nthreads=8)
+    pinned = spread < 1e-6
+    assert (rel[pinned] <= 1e-6).all() and (ab[pinned] <= 1e-15).all(), (rel[pinned].max(), ab[pinned].max())
+    assert (rel[~pinned] <= 2.0 * spread[~pinned]).all(), (rel[~pinned], spread[~pinned])
+
+
 def test_nse_matches_checker(solver_mod, abi, orc, wl):
     """compute_nse on the device (nuppn_nse) against the checker: same outcome, X within 1e-9 relative
     for X > 1e-12 and the chemical potentials within 1e-9 (isotope sums differ in rounding order)."""
