@@ -93,12 +93,19 @@ typedef struct nuppn_knobs {
   int32_t lu_precision;        /* 0 = FP64 factor, 1 = FP32 factor + FP64 iterative refinement */
   int32_t ir_max_iters;        /* refinement sweeps per solve in mode 1 (default 3)           */
   double ir_rtol;              /* refinement stops when |dx| <= ir_rtol*|x| (default 1e-14)   */
-  int32_t threads_per_zone;    /* CTA size (0 = library choice)                               */
+  int32_t threads_per_zone;    /* threads that integrate one zone: 32 = one warp per zone, with
+                                  zones_per_cta zones in each CTA; 64..256 (a multiple of 32) =
+                                  one CTA of that size per zone; 0 = one CTA of 256 per zone     */
   int32_t lu_onewarp_max;      /* active systems up to this size are factored/solved by one warp
                                   (0 = library default; larger ones use sync-free multi-warp)    */
   int32_t lu_tile_max;         /* active systems up to this size (at most 64) are factored in a
                                   dense tile and solved in registers (0 = 64, negative = never)  */
-  int32_t reserved[5];
+  int32_t zones_per_cta;       /* one warp per zone: warps (zones) per CTA, 1..8 (0 = 8)         */
+  int32_t zone_smem;           /* shared-memory bytes for each zone's active subsystem (0 =
+                                  library choice: 72 KB per CTA, or the CTA's 216 KB split evenly
+                                  among its zones); a zone whose system does not fit uses its
+                                  global workspace                                                */
+  int32_t reserved[3];
 } nuppn_knobs;
 
 /* Network description in the reference's slot layout (what rnetw2007, reaclib_init, netgen_init,
@@ -299,6 +306,29 @@ nuppn_status nuppn_integrate_device_noalloc(nuppn_net *net, int32_t nz, double *
 /* Number of kernel launches issued by the library since the handle was created (server launches
  * are counted by nuppn_serve_info). */
 int64_t nuppn_launch_count(const nuppn_net *net);
+
+/* ---- Autotuning of the integration kernel's shape ---------------------------------------------
+ * No counterpart in the reference (one zone per MPI rank, no kernel to shape). The integration
+ * kernel runs either one zone per CTA (every warp of the CTA shares the zone's wide phases, one warp
+ * walks its dependency chains) or one zone per warp (each warp does all of its zone's work; several
+ * zones per CTA). Which is faster depends on the network, on how many zones a call carries and on
+ * how uneven their costs are, so nuppn_autotune measures it: it integrates the caller's batch (or
+ * its first `sample` zones, 0 = all) once with each candidate shape from the same inputs, timed
+ * with CUDA events, and keeps the shape with the most accepted zone sub-steps per second. Host
+ * buffers as for nuppn_integrate; the inputs are not modified. The chosen shape is applied to the
+ * handle (as nuppn_set_knobs would; the other knobs are unchanged). If `report` is not NULL, up to
+ * `ncand` candidates are written there and *nreport gets their number. */
+typedef struct nuppn_tune_result {
+  int32_t threads_per_zone, zones_per_cta, zone_smem; /* the candidate's shape knobs                */
+  int32_t zones_per_sm;                               /* zones resident per SM with that shape      */
+  double ms;                                          /* one call over the sample                    */
+  double zone_steps_per_s;                            /* accepted sub-steps per second               */
+  int32_t chosen, reserved;
+} nuppn_tune_result;
+nuppn_status nuppn_autotune(nuppn_net *net, int32_t nz, const double *X, int32_t ldx, const double *t9_0,
+                            const double *t9_1, const double *rho_0, const double *rho_1, const double *ye,
+                            const double *dtwant, int32_t sample, nuppn_tune_result *report, int32_t ncand,
+                            int32_t *nreport);
 
 /* ---- Serving: continuous batching of independent requests ------------------------------------
  * Each request is one call of integrate_network (solver.F90:53) for one zone, or one tppnp

@@ -37,7 +37,8 @@ class Knobs(C.Structure):
                 ("lu_precision", C.c_int32), ("ir_max_iters", C.c_int32),
                 ("ir_rtol", C.c_double), ("threads_per_zone", C.c_int32),
                 ("lu_onewarp_max", C.c_int32), ("lu_tile_max", C.c_int32),
-                ("reserved", C.c_int32 * 5)]
+                ("zones_per_cta", C.c_int32), ("zone_smem", C.c_int32),
+                ("reserved", C.c_int32 * 3)]
 
 
 def default_knobs(**over) -> Knobs:
@@ -103,6 +104,12 @@ class ServeStats(C.Structure):
     _fields_ = [("lanes", C.c_int32), ("max_batch", C.c_int32), ("slots_per_lane", C.c_int32),
                 ("pending", C.c_int32), ("in_flight", C.c_int32), ("launches", C.c_int64),
                 ("batches", C.c_int64), ("completed", C.c_int64), ("device_bytes", C.c_int64)]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("threads_per_zone", C.c_int32), ("zones_per_cta", C.c_int32), ("zone_smem", C.c_int32),
+                ("zones_per_sm", C.c_int32), ("ms", C.c_double), ("zone_steps_per_s", C.c_double),
+                ("chosen", C.c_int32), ("reserved", C.c_int32)]
 
 
 class NetInfo(C.Structure):

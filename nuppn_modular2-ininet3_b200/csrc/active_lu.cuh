@@ -18,7 +18,7 @@
 // registers of one warp; larger ones use the sparse row-oriented factorization.
 #pragma once
 
-namespace nuppn {
+NUPPN_BEGIN
 
 constexpr int kSpinLimit = 1 << 22;  // per wait; a timeout marks the zone as failed, never hangs
 
@@ -119,14 +119,14 @@ __device__ __forceinline__ void act_bind(Act &A, char *base, int na, int nnz, in
 // Exclusive scan of v[0..n) in place (block-wide, deterministic); returns the total. Each warp takes
 // a contiguous segment and walks it 32 elements at a time, so every load and store is coalesced.
 __device__ int block_scan_excl(int *v, int n, int *sint) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int lane = GT & 31, w = GT >> 5, nw = GN >> 5;
   const int seg = (n + nw - 1) / nw, b0 = min(n, w * seg), b1 = min(n, b0 + seg);
   int tot = 0;
   for (int i = b0 + lane; i < b1; i += 32) tot += v[i];
   for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(NUPPN_FULL, tot, o);
-  __syncthreads();  // sint may still be read by the previous scan
+  GSYNC();  // sint may still be read by the previous scan
   if (lane == 0) sint[w] = tot;
-  __syncthreads();
+  GSYNC();
   int base = 0, total = 0;
   for (int i = 0; i < nw; ++i) {
     if (i < w) base += sint[i];
@@ -143,7 +143,7 @@ __device__ int block_scan_excl(int *v, int n, int *sint) {
     if (i < b1) v[i] = base + incl - x;
     base += __shfl_sync(NUPPN_FULL, incl, 31);
   }
-  __syncthreads();
+  GSYNC();
   return total;
 }
 
@@ -170,25 +170,25 @@ __device__ __forceinline__ bool spin_until(const int *flag, int gen) {
 
 // Compact the active subsystem after the mask is known. smem/smem_bytes: the CTA's budget.
 __device__ void dev_compact(const DevNet &N, const Ws &W, Act &A, char *smem, size_t smem_bytes, int *sint) {
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
+  const int tid = GT, nt = GN, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
   int *sys2c = W.act_tmp;                  // [nsys]
   int *tmp_arow = W.act_tmp + N.nsys + 1;  // [nsys]
   int *cnt = W.act_tmp + 2 * (N.nsys + 1); // [nsys+1]
   for (int i = tid; i < N.nsys; i += nt) sys2c[i] = W.mask[N.sp_of_sys[i]] ? 1 : 0;
-  __syncthreads();
+  GSYNC();
   const int na = block_scan_excl(sys2c, N.nsys, sint);
   for (int i = tid; i < N.nsys; i += nt) {
     if (W.mask[N.sp_of_sys[i]]) tmp_arow[sys2c[i]] = i;
     else sys2c[i] = -1;
   }
-  __syncthreads();
+  GSYNC();
   for (int c = w; c < na; c += nw) {  // entries per active row: static entries in active columns
     int i = tmp_arow[c], n = 0;
     for (int p = N.lu_rowptr[i] + lane; p < N.lu_rowptr[i + 1]; p += 32) n += sys2c[N.lu_col[p]] >= 0;
     for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(NUPPN_FULL, n, o);
     if (lane == 0) cnt[c] = n;
   }
-  __syncthreads();
+  GSYNC();
   const int nnz = block_scan_excl(cnt, na, sint);
   const int trows = tile_rows_for(na, N.kn.lu_tile_max);
   const bool mixed = N.kn.lu_precision == 1 && trows > 0;
@@ -228,7 +228,7 @@ __device__ void dev_compact(const DevNet &N, const Ws &W, Act &A, char *smem, si
       base += __popc(m);
     }
   }
-  __syncthreads();
+  GSYNC();
   A.onewarp = na <= (N.kn.lu_onewarp_max > 0 ? N.kn.lu_onewarp_max : kOneWarpMax);
   A.onewarp_f = na <= (N.kn.lu_onewarp_max > 0 ? N.kn.lu_onewarp_max : kOneWarpFactorMax);
 }
@@ -275,7 +275,7 @@ __device__ __forceinline__ double jac_contrib(const DevNet &N, const Ws &W, int 
 // Jacobian (jac_rhs.F90:350-392); a passing reaction masks all its participants, so P is part of K.
 // Both lists are in flattened order (active row, then reaction index).
 __device__ void dev_active_reactions(const DevNet &N, const Ws &W, Act &A, int *sint) {
-  const int tid = threadIdx.x, nt = blockDim.x, na = A.na, g = N.ig;
+  const int tid = GT, nt = GN, na = A.na, g = N.ig;
   int *off = W.rx;                  // [na+1]
   int *ra = off + (N.nsys + 1);     // [T] reaction of each flattened position
   int *kf = ra + (N.nact + 1);      // [T+1] kept flags, then their positions
@@ -286,10 +286,10 @@ __device__ void dev_active_reactions(const DevNet &N, const Ws &W, Act &A, int *
     const int s = N.sp_of_sys[A.arow[c]];
     off[c] = N.k1_ptr[s + 1] - N.k1_ptr[s];
   }
-  __syncthreads();
+  GSYNC();
   const int T = block_scan_excl(off, na, sint);
   if (tid == 0) off[na] = T;
-  __syncthreads();
+  GSYNC();
   for (int t = tid; t < T; t += nt) {
     const int c = seg_of(off, na, t);
     const int a = N.k1_list[N.k1_ptr[N.sp_of_sys[A.arow[c]]] + (t - off[c])];
@@ -298,21 +298,21 @@ __device__ void dev_active_reactions(const DevNet &N, const Ws &W, Act &A, int *
     kf[t] = (k3 == g || W.mask[k3]) ? 1 : 0;
     pf[t] = W.flux[a] != 0.0 ? 1 : 0;
   }
-  __syncthreads();
+  GSYNC();
   const int nK = block_scan_excl(kf, T, sint);
   const int nP = block_scan_excl(pf, T, sint);
   if (tid == 0) {
     kf[T] = nK;
     pf[T] = nP;
   }
-  __syncthreads();
+  GSYNC();
   for (int t = tid; t < T; t += nt) {
     if (kf[t + 1] > kf[t]) A.Klist[kf[t]] = ra[t];
     if (pf[t + 1] > pf[t]) A.Plist[pf[t]] = ra[t];
   }
   A.nK = nK;
   A.nP = nP;
-  __syncthreads();
+  GSYNC();
 }
 
 // Jacobian values (1e-99 + the contributions of every passing reaction, as in the reference) and
@@ -320,17 +320,17 @@ __device__ void dev_active_reactions(const DevNet &N, const Ws &W, Act &A, int *
 // evaluate it as one flattened, block-parallel list; the few entries with long lists (among n, p
 // and alpha) take their contributions from the passing reactions P. Each entry is summed by a warp.
 __device__ void dev_jacobian_active(const DevNet &N, const Ws &W, Act &A, int *sint) {
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
+  const int tid = GT, nt = GN, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
   int *off = W.act_otmp;  // [nnz+1] <= nnzLU + 1
   for (int p = tid; p < A.nnz; p += nt) {
     const int e = N.lu_src[A.csrc[p]];
     const int len = e >= 0 ? N.jg_ptr[e + 1] - N.jg_ptr[e] : 0;
     off[p] = len <= kLongList ? len : 0;
   }
-  __syncthreads();
+  GSYNC();
   const int T = block_scan_excl(off, A.nnz, sint);
   if (tid == 0) off[A.nnz] = T;
-  __syncthreads();
+  GSYNC();
   double *dv = W.act_dtmp;
   uint8_t *sf = W.act_btmp;
   for (int t = tid; t < T; t += nt) {
@@ -341,15 +341,17 @@ __device__ void dev_jacobian_active(const DevNet &N, const Ws &W, Act &A, int *s
     dv[t] = jac_contrib(N, W, it >> 3, it & 7, set);
     sf[t] = set ? 1 : 0;
   }
-  __syncthreads();
+  GSYNC();
   // Short entries: one thread each, summed in the static list's order from 1e-99 (the reference's
   // accumulation: jac = 1e-99, then += each contribution in reaction order, jac_rhs.F90:309-392).
   // Long entries (a few: among n, p, alpha) are listed and summed by a warp each from P.
   constexpr int kMaxLong = 128;
-  __shared__ int s_nlong;
-  __shared__ int s_longp[kMaxLong];
+  __shared__ int s_nlong_g[NUPPN_MAX_GROUPS];
+  __shared__ int s_longp_g[NUPPN_MAX_GROUPS][kMaxLong];
+  int &s_nlong = s_nlong_g[GID];
+  int *s_longp = s_longp_g[GID];
   if (tid == 0) s_nlong = 0;
-  __syncthreads();
+  GSYNC();
   for (int p = tid; p < A.nnz; p += nt) {
     const int e = N.lu_src[A.csrc[p]];
     if (e < 0) {
@@ -371,7 +373,7 @@ __device__ void dev_jacobian_active(const DevNet &N, const Ws &W, Act &A, int *s
     A.jval[p] = acc;
     A.jflag[p] = (uint8_t)((set ? JF_SET : 0) | (N.jdiag[N.jrow[e]] == e ? JF_DIAG : 0));
   }
-  __syncthreads();
+  GSYNC();
   const int nlong = s_nlong;
   const int nwork = nlong <= kMaxLong ? nlong : A.nnz;  // more than kMaxLong: scan every position
   for (int k = w; k < nwork; k += nw) {
@@ -403,13 +405,13 @@ __device__ void dev_jacobian_active(const DevNet &N, const Ws &W, Act &A, int *s
       A.jflag[p] = (uint8_t)((set ? JF_SET : 0) | (N.jdiag[N.jrow[e]] == e ? JF_DIAG : 0));
     }
   }
-  __syncthreads();
+  GSYNC();
 }
 
 // Jacobian values and flags of the compact positions from a full Jacobian in W.jac / W.eset (the
 // reduced-solve parity entry point supplies them instead of dev_jacobian_active).
 __device__ void dev_load_active_jacobian(const DevNet &N, const Ws &W, Act &A) {
-  for (int p = threadIdx.x; p < A.nnz; p += blockDim.x) {
+  for (int p = GT; p < A.nnz; p += GN) {
     const int e = N.lu_src[A.csrc[p]];
     if (e < 0) {
       A.jval[p] = 0.0;
@@ -419,7 +421,7 @@ __device__ void dev_load_active_jacobian(const DevNet &N, const Ws &W, Act &A) {
       A.jflag[p] = (uint8_t)((W.eset[e] ? JF_SET : 0) | (N.jdiag[N.jrow[e]] == e ? JF_DIAG : 0));
     }
   }
-  __syncthreads();
+  GSYNC();
 }
 
 // Entry p of I - hJ under reduce_jacobian's rules (jac_rhs.F90:97-140): an entry that was set but
@@ -455,13 +457,13 @@ __device__ __forceinline__ bool pivot_ok(float d) { return d != 0.0f && isfinite
 template <int R, typename F = double>
 __device__ bool tile_factor_block(F *T, F *rinv, int na) {
   constexpr int S = 32 * R;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int lane = GT & 31, w = GT >> 5, nw = GN >> 5;
   int bad = 0;
   for (int k = 0; k < na; ++k) {
     const F piv = T[k * (S + 1)];
     bad |= !pivot_ok(piv);
     const F rp = F(1) / piv;
-    if (threadIdx.x == 0) rinv[k] = rp;
+    if (GT == 0) rinv[k] = rp;
     F l[R];
     bool any = false;
 #pragma unroll
@@ -483,16 +485,16 @@ __device__ bool tile_factor_block(F *T, F *rinv, int na) {
           if (l[i] != F(0)) T[m * S + lane + 32 * i] -= l[i] * u;
       }
     }
-    __syncthreads();
+    GSYNC();
   }
-  for (int i = threadIdx.x; i < na * S; i += blockDim.x) {  // L columns: a_rk * (1 / a_kk)
+  for (int i = GT; i < na * S; i += GN) {  // L columns: a_rk * (1 / a_kk)
     const int c = i / S, r = i - c * S;
     if (r > c && r < na) {
       const F a = T[i];
       if (a != F(0)) T[i] = a * rinv[c];
     }
   }
-  return __syncthreads_or(bad) == 0;
+  return g_or(bad) == 0;
 }
 
 // Power of two that brings |m| into [1, 2) (1 for 0 or non-finite m).
@@ -508,7 +510,7 @@ __device__ __forceinline__ double pow2_scale(double m) {
 template <int R>
 __device__ bool tile_factor_mixed(Act &A, int na) {
   constexpr int S = 32 * R;
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
+  const int tid = GT, nt = GN, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
   const double *T = A.T;
   for (int c = w; c < na; c += nw) {  // column scales (columns are contiguous)
     double m = 0.0;
@@ -516,18 +518,18 @@ __device__ bool tile_factor_mixed(Act &A, int na) {
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(NUPPN_FULL, m, o));
     if (lane == 0) A.scol[c] = pow2_scale(m);
   }
-  __syncthreads();
+  GSYNC();
   for (int r = tid; r < na; r += nt) {  // row scales of the column-scaled matrix
     double m = 0.0;
     for (int c = 0; c < na; ++c) m = fmax(m, fabs(T[c * S + r]) * A.scol[c]);
     A.srow[r] = pow2_scale(m);
   }
-  __syncthreads();
+  GSYNC();
   for (int i = tid; i < na * S; i += nt) {
     const int c = i / S, r = i - c * S;
     A.T32[i] = r < na ? (float)(T[i] * A.scol[c] * A.srow[r]) : 0.0f;
   }
-  __syncthreads();
+  GSYNC();
   return tile_factor_block<R, float>(A.T32, A.rinv32, na);
 }
 
@@ -749,17 +751,17 @@ __device__ void tile_solve_xs(const Act &A, int lane) {
 // I - hJ on the active subsystem and its factorization in the static order, no pivoting.
 // Returns false on a zero or non-finite pivot, or if a dependency wait timed out.
 __device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h) {
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
+  const int tid = GT, nt = GN, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
   const int na = A.na;
   if (A.tile) {
     // dense tile, column-major: T[c*S + r] = entry (r, c); rows na..S-1 stay zero
     const int S = A.tile_rows;
     double *T = A.T;
     for (int i = tid; i < na * S; i += nt) T[i] = 0.0;
-    __syncthreads();
+    GSYNC();
     for (int c = w; c < na; c += nw)
       for (int p = A.crp[c] + lane; p < A.crp[c + 1]; p += 32) T[A.ccol[p] * S + c] = assemble_entry(A, p, h);
-    __syncthreads();
+    GSYNC();
     if (A.mixed) {
       A.mixed_now = S == 32 ? tile_factor_mixed<1>(A, na) : tile_factor_mixed<2>(A, na);
       if (A.mixed_now) return true;  // otherwise factor in FP64 (T is still unfactored)
@@ -767,7 +769,7 @@ __device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h
     return S == 32 ? tile_factor_block<1>(T, A.rinv, na) : tile_factor_block<2>(T, A.rinv, na);
   }
   for (int p = tid; p < A.nnz; p += nt) A.cval[p] = assemble_entry(A, p, h);
-  __syncthreads();
+  GSYNC();
   if (A.onewarp_f) {  // one warp, rows in order
     int bad = 0;
     if (w == 0) {
@@ -796,7 +798,7 @@ __device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h
         __syncwarp();
       }
     }
-    return __syncthreads_or(bad) == 0;
+    return g_or(bad) == 0;
   }
   const int gen = ++A.genF;
   bool ok = true;
@@ -827,19 +829,19 @@ __device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h
     __syncwarp();
     if (lane == 0) *(volatile int *)&A.flagF[c] = gen;
   }
-  __syncthreads();
-  return __syncthreads_and(ok) != 0;
+  GSYNC();
+  return g_and(ok) != 0;
 }
 
 // Solve the factored active subsystem in place on A.xs (compact right-hand side in, solution out).
 __device__ bool dev_solve_active(Act &A) {
-  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
+  const int tid = GT, lane = tid & 31, w = tid >> 5, nw = GN >> 5;
   if (A.tile) {
     if (w == 0) {
       if (A.tile_rows == 32) tile_solve_xs<1>(A, lane);
       else tile_solve_xs<2>(A, lane);
     }
-    __syncthreads();
+    GSYNC();
     return true;
   }
   if (A.onewarp) {  // one warp: forward then backward substitution, a row at a time
@@ -864,7 +866,7 @@ __device__ bool dev_solve_active(Act &A) {
         __syncwarp();
       }
     }
-    __syncthreads();
+    GSYNC();
     return true;
   }
   bool ok = true;
@@ -884,7 +886,7 @@ __device__ bool dev_solve_active(Act &A) {
     }
     __syncwarp();
   }
-  __syncthreads();
+  GSYNC();
   const int g2 = ++A.genS;
   for (int q = w; q < A.na; q += nw) {
     const int c = A.na - 1 - q;
@@ -902,18 +904,18 @@ __device__ bool dev_solve_active(Act &A) {
     }
     __syncwarp();
   }
-  __syncthreads();
-  return __syncthreads_and(ok) != 0;
+  GSYNC();
+  return g_and(ok) != 0;
 }
 
 // Species-indexed solve for the parity entry point: x = 0 off the active set.
 __device__ bool dev_solve_species(const DevNet &N, Act &A, const double *rhs, double *x) {
-  for (int c = threadIdx.x; c < A.na; c += blockDim.x) A.xs[c] = rhs[N.sp_of_sys[A.arow[c]]];
-  for (int s = threadIdx.x; s < N.nsp; s += blockDim.x) x[s] = 0.0;
-  __syncthreads();
+  for (int c = GT; c < A.na; c += GN) A.xs[c] = rhs[N.sp_of_sys[A.arow[c]]];
+  for (int s = GT; s < N.nsp; s += GN) x[s] = 0.0;
+  GSYNC();
   bool ok = dev_solve_active(A);
-  for (int c = threadIdx.x; c < A.na; c += blockDim.x) x[N.sp_of_sys[A.arow[c]]] = A.xs[c];
-  __syncthreads();
+  for (int c = GT; c < A.na; c += GN) x[N.sp_of_sys[A.arow[c]]] = A.xs[c];
+  GSYNC();
   return ok;
 }
 
@@ -941,7 +943,7 @@ __device__ __forceinline__ void put_rhs_item(const DevNet &N, const Ws &W, Act &
 }
 
 __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem, size_t smem_bytes, int *sint) {
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
+  const int tid = GT, nt = GN, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
   const int *sys2c = W.act_tmp;              // system index -> active row (dev_compact), -1 if frozen
   int *cnt = W.act_tmp + 2 * (N.nsys + 1);   // [na+1] items per row, then row offsets
   int *off = W.act_tmp + 3 * (N.nsys + 1);   // [na+1] offsets of the short rows' static lists
@@ -952,22 +954,22 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
     const int len = N.dg_ptr[s + 1] - N.dg_ptr[s];
     off[c] = len <= kLongList ? len : 0;
   }
-  __syncthreads();
+  GSYNC();
   const int T = block_scan_excl(off, na, sint);
   if (tid == 0) off[na] = T;
-  __syncthreads();
+  GSYNC();
   for (int t = tid; t < T; t += nt) {  // flattened static lists of the short rows
     const int c = seg_of(off, na, t);
     const int a = N.dg_item[N.dg_ptr[N.sp_of_sys[A.arow[c]]] + (t - off[c])] >> 2;
     const int *k = N.act_k + (size_t)a * 8;
     flag[t] = (W.mask[k[0]] && (k[2] == g || W.mask[k[2]])) ? 1 : 0;
   }
-  __syncthreads();
+  GSYNC();
   const int nS = block_scan_excl(flag, T, sint);
   if (tid == 0) flag[T] = nS;
-  __syncthreads();
+  GSYNC();
   for (int c = tid; c < na; c += nt) cnt[c] = flag[off[c + 1]] - flag[off[c]];  // 0 for long rows
-  __syncthreads();
+  GSYNC();
   for (int c = w; c < na; c += nw) {  // long rows: count their slots among the kept reactions
     const int s = N.sp_of_sys[A.arow[c]];
     if (N.dg_ptr[s + 1] - N.dg_ptr[s] <= kLongList) continue;
@@ -979,7 +981,7 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
     for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(NUPPN_FULL, n, o);
     if (lane == 0) cnt[c] = n;
   }
-  __syncthreads();
+  GSYNC();
   const int ngi = block_scan_excl(cnt, na, sint);
   const size_t lu_need = act_bytes(na, A.nnz, nw, A.tile_rows, A.mixed), need = rhs_bytes(na, ngi);
   char *base;
@@ -1023,7 +1025,7 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
       base_q += __shfl_sync(NUPPN_FULL, incl, 31);
     }
   }
-  __syncthreads();
+  GSYNC();
 }
 
 // Term q of the right-hand side from the compact molar abundances A.xnc: coefficient times the
@@ -1050,14 +1052,14 @@ __device__ __forceinline__ double gather_dxdt(const Act &A, int c) {
 
 // calculate_dxdt on the active rows: compact abundances yc in, compact dX/dt out.
 __device__ void dev_dxdt_active(const Act &A, const double *yc, double *dxc) {
-  const int tid = threadIdx.x, nt = blockDim.x;
+  const int tid = GT, nt = GN;
   for (int c = tid; c < A.na; c += nt) A.xnc[c] = yc[c] / A.anc[c];
-  __syncthreads();
+  GSYNC();
 #pragma unroll 4
   for (int q = tid; q < A.ngi; q += nt) A.gterm[q] = rhs_term(A, q);
-  __syncthreads();
+  GSYNC();
   for (int c = tid; c < A.na; c += nt) dxc[c] = gather_dxdt(A, c);
-  __syncthreads();
+  GSYNC();
 }
 
-}  // namespace nuppn
+NUPPN_END

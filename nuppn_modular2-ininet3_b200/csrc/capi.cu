@@ -23,14 +23,24 @@
 #include "nuppn_internal.h"
 
 namespace nuppn {
+namespace cta {  // solver.cu with one zone per CTA
 cudaError_t launch_integrate(const DevNet &N, const WsLayout &L, char *ws, int grid, int block, int act_smem,
                              const IntegrateArgs &A, cudaStream_t st);
 cudaError_t launch_phase(const DevNet &N, const WsLayout &L, char *ws, int grid, int block, int act_smem,
                          const PhaseArgs &A, cudaStream_t st);
-cudaError_t configure_kernels(int act_smem);
+cudaError_t configure_kernels(int dyn_smem);
 cudaError_t launch_zone_order(const double *key, const double *key_b, int stride, int nz, int *order,
                               cudaStream_t st);
 cudaError_t occupancy_integrate(int block, int act_smem, int *per_sm);
+}  // namespace cta
+namespace warp {  // solver.cu with one zone per warp
+cudaError_t launch_integrate(const DevNet &N, const WsLayout &L, char *ws, int grid, int block, int act_smem,
+                             const IntegrateArgs &A, cudaStream_t st);
+cudaError_t configure_kernels(int dyn_smem);
+cudaError_t occupancy_integrate(int block, int act_smem, int *per_sm);
+}  // namespace warp
+using cta::launch_phase;
+using cta::launch_zone_order;
 }  // namespace nuppn
 
 using namespace nuppn;
@@ -74,8 +84,13 @@ struct nuppn_net {
   WsLayout L;
   DevBuf ws, stage, counter, order;  // order: the zone schedule of the allocating entry points
   int ws_slots = 0;
+  // integration kernel: one zone per CTA of `block` threads (warp_zones = 0), or one zone per warp
+  // with `block` / 32 zones per CTA (warp_zones = 1); act_smem = shared memory of each zone's group
+  int warp_zones = 0;
   int block = 256;
-  int act_smem = 72 * 1024;  // shared-memory budget per CTA for the active subsystem (3 CTAs per SM)
+  int act_smem = 72 * 1024;  // CTA per zone: shared-memory budget per CTA for the active subsystem (3 CTAs per SM)
+  int phase_block = 256;     // the parity entry points always run one zone per CTA of 256 threads
+  int phase_smem = 72 * 1024;
   int device = 0;
   int nsm = 0;
   int64_t launches = 0;
@@ -225,10 +240,84 @@ nuppn_status ensure_ws(nuppn_net *net, int slots) {
   return NUPPN_OK;
 }
 
-int resident_slots(nuppn_net *net) {
+int zones_per_cta(const nuppn_net *net) { return net->warp_zones ? net->block / 32 : 1; }
+
+// CTAs of the integration kernel resident on the whole GPU
+int resident_ctas(const nuppn_net *net) {
   int per = 0;
-  if (occupancy_integrate(net->block, net->act_smem, &per) != cudaSuccess || per <= 0) per = 1;
+  cudaError_t e = net->warp_zones ? warp::occupancy_integrate(net->block, net->act_smem, &per)
+                                  : cta::occupancy_integrate(net->block, net->act_smem, &per);
+  if (e != cudaSuccess || per <= 0) per = 1;
   return per * net->nsm;
+}
+
+// zones in flight at once (one workspace slab each)
+int resident_slots(const nuppn_net *net) { return resident_ctas(net) * zones_per_cta(net); }
+
+// CTAs of the parity kernel (one zone per CTA of phase_block threads)
+int phase_slots(const nuppn_net *net) {
+  int per = 0;
+  if (cta::occupancy_integrate(net->phase_block, net->phase_smem, &per) != cudaSuccess || per <= 0) per = 1;
+  return per * net->nsm;
+}
+
+// CTAs for nz zones: whole CTAs' worth of zones, at most the resident CTAs and `slabs` workspace slabs
+int integrate_grid(const nuppn_net *net, int nz, int slabs) {
+  const int zpc = zones_per_cta(net);
+  int grid = std::min((nz + zpc - 1) / zpc, resident_ctas(net));
+  return std::max(1, std::min(grid, slabs / zpc));
+}
+
+cudaError_t launch_integrate_net(const nuppn_net *net, char *ws, int grid, const IntegrateArgs &A, cudaStream_t s) {
+  return net->warp_zones ? warp::launch_integrate(net->D, net->L, ws, grid, net->block, net->act_smem, A, s)
+                         : cta::launch_integrate(net->D, net->L, ws, grid, net->block, net->act_smem, A, s);
+}
+
+// Largest dynamic shared memory of one CTA of the warp-per-zone kernel: the 227 KB opt-in limit
+// per CTA less the kernel's ~7 KB of static arrays (per-warp reduction and scan scratch, long-entry
+// lists) and a margin.
+constexpr int kWarpCtaSmem = 216 * 1024;
+
+nuppn_status check_shape(const nuppn_knobs &kn) {
+  const int t = kn.threads_per_zone;
+  if (t < 0 || t % 32 || t > 256) {
+    set_error("threads_per_zone must be 0 or a multiple of 32 up to 256");
+    return NUPPN_ERR_ARG;
+  }
+  if (kn.zones_per_cta < 0 || kn.zones_per_cta > 8) {
+    set_error("zones_per_cta must be 0..8");
+    return NUPPN_ERR_ARG;
+  }
+  if (kn.zone_smem < 0 || kn.zone_smem > kWarpCtaSmem) {
+    set_error("zone_smem must be 0..216 KB");
+    return NUPPN_ERR_ARG;
+  }
+  return NUPPN_OK;
+}
+
+// Kernel shape from the knobs: one zone per warp (threads_per_zone = 32) or one per CTA, the CTA
+// size and each zone's shared memory; sets the kernels' dynamic shared-memory limits to match.
+nuppn_status apply_shape(nuppn_net *net, const nuppn_knobs &kn) {
+  net->warp_zones = kn.threads_per_zone == 32 ? 1 : 0;
+  if (net->warp_zones) {
+    const int zpc = kn.zones_per_cta > 0 ? kn.zones_per_cta : 8;
+    net->block = 32 * zpc;
+    const int share = (kWarpCtaSmem / zpc) & ~15;
+    net->act_smem = kn.zone_smem > 0 ? std::min(kn.zone_smem & ~15, share) : share;
+    net->phase_block = 256;
+  } else {
+    net->block = kn.threads_per_zone > 0 ? kn.threads_per_zone : 256;
+    net->act_smem = kn.zone_smem > 0 ? (kn.zone_smem & ~15) : 72 * 1024;
+    net->phase_block = net->block;
+  }
+  net->phase_smem = net->warp_zones ? 72 * 1024 : net->act_smem;
+  cudaError_t e = cta::configure_kernels(std::max(net->phase_smem, net->warp_zones ? 0 : net->act_smem));
+  if (e == cudaSuccess && net->warp_zones) e = warp::configure_kernels(net->act_smem * zones_per_cta(net));
+  if (e != cudaSuccess) {
+    set_error(std::string("cannot configure dynamic shared memory: ") + cudaGetErrorString(e));
+    return NUPPN_ERR_CUDA;
+  }
+  return NUPPN_OK;
 }
 
 nuppn_status check_zone_args(nuppn_net *net, int nz, int ldx) {
@@ -339,20 +428,17 @@ nuppn_status nuppn_net_create(const nuppn_net_desc *desc, const nuppn_knobs *kno
   }
   net->device = device;
   net->nsm = prop.multiProcessorCount;
-  net->block = kn.threads_per_zone > 0 ? kn.threads_per_zone : 256;
-  if (net->block % 32 || net->block > 256) { delete net; set_error("threads_per_zone must be a multiple of 32, <= 256"); return NUPPN_ERR_ARG; }
   if (kn.lu_precision != 0 && kn.lu_precision != 1) {
     delete net;
     set_error("lu_precision must be 0 (FP64) or 1 (FP32 factor + FP64 refinement)");
     return NUPPN_ERR_ARG;
   }
-  nuppn_status st = upload(net);
+  nuppn_status st = check_shape(kn);
   if (st != NUPPN_OK) { delete net; return st; }
-  if (configure_kernels(net->act_smem) != cudaSuccess) {
-    set_error("cannot configure dynamic shared memory");
-    nuppn_net_destroy(net);
-    return NUPPN_ERR_CUDA;
-  }
+  st = upload(net);
+  if (st != NUPPN_OK) { delete net; return st; }
+  st = apply_shape(net, kn);
+  if (st != NUPPN_OK) { nuppn_net_destroy(net); return st; }
   net->L = layout(net->H);
   if (net->counter.ensure(256) != cudaSuccess) { delete net; set_error("counter alloc"); return NUPPN_ERR_NOMEM; }
   *out = net;
@@ -392,10 +478,10 @@ nuppn_status nuppn_set_knobs(nuppn_net *net, const nuppn_knobs *knobs) {
     set_error("i_nse = 1 needs protons and Ni56 among the considered species");
     return NUPPN_ERR_NET;
   }
-  if (knobs->threads_per_zone != net->H.kn.threads_per_zone) {  // fixes the CTA size and workspace
-    set_error("threads_per_zone takes effect only at nuppn_net_create");
-    return NUPPN_ERR_ARG;
-  }
+  nuppn_status sh = check_shape(*knobs);
+  if (sh != NUPPN_OK) return sh;
+  sh = apply_shape(net, *knobs);  // the workspace grows on the next call if the shape needs more slabs
+  if (sh != NUPPN_OK) return sh;
   double old_dgrd = net->H.kn.dgrd;
   net->H.kn = *knobs;
   if (knobs->dgrd != old_dgrd) bd_constants(net->H);
@@ -441,14 +527,20 @@ nuppn_status nuppn_integrate_device_noalloc(nuppn_net *net, int32_t nz, double *
   void *base = nullptr;
   CK(noalloc_scratch(net->device, &base));
   const int slabs = (int)(((size_t)NUPPN_NOALLOC_SCRATCH_BYTES - kNoAllocCounterBytes) / slab);
-  const int grid = std::min(std::min(nz, resident_slots(net)), slabs);
+  if (slabs < zones_per_cta(net)) {
+    set_error("nuppn_integrate_device_noalloc: the static scratch holds " + std::to_string(slabs) +
+              " workspace slabs of this network, fewer than the zones of one CTA (" +
+              std::to_string(zones_per_cta(net)) + "); use fewer zones_per_cta or nuppn_integrate_device");
+    return NUPPN_ERR_LIMIT;
+  }
+  const int grid = integrate_grid(net, nz, slabs);
   cudaStream_t s = (cudaStream_t)stream;
   CK(cudaMemsetAsync(base, 0, sizeof(int), s));  // the zone counter starts at zero every call
   IntegrateArgs A = {};
   A.nz = nz; A.ldx = ldx; A.X = d_X; A.t9_0 = d_t9_0; A.t9_1 = d_t9_1; A.rho_0 = d_rho_0; A.rho_1 = d_rho_1;
   A.dtwant = d_dtwant; A.ye = d_ye; A.ierr = d_ierr; A.stats = d_stats; A.bd_state = d_bd_state;
   A.counter = (int *)base;
-  CK(launch_integrate(net->D, net->L, (char *)base + kNoAllocCounterBytes, grid, net->block, net->act_smem, A, s));
+  CK(launch_integrate_net(net, (char *)base + kNoAllocCounterBytes, grid, A, s));
   net->launches++;
   return NUPPN_OK;
 }
@@ -480,7 +572,7 @@ static nuppn_status run_phase(nuppn_net *net, int nz, int op, const double *X, i
   CK(up(oX, X, (size_t)nz * ldx * 8)); CK(up(ot9, t9, nz * 8)); CK(up(orho, rho, nz * 8)); CK(up(oye, ye, nz * 8));
   CK(up(ov, v, (size_t)nz * H.nre * 8)); CK(up(odt, dt, nz * 8)); CK(up(ojac, jac, (size_t)nz * H.nnzJ * 8));
   CK(up(oes, eset, (size_t)nz * H.nnzJ)); CK(up(omk, mask, (size_t)nz * H.nsp)); CK(up(ob, b, (size_t)nz * H.nsp * 8));
-  int grid = std::min(nz, resident_slots(net));
+  int grid = std::min(nz, phase_slots(net));
   st = ensure_ws(net, grid);
   if (st != NUPPN_OK) return st;
   PhaseArgs A;
@@ -494,7 +586,7 @@ static nuppn_status run_phase(nuppn_net *net, int nz, int op, const double *X, i
   A.out_v = out_v ? (double *)(sb + oov) : nullptr; A.out_dxdt = out_dxdt ? (double *)(sb + ood) : nullptr;
   A.out_jac = out_jac ? (double *)(sb + ooj) : nullptr; A.out_eset = out_eset ? (uint8_t *)(sb + ooe) : nullptr;
   A.out_mask = out_mask ? (uint8_t *)(sb + oom) : nullptr; A.out_x = out_x ? (double *)(sb + oox) : nullptr;
-  CK(launch_phase(net->D, net->L, (char *)net->ws.p, grid, net->block, net->act_smem, A, 0));
+  CK(launch_phase(net->D, net->L, (char *)net->ws.p, grid, net->phase_block, net->phase_smem, A, 0));
   net->launches++;
   CK(cudaDeviceSynchronize());
   auto down = [&](void *dst, size_t off, size_t bytes) -> cudaError_t {
@@ -526,7 +618,7 @@ nuppn_status nuppn_nse(nuppn_net *net, int32_t nz, const double *t9, const doubl
   CK(cudaMemcpy(sb + o1, t9, nz * 8, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(sb + o2, rho, nz * 8, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(sb + o3, ye, nz * 8, cudaMemcpyHostToDevice));
-  int grid = std::min(nz, resident_slots(net));
+  int grid = std::min(nz, phase_slots(net));
   nuppn_status st = ensure_ws(net, grid);
   if (st != NUPPN_OK) return st;
   PhaseArgs A;
@@ -535,7 +627,7 @@ nuppn_status nuppn_nse(nuppn_net *net, int32_t nz, const double *t9, const doubl
   A.t9 = (const double *)(sb + o1); A.rho = (const double *)(sb + o2); A.ye = (const double *)(sb + o3);
   A.out_x = (double *)(sb + oX); A.out_mu_p = (double *)(sb + op); A.out_mu_n = (double *)(sb + on);
   A.out_iters = (int *)(sb + oi); A.out_ierr = (int *)(sb + oe);
-  CK(launch_phase(net->D, net->L, (char *)net->ws.p, grid, net->block, net->act_smem, A, 0));
+  CK(launch_phase(net->D, net->L, (char *)net->ws.p, grid, net->phase_block, net->phase_smem, A, 0));
   net->launches++;
   CK(cudaDeviceSynchronize());
   CK(cudaMemcpy(X, sb + oX, (size_t)nz * nsp * 8, cudaMemcpyDeviceToHost));
@@ -586,8 +678,8 @@ nuppn_status nuppn_integrate_device(nuppn_net *net, int32_t nz, double *d_X, int
     return NUPPN_ERR_ARG;
   }
   CK(cudaSetDevice(net->device));
-  int grid = std::min(nz, resident_slots(net));
-  st = ensure_ws(net, grid);
+  const int grid = integrate_grid(net, nz, resident_slots(net));
+  st = ensure_ws(net, grid * zones_per_cta(net));
   if (st != NUPPN_OK) return st;
   cudaStream_t s = (cudaStream_t)stream;
   CK(net->order.ensure((size_t)nz * 4));
@@ -598,7 +690,7 @@ nuppn_status nuppn_integrate_device(nuppn_net *net, int32_t nz, double *d_X, int
   A.dtwant = d_dtwant; A.ye = d_ye; A.ierr = d_ierr; A.stats = d_stats; A.bd_state = d_bd_state;
   A.counter = (int *)net->counter.p;
   A.order = (const int *)net->order.p;
-  CK(launch_integrate(net->D, net->L, (char *)net->ws.p, grid, net->block, net->act_smem, A, s));
+  CK(launch_integrate_net(net, (char *)net->ws.p, grid, A, s));
   net->launches += 2;  // k_zone_order, k_integrate
   return NUPPN_OK;
 }
@@ -642,6 +734,122 @@ nuppn_status nuppn_integrate(nuppn_net *net, int32_t nz, double *X, int32_t ldx,
   return NUPPN_OK;
 }
 
+// ---- autotuning of the kernel shape -------------------------------------------------------------
+nuppn_status nuppn_autotune(nuppn_net *net, int32_t nz, const double *X, int32_t ldx, const double *t9_0,
+                            const double *t9_1, const double *rho_0, const double *rho_1, const double *ye,
+                            const double *dtwant, int32_t sample, nuppn_tune_result *report, int32_t ncand,
+                            int32_t *nreport) {
+  nuppn_status st = check_zone_args(net, nz, ldx);
+  if (st != NUPPN_OK) return st;
+  if (!X || !t9_0 || !t9_1 || !rho_0 || !rho_1 || !ye || !dtwant || sample < 0 || (report && ncand < 0)) {
+    set_error("null or negative argument");
+    return NUPPN_ERR_ARG;
+  }
+  if (nreport) *nreport = 0;
+  const int n = sample > 0 ? std::min(sample, nz) : nz;
+  if (n == 0) return NUPPN_OK;
+  CK(cudaSetDevice(net->device));
+  // inputs (kept) and one call's working copies
+  Stager S;
+  const size_t xb = (size_t)n * ldx * 8, vb = (size_t)n * 8;
+  size_t oX0 = S.add(xb), oX = S.add(xb), o1 = S.add(vb), o2 = S.add(vb), o3 = S.add(vb), o4 = S.add(vb);
+  size_t oy0 = S.add(vb), oy = S.add(vb), odt = S.add(vb), oi = S.add((size_t)n * 4), ob = S.add((size_t)n * 4);
+  size_t os = S.add((size_t)n * sizeof(nuppn_zone_stats));
+  DevBuf buf;
+  struct Release {
+    DevBuf &b;
+    ~Release() { b.release(); }
+  } release_buf{buf};
+  CK(buf.ensure(S.total));
+  char *b = (char *)buf.p;
+  CK(cudaMemcpy(b + oX0, X, xb, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b + o1, t9_0, vb, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b + o2, t9_1, vb, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b + o3, rho_0, vb, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b + o4, rho_1, vb, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b + oy0, ye, vb, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b + odt, dtwant, vb, cudaMemcpyHostToDevice));
+  // candidates: one zone per CTA of 256 threads (3 per SM); one zone per warp with 8 zones per CTA,
+  // 4 per CTA at the same share of shared memory (two CTAs per SM), and 4 per CTA with twice the
+  // share (64-row tiles of the hottest zones fit in shared memory, one CTA per SM)
+  struct Cand { int tpz, zpc, smem; };
+  const Cand cands[] = {{0, 0, 0}, {32, 8, 0}, {32, 4, 27648}, {32, 4, 0}};
+  const int nc = (int)(sizeof(cands) / sizeof(cands[0]));
+  const nuppn_knobs base = net->H.kn;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  std::vector<nuppn_zone_stats> stv(n);
+  std::vector<double> rate(nc, -1.0), ms(nc, 0.0);
+  std::vector<int> zsm(nc, 0);
+  nuppn_status out = NUPPN_OK;
+  for (int c = 0; c < nc && out == NUPPN_OK; ++c) {
+    nuppn_knobs kn = base;
+    kn.threads_per_zone = cands[c].tpz;
+    kn.zones_per_cta = cands[c].zpc;
+    kn.zone_smem = cands[c].smem;
+    if (apply_shape(net, kn) != NUPPN_OK) continue;  // a shape this device cannot run is skipped
+    zsm[c] = resident_slots(net) / std::max(net->nsm, 1);
+    for (int rep = 0; rep < 2 && out == NUPPN_OK; ++rep) {  // the first call grows the workspace
+      cudaError_t e = cudaMemcpyAsync(b + oX, b + oX0, xb, cudaMemcpyDeviceToDevice, 0);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(b + oy, b + oy0, vb, cudaMemcpyDeviceToDevice, 0);
+      if (e == cudaSuccess) e = cudaMemsetAsync(b + ob, 0, (size_t)n * 4, 0);
+      if (e == cudaSuccess) e = cudaEventRecord(e0, 0);
+      if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); out = NUPPN_ERR_CUDA; break; }
+      out = nuppn_integrate_device(net, n, (double *)(b + oX), ldx, (double *)(b + o1), (double *)(b + o2),
+                                   (double *)(b + o3), (double *)(b + o4), (double *)(b + oy), (double *)(b + odt),
+                                   (int *)(b + oi), (nuppn_zone_stats *)(b + os), (int *)(b + ob), nullptr);
+      if (out != NUPPN_OK) break;
+      e = cudaEventRecord(e1, 0);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float t = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+      if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); out = NUPPN_ERR_CUDA; break; }
+      ms[c] = t;
+    }
+    if (out != NUPPN_OK) break;
+    if (cudaMemcpy(stv.data(), b + os, (size_t)n * sizeof(nuppn_zone_stats), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      set_error("autotune: stats copy");
+      out = NUPPN_ERR_CUDA;
+      break;
+    }
+    int64_t steps = 0;
+    for (const nuppn_zone_stats &z : stv) steps += z.nsucc;
+    rate[c] = ms[c] > 0.0 ? (double)steps / (ms[c] * 1e-3) : 0.0;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  int best = -1;
+  for (int c = 0; c < nc; ++c)
+    if (rate[c] > 0.0 && (best < 0 || rate[c] > rate[best])) best = c;
+  nuppn_knobs kn = base;
+  if (out == NUPPN_OK && best >= 0) {
+    kn.threads_per_zone = cands[best].tpz;
+    kn.zones_per_cta = cands[best].zpc;
+    kn.zone_smem = cands[best].smem;
+  }
+  const nuppn_status st2 = apply_shape(net, kn);  // the winner, or the shape the handle had
+  net->H.kn = kn;
+  net->D.kn = kn;
+  if (out == NUPPN_OK && st2 != NUPPN_OK) out = st2;
+  if (report) {
+    int k = 0;
+    for (int c = 0; c < nc && k < ncand; ++c, ++k) {
+      nuppn_tune_result &r = report[k];
+      memset(&r, 0, sizeof(r));
+      r.threads_per_zone = cands[c].tpz;
+      r.zones_per_cta = cands[c].zpc;
+      r.zone_smem = cands[c].smem;
+      r.zones_per_sm = zsm[c];
+      r.ms = ms[c];
+      r.zone_steps_per_s = rate[c];
+      r.chosen = c == best;
+    }
+    if (nreport) *nreport = k;
+  }
+  return out;
+}
+
 nuppn_status nuppn_integrate_trajectories_device(nuppn_net *net, int32_t nz, int32_t npts, double *d_X, int32_t ldx,
                                                 const double *d_time, const double *d_t9, const double *d_rho,
                                                 double *d_ye, int32_t *d_ierr, int32_t *d_fail,
@@ -655,8 +863,8 @@ nuppn_status nuppn_integrate_trajectories_device(nuppn_net *net, int32_t nz, int
     return NUPPN_ERR_ARG;
   }
   CK(cudaSetDevice(net->device));
-  int grid = std::min(nz, resident_slots(net));
-  st = ensure_ws(net, grid);
+  const int grid = integrate_grid(net, nz, resident_slots(net));
+  st = ensure_ws(net, grid * zones_per_cta(net));
   if (st != NUPPN_OK) return st;
   cudaStream_t s = (cudaStream_t)stream;
   CK(net->order.ensure((size_t)nz * 4));
@@ -667,7 +875,7 @@ nuppn_status nuppn_integrate_trajectories_device(nuppn_net *net, int32_t nz, int
   A.counter = (int *)net->counter.p;
   A.order = (const int *)net->order.p;
   A.npts = npts; A.tr_time = d_time; A.tr_t9 = d_t9; A.tr_rho = d_rho; A.tr_fail = d_fail;
-  CK(launch_integrate(net->D, net->L, (char *)net->ws.p, grid, net->block, net->act_smem, A, s));
+  CK(launch_integrate_net(net, (char *)net->ws.p, grid, A, s));
   net->launches += 2;  // k_zone_order, k_integrate
   return NUPPN_OK;
 }
@@ -876,7 +1084,7 @@ std::string lane_launch(nuppn_server *S, ServeLane &L, std::vector<ServeReq *> &
     SK(launch_zone_order(A.tr_t9, nullptr, npts, n, (int *)(d + L.oord), s));
   }
   SK(cudaMemsetAsync(d + L.ocnt, 0, sizeof(int), s));
-  SK(launch_integrate(net->D, net->L, (char *)L.ws.p, std::min(n, S->slots), net->block, net->act_smem, A, s));
+  SK(launch_integrate_net(net, (char *)L.ws.p, integrate_grid(net, n, S->slots), A, s));
   S->launches += 2;
   S->batches += 1;
   SK(d2h(L.oX, (size_t)n * nsp * 8));

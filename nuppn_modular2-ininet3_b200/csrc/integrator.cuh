@@ -11,7 +11,7 @@
 // zero, and their share of the mass sum and of the negative-abundance test is a per-step constant.
 #pragma once
 
-namespace nuppn {
+NUPPN_BEGIN
 
 struct ZoneCtl {
   nuppn_zone_stats st;
@@ -28,36 +28,36 @@ struct ZoneCtl {
 };
 
 __device__ void vcopy(double *dst, const double *src, int n) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
-  __syncthreads();
+  for (int i = GT; i < n; i += GN) dst[i] = src[i];
+  GSYNC();
 }
 
 __device__ double vsum(const double *a, int n, double *sred) {
   double s = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s += a[i];
+  for (int i = GT; i < n; i += GN) s += a[i];
   return block_sum(s, sred);
 }
 
 __device__ double vmaxneg(const double *a, int n, double *sred) {
   double m = -DBL_MAX;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, -a[i]);
+  for (int i = GT; i < n; i += GN) m = fmax(m, -a[i]);
   return block_max(m, sred);
 }
 
 // ypsplus (utils.F90:726-740)
 __device__ void ypsplus(double *y, int n) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = GT; i < n; i += GN) {
     double v = y[i];
     if (v < -1.e-27) v = 1.e-99;
     if (v < 1.e-27) v = 1.e-99;
     y[i] = v;
   }
-  __syncthreads();
+  GSYNC();
 }
 
 // renorm_1d (utils.F90:436-446): y / ksum(y), the Kahan sum (utils.F90:670-685) taken in order
 __device__ void dev_renorm_ksum(double *y, int n, double *sred) {
-  if (threadIdx.x == 0) {
+  if (GT == 0) {
     double c = 0.0, s = 0.0;
     for (int i = 0; i < n; ++i) {
       const double yy = y[i] - c;
@@ -67,17 +67,17 @@ __device__ void dev_renorm_ksum(double *y, int n, double *sred) {
     }
     sred[0] = s;
   }
-  __syncthreads();
+  GSYNC();
   const double s = sred[0];
-  __syncthreads();
-  for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = y[i] / s;
-  __syncthreads();
+  GSYNC();
+  for (int i = GT; i < n; i += GN) y[i] = y[i] / s;
+  GSYNC();
 }
 
 // calculate_ye (utils.F90:537-553)
 __device__ double dev_ye(const DevNet &N, const double *x, double *sred) {
   double s = 0.0;
-  for (int i = threadIdx.x; i < N.nsp; i += blockDim.x)
+  for (int i = GT; i < N.nsp; i += GN)
     if (N.ciso[i]) s += (N.an[i] - 2.0 * N.zn[i]) * x[i] / N.an[i];
   s = block_sum(s, sred);
   return (1.0 - s) * 0.5;
@@ -97,12 +97,12 @@ __device__ void dev_new_jacobian(const DevNet &N, const Ws &W, ZoneCtl &C, doubl
 // ---------------------------------------------------------------------------------------------
 __device__ int dev_backward_euler(const DevNet &N, const Ws &W, ZoneCtl &C, double *yps, double dt, double &dtrcmd,
                                   double *sred) {
-  const int nsp = N.nsp, tid = threadIdx.x, nt = blockDim.x;
+  const int nsp = N.nsp, tid = GT, nt = GN;
   const double rmin = 0.2, rmax = 2.0, dgrd = N.kn.dgrd;
   const double sum_check = N.kn.grdthreshold * N.nvar * dgrd;
   double *yc = W.bd, *dxc = W.bd + N.nsys;
   for (int i = tid; i < nsp; i += nt) { W.y_new[i] = yps[i]; W.y_old[i] = yps[i]; W.y_cur[i] = yps[i]; }
-  __syncthreads();
+  GSYNC();
   int iter = 0;
   double grd = 0.0;
   for (;;) {
@@ -121,13 +121,13 @@ __device__ int dev_backward_euler(const DevNet &N, const Ws &W, ZoneCtl &C, doub
     Act &A = C.act;
     bool ok = dev_factor_active(N, W, A, dt);
     for (int c = tid; c < A.na; c += nt) yc[c] = W.y_cur[N.sp_of_sys[A.arow[c]]];
-    __syncthreads();
+    GSYNC();
     dev_dxdt_active(A, yc, dxc);
     for (int c = tid; c < A.na; c += nt) {
       const int s = N.sp_of_sys[A.arow[c]];
       A.xs[c] = W.y_old[s] - W.y_cur[s] + dt * dxc[c];
     }
-    __syncthreads();
+    GSYNC();
     ok = dev_solve_active(A) && ok;
     if (!ok) return BAD_STEP;
     C.st.nfact++; C.st.nsolve++;
@@ -170,12 +170,12 @@ __device__ __forceinline__ BdVec bd_bind(const Ws &W, int nsys) {
 // one semi-implicit midpoint sub-step, bader_deuflhard_step (bader_deuflhard.F90:410-488)
 __device__ int dev_bd_substep(const DevNet &N, const Ws &W, ZoneCtl &C, const BdVec &B, double h, int stage,
                               bool huge_frozen) {
-  const int tid = threadIdx.x, nt = blockDim.x;
+  const int tid = GT, nt = GN;
   Act &A = C.act;
   dev_dxdt_active(A, B.yk, B.dxc);
   if (stage == 1) for (int c = tid; c < A.na; c += nt) A.xs[c] = h * B.dxc[c];
   else for (int c = tid; c < A.na; c += nt) A.xs[c] = h * B.dxc[c] - B.dk[c];
-  __syncthreads();
+  GSYNC();
   if (!dev_solve_active(A)) return BAD_STEP;
   C.st.nsolve++;
   bool huge = false;
@@ -197,7 +197,7 @@ __device__ int dev_bd_substep(const DevNet &N, const Ws &W, ZoneCtl &C, const Bd
 template <int R>
 __device__ int bd_level_tile(const Act &A, const BdVec &B, double h, int nseq, bool huge_frozen, int &nsolve,
                              int &ir_sweeps, int *sflag) {
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, na = A.na;
+  const int tid = GT, nt = GN, lane = tid & 31, w = tid >> 5, na = A.na;
   double y[R], d[R], ri[R], an[R];
   int sweeps = 0;  // refinement sweeps (mixed precision), counted by warp 0
   if (w == 0) {
@@ -218,11 +218,11 @@ __device__ int bd_level_tile(const Act &A, const BdVec &B, double h, int nseq, b
     }
   }
   for (int j = 0;; ++j) {
-    __syncthreads();  // xnc of sub-step j and the stop flag are written
+    GSYNC();  // xnc of sub-step j and the stop flag are written
     if (sflag[0] != 0 || j > nseq) break;
 #pragma unroll 4
     for (int q = tid; q < A.ngi; q += nt) A.gterm[q] = rhs_term(A, q);
-    __syncthreads();
+    GSYNC();
     if (w == 0) {
       const int stage = j == 0 ? 1 : (j < nseq ? 2 : 3);  // FIRST, MID, LAST
       double x[R];
@@ -262,11 +262,11 @@ __device__ int bd_level_tile(const Act &A, const BdVec &B, double h, int nseq, b
       }
     if (lane == 0) sflag[2] = sweeps;
   }
-  __syncthreads();
+  GSYNC();
   const int err = sflag[0];
   nsolve += sflag[1];
   ir_sweeps += sflag[2];
-  __syncthreads();
+  GSYNC();
   return err;
 }
 
@@ -279,7 +279,7 @@ __device__ int dev_bd_level_tile(const Act &A, const BdVec &B, double h, int nse
 // extrapolate (bader_deuflhard.F90:371-407): Neville tableau, column k, on the active rows
 __device__ void dev_extrapolate(ZoneCtl &C, const BdVec &B, int na, int k, double xest) {
   C.xhist[k] = xest;
-  for (int j = threadIdx.x; j < na; j += blockDim.x) {
+  for (int j = GT; j < na; j += GN) {
     const double yest = B.yk[j];
     if (k == 1) {
       B.Q[(size_t)k * na + j] = yest;
@@ -302,12 +302,12 @@ __device__ void dev_extrapolate(ZoneCtl &C, const BdVec &B, int na, int k, doubl
     B.Q[(size_t)k * na + j] = e;
     B.yext[j] = yz;
   }
-  __syncthreads();
+  GSYNC();
 }
 
 __device__ int dev_bader_deuflhard(const DevNet &N, const Ws &W, ZoneCtl &C, double *yps, double dt, double &dtrcmd,
                                    bool frst, double *sred) {
-  const int tid = threadIdx.x, nt = blockDim.x;
+  const int tid = GT, nt = GN;
   const double safe1 = 0.25, safe2 = 0.7, redmin = 0.7, redmax = 1.e-5, scalmx = 0.25;
   const double thr = N.kn.grdthreshold;
   int km = -1, k;
@@ -333,7 +333,7 @@ __device__ int dev_bader_deuflhard(const DevNet &N, const Ws &W, ZoneCtl &C, dou
   huge_fz = block_any(huge_fz);
   for (k = 1; k <= N.kmax; ++k) {
     for (int c = tid; c < na; c += nt) B.yk[c] = yps[N.sp_of_sys[A.arow[c]]];
-    __syncthreads();
+    GSYNC();
     // semi_implicit_extrapolation (bader_deuflhard.F90:276-316)
     const double h = dt / (double)N.nseq[k];
     const double xest = powi(h / N.nseq[k], 2);
@@ -430,7 +430,7 @@ __device__ int dev_bader_deuflhard(const DevNet &N, const Ws &W, ZoneCtl &C, dou
     }
   }
   for (int c = tid; c < na; c += nt) yps[N.sp_of_sys[A.arow[c]]] = B.yk[c];  // yps(:) = y_k(:)
-  __syncthreads();
+  GSYNC();
   return ierr;
 }
 
@@ -498,12 +498,12 @@ __device__ int dev_integrate_zone(const DevNet &N, const Ws &W, ZoneCtl &C, doub
     }
     if (ierr == 0) {
       dtdone = dtdone + dttry;
-      for (int s = threadIdx.x; s < nsp; s += blockDim.x) {
+      for (int s = GT; s < nsp; s += GN) {
         double y = fmax(yps[s], 1.e-99);
         yps[s] = y;
         W.y_old[s] = y;
       }
-      __syncthreads();
+      GSYNC();
       ye_old = ye;
       C.st.nsucc++;
       if (dtdone >= dtwant) break;
@@ -517,12 +517,12 @@ __device__ int dev_integrate_zone(const DevNet &N, const Ws &W, ZoneCtl &C, doub
   }
   if (kn.integration_method == 1) {
     double s = vsum(yps, nsp, sred);
-    for (int q = threadIdx.x; q < nsp; q += blockDim.x) yps[q] = yps[q] / s;
-    __syncthreads();
+    for (int q = GT; q < nsp; q += GN) yps[q] = yps[q] / s;
+    GSYNC();
   }
-  for (int q = threadIdx.x; q < nsp; q += blockDim.x) yps[q] = fmax(yps[q], 1.e-99);
-  __syncthreads();
+  for (int q = GT; q < nsp; q += GN) yps[q] = fmax(yps[q], 1.e-99);
+  GSYNC();
   return 0;
 }
 
-}  // namespace nuppn
+NUPPN_END

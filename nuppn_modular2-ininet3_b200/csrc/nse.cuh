@@ -8,7 +8,7 @@
 // the reference's sorted, position-masked sum (dev_nse_yedot), whose mask changes which terms count.
 #pragma once
 
-namespace nuppn {
+NUPPN_BEGIN
 
 // state that the reference keeps in module variables of nse_swj (nse_mu, nse_mu_last, first, ...)
 struct NseCtl {
@@ -27,14 +27,14 @@ __device__ __forceinline__ void nse_reset(NseCtl &S) {
 // needs K * warps <= 32 doubles of sred.
 template <int K>
 __device__ void block_sum_k(double (&v)[K], double *sred) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int lane = GT & 31, w = GT >> 5, nw = GN >> 5;
 #pragma unroll
   for (int k = 0; k < K; ++k) v[k] = warp_sum(v[k]);
-  __syncthreads();
+  GSYNC();
   if (lane == 0)
 #pragma unroll
     for (int k = 0; k < K; ++k) sred[k * nw + w] = v[k];
-  __syncthreads();
+  GSYNC();
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     double r = 0.0;
@@ -49,13 +49,13 @@ __device__ void dev_nse_coulomb(const DevNet &N, const Ws &W, NseCtl &S, double 
   const double kT_erg = K_BOLTZMANN * t9 * 1.e9, kT_mev = kT_erg * K_ERG2MEV;
   const double ae = pow(4.0 * K_PI * rho * ye * K_AVOGADRO / 3.0, -(1.0 / 3.0));
   const double Gam_e = K_QE * K_QE / kT_erg / ae;
-  for (int j = threadIdx.x; j < N.nse_num; j += blockDim.x) {
+  for (int j = GT; j < N.nse_num; j += GN) {
     const double G = Gam_e * pow(N.nse_z[j], 5.0 * (1.0 / 3.0));
     const double mc = a1 * (sqrt(G * (a2 + G)) - a2 * log(sqrt(G / a2) + sqrt(1.0 + G / a2))) +
                       2.0 * a3 * (sqrt(G) - atan(sqrt(G)));
     W.nse_mc[j] = mc * kT_mev;
   }
-  __syncthreads();
+  GSYNC();
   S.mu_p_coul = W.nse_mc[N.nse_iprot];
 }
 
@@ -67,37 +67,37 @@ __device__ void dev_nse_partition(const DevNet &N, const Ws &W, double t9) {
     const int i0 = bsearch_r8(N.pt9, kPartDim, t9c);
     const double t90 = N.pt9[i0 - 1], t91 = N.pt9[i0];
     const double Dt9 = (t9c - t90) / (t91 - t90);
-    for (int p = threadIdx.x; p < N.npart; p += blockDim.x) {
+    for (int p = GT; p < N.npart; p += GN) {
       const double *pv = N.pval + (size_t)p * kPartDim;
       W.partinter[p] = pv[i0 - 1] + (pv[i0] - pv[i0 - 1]) * Dt9;
     }
   }
-  __syncthreads();
-  for (int j = threadIdx.x; j < N.nse_num; j += blockDim.x) {
+  GSYNC();
+  for (int j = GT; j < N.nse_num; j += GN) {
     const int p = N.nse_part[j];
     W.nse_gtot[j] = (p >= 0 ? W.partinter[p] : 1.0) * N.nse_g[j];
   }
-  __syncthreads();
+  GSYNC();
 }
 
 // nse_distribution (nse_swj.F90:524-541) into W.nse_x
 __device__ void dev_nse_dist(const DevNet &N, const Ws &W, const NseCtl &S, double mu_p, double mu_n, double t9,
                              double rho) {
   const double kT_erg = K_BOLTZMANN * t9 * 1.e9, kT_mev = kT_erg * K_ERG2MEV;
-  for (int j = threadIdx.x; j < N.nse_num; j += blockDim.x) {
+  for (int j = GT; j < N.nse_num; j += GN) {
     const double m = N.nse_m[j];
     const double lam = sqrt(K_PLANCK_ERG * K_PLANCK_ERG / (2.0 * K_PI * m * kT_erg));
     const double fac = N.nse_z[j] * (mu_p + S.mu_p_coul) + N.nse_n[j] * mu_n - W.nse_mc[j] + N.nse_q[j];
     const double pre = m / rho * W.nse_gtot[j] / (lam * lam * lam);
     W.nse_x[j] = pre * exp(fac / kT_mev);
   }
-  __syncthreads();
+  GSYNC();
 }
 
 // calculate_rhs (nse_swj.F90:510-520): theta = sum X - 1, phi = sum (Z/A) X - Ye
 __device__ void dev_nse_rhs(const DevNet &N, const Ws &W, NseCtl &S, double ye, double *sred) {
   double v[2] = {0.0, 0.0};
-  for (int j = threadIdx.x; j < N.nse_num; j += blockDim.x) {
+  for (int j = GT; j < N.nse_num; j += GN) {
     v[0] += W.nse_x[j];
     v[1] += N.nse_zoa[j] * W.nse_x[j];
   }
@@ -110,7 +110,7 @@ __device__ void dev_nse_rhs(const DevNet &N, const Ws &W, NseCtl &S, double ye, 
 __device__ void dev_nse_jac(const DevNet &N, const Ws &W, double t9, double (&jac)[2][2], double *sred) {
   const double kT_mev = K_BOLTZMANN * t9 * 1.e9 * K_ERG2MEV;
   double v[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int j = threadIdx.x; j < N.nse_num; j += blockDim.x) {
+  for (int j = GT; j < N.nse_num; j += GN) {
     const double dp = W.nse_x[j] * N.nse_z[j] / kT_mev, dn = W.nse_x[j] * N.nse_n[j] / kT_mev;
     v[0] += dp;
     v[1] += dn;
@@ -278,10 +278,10 @@ __device__ int dev_compute_nse(const DevNet &N, const Ws &W, NseCtl &S, double t
     if (ierr != 0) return ierr == BAD_STEP ? BAD_STEP : NSE_CNVRG;
   }
   dev_nse_dist(N, W, S, mu_p, mu_n, t9, rho);
-  for (int s = threadIdx.x; s < N.nsp; s += blockDim.x) yps[s] = 1.e-99;
-  __syncthreads();
-  for (int j = threadIdx.x; j < N.nse_num; j += blockDim.x) yps[N.nse_idx[j]] = fmax(W.nse_x[j], 1e-99);
-  __syncthreads();
+  for (int s = GT; s < N.nsp; s += GN) yps[s] = 1.e-99;
+  GSYNC();
+  for (int j = GT; j < N.nse_num; j += GN) yps[N.nse_idx[j]] = fmax(W.nse_x[j], 1e-99);
+  GSYNC();
   S.mu_last[0] = S.mu[0];
   S.mu_last[1] = S.mu[1];
   S.first = false;
@@ -295,10 +295,10 @@ __device__ __forceinline__ bool weak_label(int lab) {  // ilabb of the weak reac
 // nse_solver_cache_lm_ov_a (nse_solver.F90:33-66): keep only the weak rates in W.v, and for each
 // parent sum (lambda_beta - lambda_ec) / A over its reactions in reaction order (the k1 lists).
 __device__ void dev_nse_cache_lm(const DevNet &N, const Ws &W) {
-  for (int l = threadIdx.x; l < N.nre; l += blockDim.x)
+  for (int l = GT; l < N.nre; l += GN)
     if (!weak_label(N.ilabb[l])) W.v[l] = 0.0;
-  __syncthreads();
-  for (int s = threadIdx.x; s < N.nsp; s += blockDim.x) {
+  GSYNC();
+  for (int s = GT; s < N.nsp; s += GN) {
     double acc = 0.0;
     for (int p = N.k1_ptr[s]; p < N.k1_ptr[s + 1]; ++p) {
       const int a = N.k1_list[p];
@@ -310,7 +310,7 @@ __device__ void dev_nse_cache_lm(const DevNet &N, const Ws &W) {
     }
     W.nse_lm[s] = acc;
   }
-  __syncthreads();
+  GSYNC();
 }
 
 // yedot (nse_solver.F90:104-113): sortedsum(x * lm_ov_a, mask = considerisotope). The reference's
@@ -319,10 +319,10 @@ __device__ void dev_nse_cache_lm(const DevNet &N, const Ws &W) {
 // shared memory when it fits) to leave out the same terms.
 __device__ double dev_nse_yedot(const DevNet &N, const Ws &W, const double *x, char *smem, size_t smem_bytes,
                                 double *sred) {
-  const int tid = threadIdx.x, nt = blockDim.x, P = N.nse_p2;
+  const int tid = GT, nt = GN, P = N.nse_p2;
   double *t = (size_t)P * 8 <= smem_bytes ? (double *)smem : W.nse_sort;
   for (int i = tid; i < P; i += nt) t[i] = i < N.nsp ? x[i] * W.nse_lm[i] : INFINITY;
-  __syncthreads();
+  GSYNC();
   for (int k = 2; k <= P; k <<= 1)
     for (int j = k >> 1; j > 0; j >>= 1) {
       for (int i = tid; i < P; i += nt) {
@@ -335,7 +335,7 @@ __device__ double dev_nse_yedot(const DevNet &N, const Ws &W, const double *x, c
           }
         }
       }
-      __syncthreads();
+      GSYNC();
     }
   double v[1] = {0.0};
   for (int i = tid; i < N.nsp; i += nt)
@@ -399,9 +399,9 @@ __device__ int dev_nse_rk4(const DevNet &N, const Ws &W, NseCtl &S, double *yps,
   } else {
     ierr = 0;
     fac = pow(fabs(ye_tol * ye / fmax(error, K_SMALL)), 1.0 / 5.0);
-    for (int s = threadIdx.x; s < N.nsp; s += blockDim.x) yps[s] = W.nse_y1[s];
+    for (int s = GT; s < N.nsp; s += GN) yps[s] = W.nse_y1[s];
   }
-  __syncthreads();
+  GSYNC();
   dtrcmd = dt * fmax(fmin(fac, maxfac), minfac);
   return ierr;
 }
@@ -426,12 +426,12 @@ __device__ int dev_nse_euler(const DevNet &N, const Ws &W, NseCtl &S, double *yp
   ye = ye + d_ye;
   ierr = dev_compute_nse(N, W, S, t9, rho, ye, W.nse_y1, mu_p, mu_n, iters, sred);
   if (ierr == 0)
-    for (int s = threadIdx.x; s < N.nsp; s += blockDim.x) yps[s] = W.nse_y1[s];
+    for (int s = GT; s < N.nsp; s += GN) yps[s] = W.nse_y1[s];
   else
     ierr = NSE_CNVRG;
-  __syncthreads();
+  GSYNC();
   dtrcmd = deltamax / fabs(dyedt);
   return ierr;
 }
 
-}  // namespace nuppn
+NUPPN_END

@@ -20,7 +20,7 @@
 
 #include "solver.cuh"
 
-namespace nuppn {
+NUPPN_BEGIN
 
 __constant__ double c_fact[5] = {1.0, 1.0, 0.5, 1.0 / 6.0, 1.0 / 24.0};
 
@@ -59,27 +59,33 @@ struct Red {
 // Every thread returns the same value (partials combined in a fixed order).
 __device__ double block_sum(double v, double *sbuf) {
   v = warp_sum(v);
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0) sbuf[threadIdx.x >> 5] = v;
-  __syncthreads();
+#if NUPPN_GROUP_WARP
+  return v;  // the xor butterfly leaves the same sum in every lane
+#endif
+  GSYNC();
+  if ((GT & 31) == 0) sbuf[GT >> 5] = v;
+  GSYNC();
   double r = 0.0;
-  const int nw = blockDim.x >> 5;
+  const int nw = GN >> 5;
   for (int i = 0; i < nw; ++i) r += sbuf[i];
   return r;
 }
 
 __device__ double block_max(double v, double *sbuf) {
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(NUPPN_FULL, v, o));
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0) sbuf[threadIdx.x >> 5] = v;
-  __syncthreads();
+#if NUPPN_GROUP_WARP
+  return v;
+#endif
+  GSYNC();
+  if ((GT & 31) == 0) sbuf[GT >> 5] = v;
+  GSYNC();
   double r = -DBL_MAX;
-  const int nw = blockDim.x >> 5;
+  const int nw = GN >> 5;
   for (int i = 0; i < nw; ++i) r = fmax(r, sbuf[i]);
   return r;
 }
 
-__device__ bool block_any(bool p) { return __syncthreads_or(p ? 1 : 0) != 0; }
+__device__ bool block_any(bool p) { return g_or(p ? 1 : 0) != 0; }
 
 // gfortran integer power (square-and-multiply, libgcc __powidf2)
 __device__ __forceinline__ double powi(double x, int m) {
@@ -139,7 +145,7 @@ __device__ __forceinline__ double screening(const DevNet &N, const Screen &S, do
 // evaluate_all_rates for the CTA's zone; y = mass fractions (read for screening and VITAL)
 __device__ void dev_eval_rates(const DevNet &N, const Ws &W, double t9, double rho, double ye, const double *y,
                                double *sred) {
-  const int tid = threadIdx.x, nt = blockDim.x;
+  const int tid = GT, nt = GN;
   // partition functions (reaclib.F90:586-605)
   if (N.npart > 0) {
     double t9c = fmax(N.pt9[0], fmin(t9, N.pt9[kPartDim - 1]));
@@ -151,7 +157,7 @@ __device__ void dev_eval_rates(const DevNet &N, const Ws &W, double t9, double r
       W.partinter[p] = pv[i0 - 1] + (pv[i0] - pv[i0 - 1]) * Dt9;
     }
   }
-  __syncthreads();
+  GSYNC();
   // REACLIB rates (reaclib.F90:471-581)
   {
     double t = fmax(t9, 0.01), rhoye = rho * ye;
@@ -272,7 +278,7 @@ __device__ void dev_eval_rates(const DevNet &N, const Ws &W, double t9, double r
     double g = N.gspin_nse[s];
     W.G[s] = g != 0.0 ? (N.spart[s] >= 0 ? W.partinter[N.spart[s]] : 1.0) * g : 1.0;
   }
-  __syncthreads();
+  GSYNC();
   // gather by source (ppn_physics.F90:550-589), VITAL, constants; rate factors (evaluate_rates.F90:195)
   {
     double tv = fmin(t9, 10.0), tm13 = 1.0 / pow(tv, 1.0 / 3.0);
@@ -303,7 +309,7 @@ __device__ void dev_eval_rates(const DevNet &N, const Ws &W, double t9, double r
       W.v[l] = fmax(v * N.rfac[l], 1.e-99);
     }
   }
-  __syncthreads();
+  GSYNC();
   // detailed balance (reverse.F90:107-335, Coulomb corrections off); forwards read before writes
   if (N.kn.detailed_balance) {
     double kTerg = K_BOLTZMANN * t9 * 1.e9, kTMeV = kTerg * K_ERG2MEV;
@@ -329,7 +335,7 @@ __device__ void dev_eval_rates(const DevNet &N, const Ws &W, double t9, double r
       }
       W.contrib[l] = out;
     }
-    __syncthreads();
+    GSYNC();
     for (int l = tid; l < N.nre; l += nt)
       if (W.contrib[l] >= 0.0) W.v[N.irev[l]] = W.contrib[l];
   }
@@ -388,21 +394,21 @@ __device__ void dev_eval_rates(const DevNet &N, const Ws &W, double t9, double r
       W.v[l] = fmax(v, 1.e-99);
     }
   }
-  __syncthreads();
+  GSYNC();
 }
 
 // ---------------------------------------------------------------------------------------------
 // RHS: calculate_dxdt (jac_rhs.F90:217-278)
 __device__ void dev_dxdt(const DevNet &N, const Ws &W, const double *x, double *dxdt) {
-  const int tid = threadIdx.x, nt = blockDim.x;
+  const int tid = GT, nt = GN;
   for (int s = tid; s < N.nsp; s += nt)
     W.xn[s] = s == N.ig ? 1.0 : ((N.ciso[s] && N.an[s] != 0.0) ? x[s] / N.an[s] : 0.0);
-  __syncthreads();
+  GSYNC();
   for (int a = tid; a < N.nact; a += nt) {
     const int *k = N.act_k + (size_t)a * 8;
     W.flux[a] = c_fact[k[1]] * W.v[N.act_slot[a]] * powi(W.xn[k[0]], k[1]) * W.xn[k[2]];
   }
-  __syncthreads();
+  GSYNC();
   for (int s = tid; s < N.nsp; s += nt) {
     int p0 = N.dg_ptr[s], p1 = N.dg_ptr[s + 1];
     if (p1 - p0 > kLongList) continue;
@@ -425,7 +431,7 @@ __device__ void dev_dxdt(const DevNet &N, const Ws &W, const double *x, double *
       }
     }
   }
-  __syncthreads();
+  GSYNC();
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -434,14 +440,14 @@ __device__ void dev_dxdt(const DevNet &N, const Ws &W, const double *x, double *
 // its participants were masked by a reaction a' <= a. first_l[s] = min a' that masks s reproduces
 // that exactly.
 __device__ void dev_jacobian(const DevNet &N, const Ws &W, double dzeit, const double *x) {
-  const int tid = threadIdx.x, nt = blockDim.x, g = N.ig;
+  const int tid = GT, nt = GN, g = N.ig;
   const double dfdNmin = N.kn.cyminformal / dzeit;
   for (int s = tid; s < N.nsp; s += nt) {
     W.xn[s] = s == g ? 1.0 : ((N.ciso[s] && N.an[s] > 0.0) ? x[s] / N.an[s] : 0.0);
     W.first_l[s] = 0x7fffffff;
   }
   for (int e = tid; e < N.nnzJ; e += nt) W.eset[e] = 0;
-  __syncthreads();
+  GSYNC();
   for (int a = tid; a < N.nact; a += nt) {
     const int *k = N.act_k + (size_t)a * 8;
     double v = W.v[N.act_slot[a]];
@@ -478,7 +484,7 @@ __device__ void dev_jacobian(const DevNet &N, const Ws &W, double dzeit, const d
     c[6] = (in2 != g && out1 != g) ? dfout1dy2 * aout1 / ain2 : 0.0;
     c[7] = (in2 != g && out2 != g) ? dfout2dy2 * aout2 / ain2 : 0.0;
   }
-  __syncthreads();
+  GSYNC();
   for (int a = tid; a < N.nact; a += nt) {
     if (W.flux[a] == 0.0) continue;
     const int *k = N.act_k + (size_t)a * 8;
@@ -514,20 +520,20 @@ __device__ void dev_jacobian(const DevNet &N, const Ws &W, double dzeit, const d
     }
   }
   for (int s = tid; s < N.nsp; s += nt) W.mask[s] = (W.first_l[s] != 0x7fffffff && s != g) ? 1 : 0;
-  __syncthreads();
+  GSYNC();
 }
 
 // First pass of calculate_jacobian for the integrator: only the dynamic-network mask (first_l, mask)
 // and each reaction's rate test (flux[a] = 1 if |v|/dt > min_rate_ov_dt). The values and entry flags
 // are then built for the active subsystem only (dev_jacobian_active, active_lu.cuh).
 __device__ void dev_jacobian_mask(const DevNet &N, const Ws &W, double dzeit, const double *x) {
-  const int tid = threadIdx.x, nt = blockDim.x, g = N.ig;
+  const int tid = GT, nt = GN, g = N.ig;
   const double dfdNmin = N.kn.cyminformal / dzeit;
   for (int s = tid; s < N.nsp; s += nt) {
     W.xn[s] = s == g ? 1.0 : ((N.ciso[s] && N.an[s] > 0.0) ? x[s] / N.an[s] : 0.0);
     W.first_l[s] = 0x7fffffff;
   }
-  __syncthreads();
+  GSYNC();
   for (int a = tid; a < N.nact; a += nt) {
     const int *k = N.act_k + (size_t)a * 8;
     const double v = W.v[N.act_slot[a]];
@@ -542,49 +548,61 @@ __device__ void dev_jacobian_mask(const DevNet &N, const Ws &W, double dzeit, co
       atomicMin(&W.first_l[k[4]], a); atomicMin(&W.first_l[k[6]], a);
     }
   }
-  __syncthreads();
+  GSYNC();
   for (int s = tid; s < N.nsp; s += nt) W.mask[s] = (W.first_l[s] != 0x7fffffff && s != g) ? 1 : 0;
-  __syncthreads();
+  GSYNC();
 }
-}  // namespace nuppn
+NUPPN_END
 
 #include "active_lu.cuh"
 #include "nse.cuh"
 #include "integrator.cuh"
 
-namespace nuppn {
+NUPPN_BEGIN
 
 // ---------------------------------------------------------------------------------------------
 // kernels: persistent CTAs, one zone at a time, workspace slab per CTA; dynamic shared memory holds
 // the active-subsystem LU when it fits (act_smem bytes).
 // kTraj: tppnp's trajectory loop per zone (IntegrateArgs::npts > 0); a separate instantiation so the
 // single-interval kernel keeps its own register allocation.
+// One zone per group: a CTA of the cta variant (3 resident per SM), a warp of the warp variant (8
+// per CTA, one CTA per SM: the groups' shares of shared memory set the residency). Each group owns
+// workspace slab blockIdx.x * groups + GID and act_smem bytes of the dynamic shared memory.
+#if NUPPN_GROUP_WARP
+#define NUPPN_INTEGRATE_BOUNDS __launch_bounds__(256, 1)
+#else
+#define NUPPN_INTEGRATE_BOUNDS __launch_bounds__(256, 3)
+#endif
 template <bool kTraj>
-__global__ void __launch_bounds__(256, 3) k_integrate(const __grid_constant__ DevNet N, const __grid_constant__ WsLayout L,
+__global__ void NUPPN_INTEGRATE_BOUNDS k_integrate(const __grid_constant__ DevNet N, const __grid_constant__ WsLayout L,
                                                    char *ws, const __grid_constant__ IntegrateArgs A, int act_smem) {
   extern __shared__ __align__(16) char smem_dyn[];
-  __shared__ double sred[32];
-  __shared__ int sint[32];
-  __shared__ int zsh;
-  const Ws W = ws_bind(ws + (size_t)blockIdx.x * L.bytes, L);
+  __shared__ double sred_g[NUPPN_MAX_GROUPS][32];
+  __shared__ int sint_g[NUPPN_MAX_GROUPS][32];
+  __shared__ int zsh_g[NUPPN_MAX_GROUPS];
+  double *sred = sred_g[GID];
+  int *sint = sint_g[GID];
+  int &zsh = zsh_g[GID];
+  const int groups = (int)blockDim.x / GN;
+  const Ws W = ws_bind(ws + ((size_t)blockIdx.x * groups + GID) * L.bytes, L);
   for (;;) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    GSYNC();
+    if (GT == 0) {
       const int k = atomicAdd(A.counter, 1);
       zsh = (k < A.nz && A.order) ? A.order[k] : k;
     }
-    __syncthreads();
+    GSYNC();
     const int z = zsh;
     if (z >= A.nz) break;
-    for (int s = threadIdx.x; s < N.nsp; s += blockDim.x) W.y[s] = A.X[(size_t)z * A.ldx + s];
-    __syncthreads();
+    for (int s = GT; s < N.nsp; s += GN) W.y[s] = A.X[(size_t)z * A.ldx + s];
+    GSYNC();
     ZoneCtl C;
     memset(&C.st, 0, sizeof(C.st));
     int st = A.bd_state ? A.bd_state[z] : 0;
     C.kopt = (st >= 2 && st <= N.kmax) ? st : N.kopt0;
     C.reduce = false;
     C.sumerr = 0.0;
-    C.smem = smem_dyn;
+    C.smem = smem_dyn + (size_t)GID * act_smem;
     C.smem_bytes = act_smem;
     C.sint = sint;
     nse_reset(C.nse);
@@ -610,8 +628,8 @@ __global__ void __launch_bounds__(256, 3) k_integrate(const __grid_constant__ De
     } else {
       ierr = dev_integrate_zone(N, W, C, A.t9_0[z], A.t9_1[z], A.rho_0[z], A.rho_1[z], ye, A.dtwant[z], st <= 0, sred);
     }
-    for (int s = threadIdx.x; s < N.nsp; s += blockDim.x) A.X[(size_t)z * A.ldx + s] = W.y[s];
-    if (threadIdx.x == 0) {
+    for (int s = GT; s < N.nsp; s += GN) A.X[(size_t)z * A.ldx + s] = W.y[s];
+    if (GT == 0) {
       A.ye[z] = ye;
       A.ierr[z] = ierr;
       if (A.stats) A.stats[z] = C.st;
@@ -621,19 +639,20 @@ __global__ void __launch_bounds__(256, 3) k_integrate(const __grid_constant__ De
   }
 }
 
+#if !NUPPN_GROUP_WARP
 __global__ void __launch_bounds__(256) k_phase(const __grid_constant__ DevNet N, const __grid_constant__ WsLayout L,
                                                char *ws, const __grid_constant__ PhaseArgs A, int act_smem) {
   extern __shared__ __align__(16) char smem_dyn[];
   __shared__ double sred[32];
   __shared__ int sint[32];
   const Ws W = ws_bind(ws + (size_t)blockIdx.x * L.bytes, L);
-  const int tid = threadIdx.x, nt = blockDim.x;
+  const int tid = GT, nt = GN;
   for (int z = blockIdx.x; z < A.nz; z += gridDim.x) {
     if (A.X)
       for (int s = tid; s < N.nsp; s += nt) W.y[s] = A.X[(size_t)z * A.ldx + s];
     if (A.v_in)
       for (int l = tid; l < N.nre; l += nt) W.v[l] = A.v_in[(size_t)z * N.nre + l];
-    __syncthreads();
+    GSYNC();
     if (A.op == 0) {
       dev_eval_rates(N, W, A.t9[z], A.rho[z], A.ye[z], W.y, sred);
       for (int l = tid; l < N.nre; l += nt) A.out_v[(size_t)z * N.nre + l] = W.v[l];
@@ -656,7 +675,7 @@ __global__ void __launch_bounds__(256) k_phase(const __grid_constant__ DevNet N,
         W.mask[s] = A.mask_in[(size_t)z * N.nsp + s];
         W.rhs[s] = A.b[(size_t)z * N.nsp + s];
       }
-      __syncthreads();
+      GSYNC();
       Act act;
       dev_compact(N, W, act, smem_dyn, act_smem, sint);
       dev_load_active_jacobian(N, W, act);
@@ -677,7 +696,7 @@ __global__ void __launch_bounds__(256) k_phase(const __grid_constant__ DevNet N,
         A.out_ierr[z] = ierr;
       }
     }
-    __syncthreads();
+    GSYNC();
   }
 }
 
@@ -692,8 +711,8 @@ constexpr int kOrderBins = 1024;
 __global__ void __launch_bounds__(1024) k_zone_order(const double *key, const double *key_b, int stride, int nz,
                                                      int *order) {
   __shared__ int cnt[kOrderBins];
-  for (int b = threadIdx.x; b < kOrderBins; b += blockDim.x) cnt[b] = 0;
-  __syncthreads();
+  for (int b = GT; b < kOrderBins; b += GN) cnt[b] = 0;
+  GSYNC();
   auto bin_of = [&](int z) {
     double t = key[(size_t)z * stride];
     if (key_b) t = fmax(t, key_b[(size_t)z * stride]);
@@ -702,9 +721,9 @@ __global__ void __launch_bounds__(1024) k_zone_order(const double *key, const do
     const int b = u <= 0.0 ? 0 : (u >= kOrderBins - 1 ? kOrderBins - 1 : (int)u);
     return kOrderBins - 1 - b;  // hottest first
   };
-  for (int z = threadIdx.x; z < nz; z += blockDim.x) atomicAdd(&cnt[bin_of(z)], 1);
-  __syncthreads();
-  if (threadIdx.x == 0) {  // exclusive offsets (1024 bins: a serial pass is a few microseconds)
+  for (int z = GT; z < nz; z += GN) atomicAdd(&cnt[bin_of(z)], 1);
+  GSYNC();
+  if (GT == 0) {  // exclusive offsets (1024 bins: a serial pass is a few microseconds)
     int acc = 0;
     for (int b = 0; b < kOrderBins; ++b) {
       const int c = cnt[b];
@@ -712,8 +731,8 @@ __global__ void __launch_bounds__(1024) k_zone_order(const double *key, const do
       acc += c;
     }
   }
-  __syncthreads();
-  for (int z = threadIdx.x; z < nz; z += blockDim.x) order[atomicAdd(&cnt[bin_of(z)], 1)] = z;
+  GSYNC();
+  for (int z = GT; z < nz; z += GN) order[atomicAdd(&cnt[bin_of(z)], 1)] = z;
 }
 
 cudaError_t launch_zone_order(const double *key, const double *key_b, int stride, int nz, int *order,
@@ -722,29 +741,41 @@ cudaError_t launch_zone_order(const double *key, const double *key_b, int stride
   return cudaGetLastError();
 }
 
+#endif  // !NUPPN_GROUP_WARP
+
+// act_smem: shared-memory bytes of each group; the launch gives every group of the CTA its share.
 cudaError_t launch_integrate(const DevNet &N, const WsLayout &L, char *ws, int grid, int block, int act_smem,
                              const IntegrateArgs &A, cudaStream_t st) {
-  if (A.npts > 0) k_integrate<true><<<grid, block, act_smem, st>>>(N, L, ws, A, act_smem);
-  else k_integrate<false><<<grid, block, act_smem, st>>>(N, L, ws, A, act_smem);
+  const size_t dyn = (size_t)act_smem * NUPPN_GROUPS_PER_CTA(block);
+  if (A.npts > 0) k_integrate<true><<<grid, block, dyn, st>>>(N, L, ws, A, act_smem);
+  else k_integrate<false><<<grid, block, dyn, st>>>(N, L, ws, A, act_smem);
   return cudaGetLastError();
 }
 
+#if !NUPPN_GROUP_WARP
 cudaError_t launch_phase(const DevNet &N, const WsLayout &L, char *ws, int grid, int block, int act_smem,
                          const PhaseArgs &A, cudaStream_t st) {
   k_phase<<<grid, block, act_smem, st>>>(N, L, ws, A, act_smem);
   return cudaGetLastError();
 }
+#endif
 
-cudaError_t configure_kernels(int act_smem) {
-  cudaError_t e = cudaFuncSetAttribute(k_integrate<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, act_smem);
+// dyn_smem: dynamic shared memory of a whole CTA
+cudaError_t configure_kernels(int dyn_smem) {
+  cudaError_t e = cudaFuncSetAttribute(k_integrate<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_smem);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_integrate<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, act_smem);
+  e = cudaFuncSetAttribute(k_integrate<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_smem);
+#if !NUPPN_GROUP_WARP
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_phase, cudaFuncAttributeMaxDynamicSharedMemorySize, act_smem);
+  e = cudaFuncSetAttribute(k_phase, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_smem);
+#endif
+  return e;
 }
 
+// CTAs of `block` threads resident per SM when every group has act_smem bytes of shared memory
 cudaError_t occupancy_integrate(int block, int act_smem, int *per_sm) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_integrate<false>, block, act_smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_integrate<false>, block,
+                                                       (size_t)act_smem * NUPPN_GROUPS_PER_CTA(block));
 }
 
-}  // namespace nuppn
+NUPPN_END

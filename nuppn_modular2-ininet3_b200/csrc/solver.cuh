@@ -1,11 +1,20 @@
-// solver.cuh -- device side of the B200 solver: one CTA advances one zone at a time.
+// solver.cuh -- device side of the B200 solver: a thread group advances one zone at a time.
 //
-// Data layout: the network (DevNet) is zone-shared and read-only; every CTA owns a workspace slab
+// Data layout: the network (DevNet) is zone-shared and read-only; every group owns a workspace slab
 // (WsLayout) holding its zone's rates, Jacobian values, LU values and integrator vectors, so each
-// per-zone sweep is a contiguous, coalesced stream. Every phase below is a block-wide loop followed
-// by a barrier; scalar control flow (step-size logic of solver.F90, backward_euler.F90 and
-// bader_deuflhard.F90) is evaluated redundantly by all threads from block-reduced values, so it
-// is uniform across the CTA.
+// per-zone sweep is a contiguous, coalesced stream. Every phase below is a group-wide loop followed
+// by a group barrier; scalar control flow (step-size logic of solver.F90, backward_euler.F90 and
+// bader_deuflhard.F90) is evaluated redundantly by all threads of the group from group-reduced
+// values, so it is uniform across the group.
+//
+// The group is a compile-time choice: solver.cu is compiled twice.
+//   NUPPN_GROUP_WARP = 0 (namespace nuppn::cta):  the group is the whole CTA, one zone per CTA; the
+//                                                  wide phases use every warp, the chains one warp.
+//   NUPPN_GROUP_WARP = 1 (namespace nuppn::warp): the group is one warp, one zone per warp and as
+//                                                  many zones per CTA as it has warps; every phase,
+//                                                  chains included, runs on that warp.
+// GT / GN / GID are the thread's rank in its group, the group size and the group's index in the CTA;
+// GSYNC() is the group barrier, g_or / g_and its predicate reductions.
 #pragma once
 #include <cuda_runtime.h>
 #include <float.h>
@@ -14,7 +23,41 @@
 
 #include "nuppn_internal.h"
 
-namespace nuppn {
+#ifndef NUPPN_GROUP_WARP
+#define NUPPN_GROUP_WARP 0
+#endif
+
+#if NUPPN_GROUP_WARP
+#define NUPPN_VNS warp
+#define GT ((int)(threadIdx.x & 31u))
+#define GN 32
+#define GID ((int)(threadIdx.x >> 5))
+#define GSYNC() __syncwarp()
+#define NUPPN_MAX_GROUPS 8
+__device__ __forceinline__ int g_or(int p) { return __any_sync(0xffffffffu, p); }
+__device__ __forceinline__ int g_and(int p) { return __all_sync(0xffffffffu, p); }
+#else
+#define NUPPN_VNS cta
+#define GT ((int)threadIdx.x)
+#define GN ((int)blockDim.x)
+#define GID 0
+#define GSYNC() __syncthreads()
+#define NUPPN_MAX_GROUPS 1
+__device__ __forceinline__ int g_or(int p) { return __syncthreads_or(p); }
+__device__ __forceinline__ int g_and(int p) { return __syncthreads_and(p); }
+#endif
+
+// groups (zones) in a CTA of `block` threads, for host code
+#define NUPPN_GROUPS_PER_CTA(block) (NUPPN_GROUP_WARP ? (block) / 32 : 1)
+
+#define NUPPN_BEGIN \
+  namespace nuppn {  \
+  namespace NUPPN_VNS {
+#define NUPPN_END \
+  }                \
+  }
+
+NUPPN_BEGIN
 
 #define NUPPN_FULL 0xffffffffu
 
@@ -69,4 +112,4 @@ __device__ __forceinline__ Ws ws_bind(char *base, const WsLayout &L) {
   return w;
 }
 
-}  // namespace nuppn
+NUPPN_END

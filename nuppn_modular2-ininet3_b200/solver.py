@@ -53,6 +53,7 @@ def load_library():
     L.nuppn_solve_reduced.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp]
     L.nuppn_integrate.argtypes = [vp, i32, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.nuppn_integrate_device.argtypes = [vp, i32, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.nuppn_autotune.argtypes = [vp, i32, vp, i32, vp, vp, vp, vp, vp, vp, i32, vp, i32, vp]
     L.nuppn_launch_count.argtypes = [vp]
     L.nuppn_launch_count.restype = i64
     L.nuppn_nse.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp]
@@ -70,7 +71,7 @@ def load_library():
                  "nuppn_solve_reduced", "nuppn_integrate", "nuppn_integrate_device", "nuppn_nse",
                  "nuppn_integrate_trajectories", "nuppn_integrate_trajectories_device",
                  "nuppn_serve_open", "nuppn_serve_submit", "nuppn_serve_submit_trajectory", "nuppn_serve_poll",
-                 "nuppn_serve_info", "nuppn_serve_close"):
+                 "nuppn_serve_info", "nuppn_serve_close", "nuppn_autotune"):
         getattr(L, name).restype = i32
     _LIB = L
     return L
@@ -231,6 +232,20 @@ class NetworkSolver:
         self._check(self.L.nuppn_integrate(self.h, nz, _p(X), X.shape[1], _p(t9_0), _p(t9_1), _p(rho_0),
                                            _p(rho_1), _p(ye), _p(dtwant), _p(ierr), stats, _p(bd)))
         return X, ye, ierr, stats, bd
+
+    def autotune(self, X, t9_0, t9_1, rho_0, rho_1, ye, dtwant, sample=0):
+        """nuppn_autotune: time each kernel shape on this batch (host arrays), keep the fastest.
+        Returns one dict per candidate (shape knobs, zones per SM, ms per call, zone-steps/s, chosen)."""
+        X = np.ascontiguousarray(np.atleast_2d(X), dtype=np.float64)
+        nz = X.shape[0]
+        f = lambda a: _f64(a, nz)
+        args = [f(a) for a in (t9_0, t9_1, rho_0, rho_1, ye, dtwant)]
+        rep = (abi.TuneResult * 8)()
+        n = C.c_int32(0)
+        self._check(self.L.nuppn_autotune(self.h, nz, _p(X), X.shape[1], *[_p(a) for a in args], int(sample), rep, 8,
+                                          C.byref(n)))
+        return [{k: getattr(rep[i], k) for k, _ in abi.TuneResult._fields_ if k != "reserved"}
+                for i in range(n.value)]
 
     def integrate_device(self, X, t9_0, t9_1, rho_0, rho_1, ye, dtwant, ierr, stats=None, bd_state=None,
                          stream=0):
