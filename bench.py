@@ -427,8 +427,10 @@ def run_serve(args, rank, world):
     one-trajectory requests, 40 % He-shell zones (1109 species, BD over 1e10 s), 40 % H-burning zones
     on the 300-species network (T9 U[0.015, 0.08], rho log-U[1, 1e3], BD over 1e10 s), 20 % tppnp
     trajectories (1109 species, 21 points to 10 s), submitted as they arrive to two servers (one per
-    network) on one GPU and polled from this thread. value = accepted zone sub-steps of all requests
-    / (last completion - first arrival); latency = completion - arrival, from the polling loop."""
+    network, 2/3 and 1/3 of the GPU's zone slots) and polled from this thread. The same stream is
+    served twice: by the batched form (one zone per warp) and by the plain form (one zone per CTA).
+    value = accepted zone sub-steps of all requests / (last completion - first arrival); latency =
+    completion - arrival, from the polling loop."""
     if rank != 0:
         return
     if args.impl == "reference":
@@ -452,76 +454,90 @@ def run_serve(args, rank, world):
     pick = rng.integers(0, 1 << 30, size=arrive.size)
     hb_t9 = rng.uniform(0.015, 0.08, size=arrive.size)
     hb_rho = 10.0 ** rng.uniform(0.0, 3.0, size=arrive.size)
-    kn = abi.default_knobs(integration_method=1)
-    d1107 = solver.NetworkSolver(n1107, kn, device=torch.cuda.current_device())
-    d300 = solver.NetworkSolver(n300, kn, device=torch.cuda.current_device())
-    lanes = args.serve_lanes or 4
-    s1107 = solver.Server(d1107, lanes=lanes, max_batch=args.serve_batch)
-    s300 = solver.Server(d300, lanes=max(1, lanes // 2), max_batch=args.serve_batch)
+    dev = torch.cuda.current_device()
 
-    def submit(i):
-        k = kinds[i]
-        if k == 0:
-            z = pick[i] % he.nz
-            return s1107, s1107.submit(he.X[z], he.t9_0[z], he.t9_1[z], he.rho_0[z], he.rho_1[z], he.ye[z], he.dtwant[z])
-        if k == 1:
-            return s300, s300.submit(hb0.X[0], hb_t9[i], hb_t9[i], hb_rho[i], hb_rho[i], hb0.ye[0], 1.0e10)
-        j = pick[i] % tr.nz
-        return s1107, s1107.submit_trajectory(tr.X0[j], tt[j], t9g[j], rhog[j])
+    def serve_stream(shape):
+        kn = abi.default_knobs(integration_method=1, **shape)
+        d1107 = solver.NetworkSolver(n1107, kn, device=dev)
+        d300 = solver.NetworkSolver(n300, kn, device=dev)
+        probe = solver.Server(d1107)  # every zone slot of this kernel shape, to split between the servers
+        total = probe.info().slots
+        probe.close()
+        s1107 = solver.Server(d1107, slots=max(1, (2 * total) // 3))
+        s300 = solver.Server(d300, slots=max(1, total - (2 * total) // 3))
 
-    for i in range(min(args.warmup, arrive.size) * 8):  # warm-up: a few requests of each kind, waited for
-        srv, rid = submit(i % arrive.size)
-        srv.wait(rid)
-    lat = [[], [], []]
-    steps = 0
-    fails = [{}, {}, {}]  # per kind: ierr code -> count
-    out = {}
-    t0 = time.perf_counter()
-    nxt = 0
-    last_done = t0
-    with ClockSampler(torch.cuda.current_device()) as clk:
-        clk.mark()
-        while nxt < arrive.size or out:
-            now = time.perf_counter() - t0
-            while nxt < arrive.size and arrive[nxt] <= now:
-                out[nxt] = submit(nxt)
-                nxt += 1
-            for i in list(out):
-                srv, rid = out[i]
-                r = srv.poll(rid)
-                if r is None:
-                    continue
-                tdone = time.perf_counter()
-                last_done = tdone
-                lat[kinds[i]].append((tdone - t0 - arrive[i]) * 1e3)
-                steps += r[3].nsucc
-                if r[2] != 0:
-                    fails[kinds[i]][str(r[2])] = fails[kinds[i]].get(str(r[2]), 0) + 1
-                del out[i]
-            time.sleep(2e-4)
-    elapsed = last_done - t0 - (arrive[0] if arrive.size else 0.0)
-    s_info = (s1107.info(), s300.info())
-    launches = s_info[0].launches + s_info[1].launches
-    s1107.close()
-    s300.close()
-    allv = np.concatenate([np.array(v) for v in lat if v]) if arrive.size else np.zeros(1)
-    pct = lambda v: {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99))} if len(v) else None
-    value = steps / elapsed
-    print(json.dumps({"metric": "zone-timesteps/s", "value": value, "unit": "zone-timesteps/s", "n_gpus": 1,
-                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
-                      "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        def submit(i):
+            k = kinds[i]
+            if k == 0:
+                z = pick[i] % he.nz
+                return s1107, s1107.submit(he.X[z], he.t9_0[z], he.t9_1[z], he.rho_0[z], he.rho_1[z], he.ye[z],
+                                           he.dtwant[z])
+            if k == 1:
+                return s300, s300.submit(hb0.X[0], hb_t9[i], hb_t9[i], hb_rho[i], hb_rho[i], hb0.ye[0], 1.0e10)
+            j = pick[i] % tr.nz
+            return s1107, s1107.submit_trajectory(tr.X0[j], tt[j], t9g[j], rhog[j])
+
+        for i in range(min(args.warmup, arrive.size) * 8):  # warm-up: a few requests of each kind, waited for
+            srv, rid = submit(i % arrive.size)
+            srv.wait(rid)
+        lat = [[], [], []]
+        steps = 0
+        fails = [{}, {}, {}]  # per kind: ierr code -> count
+        out = {}
+        t0 = time.perf_counter()
+        nxt = 0
+        last_done = t0
+        with ClockSampler(dev) as clk:
+            clk.mark()
+            while nxt < arrive.size or out:
+                now = time.perf_counter() - t0
+                while nxt < arrive.size and arrive[nxt] <= now:
+                    out[nxt] = submit(nxt)
+                    nxt += 1
+                for i in list(out):
+                    srv, rid = out[i]
+                    r = srv.poll(rid)
+                    if r is None:
+                        continue
+                    tdone = time.perf_counter()
+                    last_done = tdone
+                    lat[kinds[i]].append((tdone - t0 - arrive[i]) * 1e3)
+                    steps += r[3].nsucc
+                    if r[2] != 0:
+                        fails[kinds[i]][str(r[2])] = fails[kinds[i]].get(str(r[2]), 0) + 1
+                    del out[i]
+                time.sleep(1e-4)
+        elapsed = last_done - t0 - (arrive[0] if arrive.size else 0.0)
+        info = (s1107.info(), s300.info())
+        s1107.close()
+        s300.close()
+        allv = np.concatenate([np.array(v) for v in lat if v]) if arrive.size else np.zeros(1)
+        pct = lambda v: {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99))} if len(v) else None
+        return {"value": steps / elapsed, "latency_ms": {"all": pct(allv), "heshell_zone": pct(lat[0]),
+                                                         "hburn_zone": pct(lat[1]), "trajectory": pct(lat[2])},
+                "requests_failed": {"heshell_zone": fails[0], "hburn_zone": fails[1], "trajectory": fails[2]},
+                "drain_s": float(elapsed - args.serve_seconds),
+                "zone_slots": {"1107": info[0].slots, "300": info[1].slots},
+                "loop_launches": int(info[0].launches + info[1].launches), "clocks": clk.summary()}
+
+    batched = serve_stream({"threads_per_zone": 32})
+    plain = serve_stream({})
+    print(json.dumps({"metric": "zone-timesteps/s", "value": batched["value"], "unit": "zone-timesteps/s",
+                      "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                      "data": "synthetic",
                       "config": {"workload": "serve: Poisson stream, 40% heshell-1107 zones, 40% hburn-300 zones, "
                                              "20% tppnp-1107 trajectories (21 points)",
                                  "rate_req_per_s": args.rate, "arrival_window_s": args.serve_seconds,
-                                 "requests": int(arrive.size),
-                                 "lanes": {"1107": s_info[0].lanes, "300": s_info[1].lanes},
-                                 "max_batch": {"1107": s_info[0].max_batch, "300": s_info[1].max_batch}},
-                      "latency_ms": {"all": pct(allv), "heshell_zone": pct(lat[0]), "hburn_zone": pct(lat[1]),
-                                     "trajectory": pct(lat[2])},
-                      "requests_failed": {"heshell_zone": fails[0], "hburn_zone": fails[1], "trajectory": fails[2]}, "drain_s": float(elapsed - args.serve_seconds),
-                      "e2e": {"value": value, "unit": "zone-timesteps/s",
+                                 "requests": int(arrive.size), "form": "one zone per warp, device-resident loop"},
+                      "latency_ms": batched["latency_ms"], "requests_failed": batched["requests_failed"],
+                      "drain_s": batched["drain_s"], "zone_slots": batched["zone_slots"],
+                      "plain_form": {k: plain[k] for k in ("value", "latency_ms", "requests_failed", "drain_s",
+                                                           "zone_slots")},
+                      "batched_over_plain": batched["value"] / plain["value"] if plain["value"] else None,
+                      "e2e": {"value": batched["value"], "unit": "zone-timesteps/s",
                               "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
-                      "gpu_launches": int(launches), "clocks": clk.summary()}), flush=True)
+                      "gpu_launches": batched["loop_launches"], "clocks": batched["clocks"]}), flush=True)
 
 
 def main():
@@ -538,9 +554,7 @@ def main():
                          "serve: Poisson request stream through nuppn_serve_*; hburn: the ppn frame of one "
                          "H-burning zone (200 backward-Euler frame steps)")
     ap.add_argument("--rate", type=float, default=2000.0, help="serve: mean requests per second")
-    ap.add_argument("--serve-seconds", type=float, default=5.0, help="serve: arrival window (s)")
-    ap.add_argument("--serve-lanes", type=int, default=0, help="serve: lanes of the 1109-species server (0: 4)")
-    ap.add_argument("--serve-batch", type=int, default=0, help="serve: max requests per launch (0: library)")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="serve: arrival window (s)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define NUPPN_ABI_VERSION 1
+#define NUPPN_ABI_VERSION 2
 
 typedef enum {
   NUPPN_OK = 0,
@@ -205,6 +205,17 @@ nuppn_status nuppn_net_info_get(const nuppn_net *net, nuppn_net_info *info);
  * nuppn_net_create and cannot change afterwards (NUPPN_ERR_ARG if it differs from the handle's). */
 nuppn_status nuppn_set_knobs(nuppn_net *net, const nuppn_knobs *knobs);
 
+/* read_isotopedatabase (physics/source/nuc_data.F90:50-95): the first nnn entries of an isotope
+ * database file in the reference's format (physics/run_template/isotopedatabase.txt and
+ * isotopedatabase_all.txt: three header lines, then Z, A, element symbol, a reference mass number and
+ * a T/F flag per line). Host only, no device needed. For each entry i: z[i], a[i], consider[i] (1 for
+ * T), elem[3*i .. 3*i+2] the symbol, NUL-padded. Any output pointer may be NULL. NUPPN_ERR_ARG if the
+ * file cannot be opened or a line does not parse; NUPPN_ERR_LIMIT if the file has fewer than nnn
+ * entries (where the reference stops the run). networkI (ppn_physics.F90:40-130) keeps the entries
+ * flagged T, in file order, as the network's isotopes after the VITAL species. */
+nuppn_status nuppn_isotopedatabase_read(const char *path, int32_t nnn, int32_t *z, int32_t *a, uint8_t *consider,
+                                        char *elem);
+
 /* Static Jacobian pattern of makemap (jac_rhs.F90:461-540): row/col (0-based) of each COO entry in
  * the reference's row-major numbering, and dns2csr_map[nre][8] (entry index per slot, -1 if the
  * reaction is not considered). Sizes: row/col [nnz_jac]. */
@@ -330,25 +341,30 @@ nuppn_status nuppn_autotune(nuppn_net *net, int32_t nz, const double *X, int32_t
                             const double *dtwant, int32_t sample, nuppn_tune_result *report, int32_t ncand,
                             int32_t *nreport);
 
-/* ---- Serving: continuous batching of independent requests ------------------------------------
+/* ---- Serving: a device-resident request loop ----------------------------------------------------
  * Each request is one call of integrate_network (solver.F90:53) for one zone, or one tppnp
  * trajectory (tppnp.F90:131-168), as the frames issue them one at a time; the server runs them on
- * the GPU as they arrive. It owns `lanes` CUDA streams, each with its own workspace slabs and device
- * buffers. A host worker thread, whenever a lane is idle, takes up to `max_batch` pending requests of
- * one kind (zones, or trajectories with the same number of points) in submission order and launches
- * them there, so batches admitted while others are on the GPU run beside them. A request's result
- * is the one nuppn_integrate / nuppn_integrate_trajectories gives for it alone: zones never read one
- * another's state. The knobs are those of `net` when the server is opened; do not call
- * nuppn_set_knobs or destroy `net` while a server on it is open. Submit, poll and close from one
- * host thread. */
+ * the GPU as they arrive. The server keeps a persistent launch of the integration kernel on its own
+ * stream. Its zone groups (the kernel shape of `net`: a CTA or a warp per zone) take requests one at
+ * a time, in submission order, from a queue in device memory and write each result to host-mapped
+ * memory as soon as that zone is done: a request that arrives while others are on the GPU starts
+ * when any group is free, with no batch to wait for (continuous batching at zone granularity). A
+ * host worker thread copies submitted requests into free queue slots, collects finished ones, and
+ * relaunches the loop if it has left after staying idle (its groups leave after a few tens of
+ * milliseconds without requests; every device wait is bounded). A request's result is the one
+ * nuppn_integrate / nuppn_integrate_trajectories gives for it alone: zones never read one another's
+ * state. The knobs are those of `net` when the server is opened; do not call nuppn_set_knobs or
+ * destroy `net` while a server on it is open. Submit, poll and close from one host thread. Servers on
+ * several handles (networks of different sizes) share the GPU: give each a share of the zone slots,
+ * since a persistent loop holds its CTAs while it has work. */
 typedef struct nuppn_server nuppn_server;
 
-/* lanes: 0 = 4. max_batch: requests per launch, 0 = the GPU's resident CTA slots (large batches
- * measured faster than more lanes with smaller batches: a launch's throughput grows with its batch).
- * Each lane holds
- * a workspace slab per resident CTA; lanes that do not fit in half of the free device memory are
- * not opened (NUPPN_ERR_NOMEM if not even one fits). */
-nuppn_status nuppn_serve_open(nuppn_net *net, int32_t lanes, int32_t max_batch, nuppn_server **out);
+/* slots: zones integrated at once (0 = every zone slot the GPU holds for this kernel shape), rounded
+ * down to whole CTAs and limited by admission: the workspace slabs (one per zone slot) must fit in
+ * half of the free device memory (NUPPN_ERR_NOMEM if not even one CTA's worth fits). queue: requests
+ * that can be on the device at once, waiting or running (0 = 4 x slots; at least slots). Trajectory
+ * requests have at most 512 points (NUPPN_ERR_LIMIT beyond). */
+nuppn_status nuppn_serve_open(nuppn_net *net, int32_t slots, int32_t queue, nuppn_server **out);
 
 /* One zone: X[nsp] (copied at submit), interval T9/rho end points, Ye, dtwant, bd_state (0 = fresh,
  * as for nuppn_integrate). *id identifies the request in nuppn_serve_poll. */
@@ -363,22 +379,25 @@ nuppn_status nuppn_serve_submit_trajectory(nuppn_server *srv, const double *X, i
 /* *done = 1 and the outputs filled (X[nsp], Ye, ierr, stats, bd_state, fail = failed interval or -1
  * for a trajectory) once the request has finished, after which its id is released; *done = 0 while
  * it is pending or on the GPU. Output pointers may be NULL. NUPPN_ERR_ARG for an unknown id;
- * NUPPN_ERR_CUDA if the launch that carried the request failed. */
+ * NUPPN_ERR_CUDA if a CUDA call of the server failed (every request then fails). */
 nuppn_status nuppn_serve_poll(nuppn_server *srv, int64_t id, int32_t *done, double *X, double *ye, int32_t *ierr,
                               nuppn_zone_stats *stats, int32_t *bd_state, int32_t *fail);
 
 typedef struct {
-  int32_t lanes, max_batch, slots_per_lane;
-  int32_t pending;          /* submitted, not yet on the GPU */
-  int32_t in_flight;        /* on the GPU */
-  int64_t launches;         /* kernel launches by the server */
-  int64_t batches;          /* batches launched */
-  int64_t completed;        /* requests finished */
-  int64_t device_bytes;     /* device memory held by the server */
+  int32_t slots;            /* zones integrated at once                                   */
+  int32_t queue;            /* queue slots on the device                                  */
+  int32_t ctas;             /* CTAs of the persistent loop                                */
+  int32_t pending;          /* submitted, waiting for a queue slot                        */
+  int32_t in_flight;        /* in the device queue or running                             */
+  int64_t launches;         /* launches of the persistent loop                            */
+  int64_t published;        /* requests handed to the device                              */
+  int64_t completed;        /* requests finished                                          */
+  int64_t device_bytes;     /* device memory held by the server                           */
 } nuppn_serve_stats;
 nuppn_status nuppn_serve_info(nuppn_server *srv, nuppn_serve_stats *out);
 
-/* Waits for the batches on the GPU, drops requests not yet launched, frees everything. */
+/* Waits for the requests on the device, drops those still waiting for a queue slot, stops the loop
+ * and frees everything. */
 nuppn_status nuppn_serve_close(nuppn_server *srv);
 
 #ifdef __cplusplus

@@ -101,9 +101,9 @@ class ZoneStats(C.Structure):
 
 class ServeStats(C.Structure):
     """nuppn_serve_stats (include/nuppn.h)."""
-    _fields_ = [("lanes", C.c_int32), ("max_batch", C.c_int32), ("slots_per_lane", C.c_int32),
+    _fields_ = [("slots", C.c_int32), ("queue", C.c_int32), ("ctas", C.c_int32),
                 ("pending", C.c_int32), ("in_flight", C.c_int32), ("launches", C.c_int64),
-                ("batches", C.c_int64), ("completed", C.c_int64), ("device_bytes", C.c_int64)]
+                ("published", C.c_int64), ("completed", C.c_int64), ("device_bytes", C.c_int64)]
 
 
 class TuneResult(C.Structure):

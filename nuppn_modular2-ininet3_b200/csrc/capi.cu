@@ -493,6 +493,23 @@ nuppn_status nuppn_set_knobs(nuppn_net *net, const nuppn_knobs *knobs) {
   return NUPPN_OK;
 }
 
+nuppn_status nuppn_isotopedatabase_read(const char *path, int32_t nnn, int32_t *z, int32_t *a, uint8_t *consider,
+                                        char *elem) {
+  std::vector<IsotopeEntry> e;
+  const std::string err = read_isotope_database(path, nnn, e);
+  if (!err.empty()) {
+    set_error(err);
+    return err.find("fewer than") != std::string::npos ? NUPPN_ERR_LIMIT : NUPPN_ERR_ARG;
+  }
+  for (size_t i = 0; i < e.size(); ++i) {
+    if (z) z[i] = e[i].z;
+    if (a) a[i] = e[i].a;
+    if (consider) consider[i] = e[i].consider ? 1 : 0;
+    if (elem) memcpy(elem + 3 * i, e[i].elem, 3);
+  }
+  return NUPPN_OK;
+}
+
 nuppn_status nuppn_jac_pattern(const nuppn_net *net, int32_t *row, int32_t *col, int32_t *map) {
   if (!net) return NUPPN_ERR_ARG;
   const HostNet &H = net->H;
@@ -920,12 +937,19 @@ nuppn_status nuppn_integrate_trajectories(nuppn_net *net, int32_t nz, int32_t np
 
 }  // extern "C"
 
-// ---- serving: continuous batching of independent requests --------------------------------------
-// A server owns lanes (stream, event, workspace slabs, a device "packet" of per-request arrays and
-// its pinned host twin). The worker thread launches a batch on every idle lane that finds pending
-// requests, and completes a lane's requests when its event has fired; batches on different lanes
-// run on the GPU at the same time.
+// ---- serving: a device-resident request loop -----------------------------------------------------
+// The server keeps one persistent launch of the integration kernel (trajectory instantiation, queue
+// mode) on its own stream. Its groups claim published requests one at a time from a queue in device
+// memory and write each result to host-mapped memory as soon as that zone is done, so requests that
+// arrive while others are on the GPU start as soon as a group is free, with no batch to wait for. A
+// host worker thread publishes submitted requests (asynchronous copies of their inputs, then of the
+// published count, on a second stream), collects finished ones, and relaunches the loop when it has
+// left after staying idle. Request seq uses queue slot seq % cap; a slot is reused only once its
+// previous request has finished.
 namespace {
+
+constexpr int kServeMaxPoints = 512;   // points of a trajectory request
+constexpr int kServeIdlePolls = 4000;  // empty polls (sleeps growing to 8 us) before a group leaves
 
 struct ServeReq {
   int64_t id = 0;
@@ -935,40 +959,34 @@ struct ServeReq {
   double t9_0 = 0, t9_1 = 0, rho_0 = 0, rho_1 = 0, ye = 0, dtwant = 0;
   int bd = 0, ierr = 0, fail = -1;
   nuppn_zone_stats st{};
-  int status = 0;  // 0 pending or on the GPU, 1 done, 2 its launch failed
+  long long seq = -1;
+  int status = 0;  // 0 pending or on the GPU, 1 done, 2 failed
   std::string err;
-};
-
-struct ServeLane {
-  cudaStream_t stream = nullptr;
-  cudaEvent_t done = nullptr;
-  DevBuf ws, dev;
-  char *host = nullptr;
-  size_t bytes = 0;
-  int cap = 0, cap_npts = 0;  // requests and trajectory points the packet holds
-  bool busy = false;
-  std::vector<ServeReq *> batch;
-  // packet offsets (identical in the device and the pinned host packet)
-  size_t oX = 0, oye = 0, obd = 0, oierr = 0, ofail = 0, ost = 0, ot90 = 0, ot91 = 0, orh0 = 0, orh1 = 0,
-         odt = 0, oord = 0, ocnt = 0, otime = 0, ot9 = 0, orho = 0;
-
-  size_t layout(int B, int nsp, int npts) {
-    size_t t = 0;
-    auto take = [&](size_t b) { size_t o = t; t = align256(t + std::max<size_t>(b, 8)); return o; };
-    oX = take((size_t)B * nsp * 8); oye = take(B * 8); obd = take(B * 4); oierr = take(B * 4); ofail = take(B * 4);
-    ost = take((size_t)B * sizeof(nuppn_zone_stats)); ot90 = take(B * 8); ot91 = take(B * 8); orh0 = take(B * 8);
-    orh1 = take(B * 8); odt = take(B * 8); oord = take(B * 4); ocnt = take(4);
-    otime = take((size_t)B * npts * 8); ot9 = take((size_t)B * npts * 8); orho = take((size_t)B * npts * 8);
-    return t;
-  }
 };
 
 }  // namespace
 
 struct nuppn_server {
   nuppn_net *net = nullptr;
-  int max_batch = 0, slots = 0;
-  std::vector<ServeLane> lanes;
+  int slots = 0;      // zones integrated at once (workspace slabs)
+  int grid = 0;       // CTAs of the loop
+  int cap = 0;        // queue slots
+  DevBuf ws, dq;      // workspace slabs; device queue
+  char *hmap = nullptr;    // host-mapped results: RingOut[cap], x_out[cap][nsp]
+  char *hstage = nullptr;  // pinned staging: per slot RingIn + X + grid, then published counts [cap], stop
+  size_t stage_slot = 0;
+  RingIn *d_in = nullptr;
+  double *d_xin = nullptr, *d_grid = nullptr;
+  long long *d_pub = nullptr;
+  unsigned long long *d_claimed = nullptr;
+  int *d_stop = nullptr, *h_stop = nullptr;
+  RingOut *h_out = nullptr, *d_out = nullptr;
+  double *h_xout = nullptr, *d_xout = nullptr;
+  cudaStream_t sk = nullptr, sc = nullptr;
+  cudaEvent_t kdone = nullptr;
+  bool running = false;
+  long long published = 0, claimed = 0;
+  std::vector<ServeReq *> in_slot;  // request in each queue slot, or null
   std::thread worker;
   std::mutex mu;
   std::condition_variable cv;
@@ -976,194 +994,167 @@ struct nuppn_server {
   std::unordered_map<int64_t, ServeReq *> reqs;
   int64_t next_id = 1;
   std::atomic<bool> stop{false};
-  std::atomic<int64_t> launches{0}, batches{0}, completed{0};
-  std::atomic<int> in_flight{0};
+  std::atomic<int64_t> launches{0}, completed{0};
+  std::atomic<int> in_flight{0}, queued{0};
   int64_t device_bytes = 0;
+  std::string fatal;  // a failed CUDA call of the worker: every later request fails with it
 };
 
 namespace {
 
-cudaError_t lane_alloc(ServeLane &L, const nuppn_net *net, int B, int npts) {
-  L.cap = B;
-  L.cap_npts = npts;
-  L.bytes = L.layout(B, net->H.nsp, npts);
-  cudaError_t e = L.dev.ensure(L.bytes);
-  if (e != cudaSuccess) return e;
-  if (L.host) cudaFreeHost(L.host);
-  L.host = nullptr;
-  return cudaMallocHost((void **)&L.host, L.bytes);
+// Free everything the server holds (the loop has left).
+void serve_free(nuppn_server *S) {
+  if (S->sk) cudaStreamSynchronize(S->sk);
+  if (S->sc) cudaStreamSynchronize(S->sc);
+  S->ws.release();
+  S->dq.release();
+  if (S->hmap) cudaFreeHost(S->hmap);
+  if (S->hstage) cudaFreeHost(S->hstage);
+  if (S->kdone) cudaEventDestroy(S->kdone);
+  if (S->sk) cudaStreamDestroy(S->sk);
+  if (S->sc) cudaStreamDestroy(S->sc);
+  S->hmap = S->hstage = nullptr;
+  S->kdone = nullptr;
+  S->sk = S->sc = nullptr;
 }
 
-void lane_free(ServeLane &L) {
-  if (L.stream) cudaStreamSynchronize(L.stream);
-  L.ws.release();
-  L.dev.release();
-  if (L.host) cudaFreeHost(L.host);
-  L.host = nullptr;
-  if (L.done) cudaEventDestroy(L.done);
-  if (L.stream) cudaStreamDestroy(L.stream);
-  L.done = nullptr;
-  L.stream = nullptr;
-}
-
-// Pending requests of the oldest one's kind (and point count), oldest first, at most max_batch.
-std::vector<ServeReq *> take_batch(nuppn_server *S) {
-  std::vector<ServeReq *> b;
-  std::lock_guard<std::mutex> lk(S->mu);
-  if (S->pending.empty()) return b;
-  const int kind = S->pending.front()->kind, npts = S->pending.front()->npts;
-  std::deque<ServeReq *> keep;
-  for (ServeReq *r : S->pending) {
-    if ((int)b.size() < S->max_batch && r->kind == kind && r->npts == npts) b.push_back(r);
-    else keep.push_back(r);
-  }
-  S->pending.swap(keep);
-  S->in_flight += (int)b.size();
-  return b;
-}
-
-void fail_batch(nuppn_server *S, std::vector<ServeReq *> &b, const std::string &why) {
-  std::lock_guard<std::mutex> lk(S->mu);
-  for (ServeReq *r : b) { r->status = 2; r->err = why; }
-  S->in_flight -= (int)b.size();
-  S->completed += (int64_t)b.size();
-  b.clear();
-}
-
-#define SK(call)                                                                       \
-  do {                                                                                 \
-    cudaError_t e_ = (call);                                                           \
-    if (e_ != cudaSuccess) return std::string(#call) + ": " + cudaGetErrorString(e_);  \
-  } while (0)
-
-// Stage and launch one batch on an idle lane. Returns "" or what failed.
-std::string lane_launch(nuppn_server *S, ServeLane &L, std::vector<ServeReq *> &b) {
-  nuppn_net *net = S->net;
-  const int n = (int)b.size(), nsp = net->H.nsp, kind = b[0]->kind, npts = b[0]->npts;
-  if (kind == 1 && npts > L.cap_npts) {  // rare: grow the packet (frees synchronise the device)
-    SK(lane_alloc(L, net, L.cap, std::max(npts, 2 * L.cap_npts)));
-  }
-  char *h = L.host, *d = (char *)L.dev.p;
-  for (int i = 0; i < n; ++i) {
-    const ServeReq *r = b[i];
-    memcpy(h + L.oX + (size_t)i * nsp * 8, r->X.data(), (size_t)nsp * 8);
-    ((double *)(h + L.oye))[i] = r->ye;
-    ((int *)(h + L.obd))[i] = r->bd;
-    if (kind == 0) {
-      ((double *)(h + L.ot90))[i] = r->t9_0; ((double *)(h + L.ot91))[i] = r->t9_1;
-      ((double *)(h + L.orh0))[i] = r->rho_0; ((double *)(h + L.orh1))[i] = r->rho_1;
-      ((double *)(h + L.odt))[i] = r->dtwant;
-    } else {
-      memcpy(h + L.otime + (size_t)i * npts * 8, r->time.data(), (size_t)npts * 8);
-      memcpy(h + L.ot9 + (size_t)i * npts * 8, r->t9.data(), (size_t)npts * 8);
-      memcpy(h + L.orho + (size_t)i * npts * 8, r->rho.data(), (size_t)npts * 8);
-    }
-  }
-  L.batch = b;
-  cudaStream_t s = L.stream;
-  auto h2d = [&](size_t off, size_t bytes) { return cudaMemcpyAsync(d + off, h + off, bytes, cudaMemcpyHostToDevice, s); };
-  auto d2h = [&](size_t off, size_t bytes) { return cudaMemcpyAsync(h + off, d + off, bytes, cudaMemcpyDeviceToHost, s); };
-  SK(h2d(L.oX, (size_t)n * nsp * 8));
-  SK(h2d(L.oye, (size_t)n * 8));
-  SK(h2d(L.obd, (size_t)n * 4));
+cudaError_t serve_launch(nuppn_server *S) {
   IntegrateArgs A = {};
-  A.nz = n; A.ldx = nsp; A.X = (double *)(d + L.oX); A.ye = (double *)(d + L.oye);
-  A.ierr = (int *)(d + L.oierr); A.stats = (nuppn_zone_stats *)(d + L.ost); A.bd_state = (int *)(d + L.obd);
-  A.counter = (int *)(d + L.ocnt); A.order = (const int *)(d + L.oord);
-  if (kind == 0) {
-    SK(h2d(L.ot90, (size_t)n * 8)); SK(h2d(L.ot91, (size_t)n * 8));
-    SK(h2d(L.orh0, (size_t)n * 8)); SK(h2d(L.orh1, (size_t)n * 8)); SK(h2d(L.odt, (size_t)n * 8));
-    A.t9_0 = (double *)(d + L.ot90); A.t9_1 = (double *)(d + L.ot91);
-    A.rho_0 = (double *)(d + L.orh0); A.rho_1 = (double *)(d + L.orh1); A.dtwant = (double *)(d + L.odt);
-    SK(launch_zone_order(A.t9_0, A.t9_1, 1, n, (int *)(d + L.oord), s));
-  } else {
-    const size_t np = (size_t)n * npts * 8;
-    SK(h2d(L.otime, np)); SK(h2d(L.ot9, np)); SK(h2d(L.orho, np));
-    A.npts = npts; A.tr_time = (double *)(d + L.otime); A.tr_t9 = (double *)(d + L.ot9);
-    A.tr_rho = (double *)(d + L.orho); A.tr_fail = (int *)(d + L.ofail);
-    SK(launch_zone_order(A.tr_t9, nullptr, npts, n, (int *)(d + L.oord), s));
+  ServeQueue &Q = A.queue;
+  Q.in = S->d_in; Q.out = S->d_out; Q.x_in = S->d_xin; Q.x_out = S->d_xout; Q.grid = S->d_grid;
+  Q.published = S->d_pub; Q.claimed = S->d_claimed; Q.stop = S->d_stop;
+  Q.nslots = S->cap; Q.npts_max = kServeMaxPoints; Q.idle_polls = kServeIdlePolls;
+  A.npts = 1;  // selects the trajectory instantiation, which runs the queue loop
+  cudaError_t e = launch_integrate_net(S->net, (char *)S->ws.p, S->grid, A, S->sk);
+  if (e == cudaSuccess) e = cudaEventRecord(S->kdone, S->sk);
+  if (e == cudaSuccess) {
+    S->running = true;
+    S->launches++;
   }
-  SK(cudaMemsetAsync(d + L.ocnt, 0, sizeof(int), s));
-  SK(launch_integrate_net(net, (char *)L.ws.p, integrate_grid(net, n, S->slots), A, s));
-  S->launches += 2;
-  S->batches += 1;
-  SK(d2h(L.oX, (size_t)n * nsp * 8));
-  SK(d2h(L.oye, (size_t)n * 8));
-  SK(d2h(L.obd, (size_t)n * 4));
-  SK(d2h(L.oierr, (size_t)n * 4));
-  SK(d2h(L.ost, (size_t)n * sizeof(nuppn_zone_stats)));
-  if (kind == 1) SK(d2h(L.ofail, (size_t)n * 4));
-  SK(cudaEventRecord(L.done, s));
-  L.busy = true;
-  return "";
+  return e;
 }
 
-void lane_finish(nuppn_server *S, ServeLane &L, cudaError_t e) {
-  const int nsp = S->net->H.nsp, n = (int)L.batch.size();
-  const char *h = L.host;
-  std::lock_guard<std::mutex> lk(S->mu);
-  for (int i = 0; i < n; ++i) {
-    ServeReq *r = L.batch[i];
-    if (e != cudaSuccess) {
-      r->status = 2;
-      r->err = std::string("batch failed: ") + cudaGetErrorString(e);
-      continue;
-    }
-    memcpy(r->X.data(), h + L.oX + (size_t)i * nsp * 8, (size_t)nsp * 8);
-    r->ye = ((const double *)(h + L.oye))[i];
-    r->bd = ((const int *)(h + L.obd))[i];
-    r->ierr = ((const int *)(h + L.oierr))[i];
-    r->st = ((const nuppn_zone_stats *)(h + L.ost))[i];
-    r->fail = r->kind == 1 ? ((const int *)(h + L.ofail))[i] : -1;
-    r->status = 1;
+// Publish request r in queue slot r->seq % cap: its inputs, then the new published count.
+cudaError_t serve_publish(nuppn_server *S, ServeReq *r) {
+  const int nsp = S->net->H.nsp, slot = (int)(r->seq % S->cap);
+  char *st = S->hstage + (size_t)slot * S->stage_slot;
+  RingIn *in = (RingIn *)st;
+  double *x = (double *)(st + a16(sizeof(RingIn)));
+  double *g = x + nsp;
+  memset(in, 0, sizeof(*in));
+  in->seq = r->seq; in->kind = r->kind; in->npts = r->npts; in->bd = r->bd;
+  in->t9_0 = r->t9_0; in->t9_1 = r->t9_1; in->rho_0 = r->rho_0; in->rho_1 = r->rho_1; in->ye = r->ye;
+  in->dtwant = r->dtwant;
+  memcpy(x, r->X.data(), (size_t)nsp * 8);
+  cudaError_t e = cudaMemcpyAsync(S->d_xin + (size_t)slot * nsp, x, (size_t)nsp * 8, cudaMemcpyHostToDevice, S->sc);
+  if (e == cudaSuccess && r->kind == 1) {
+    memcpy(g, r->time.data(), (size_t)r->npts * 8);
+    memcpy(g + kServeMaxPoints, r->t9.data(), (size_t)r->npts * 8);
+    memcpy(g + 2 * kServeMaxPoints, r->rho.data(), (size_t)r->npts * 8);
+    e = cudaMemcpyAsync(S->d_grid + (size_t)slot * 3 * kServeMaxPoints, g, (size_t)3 * kServeMaxPoints * 8,
+                        cudaMemcpyHostToDevice, S->sc);
   }
-  S->in_flight -= n;
-  S->completed += n;
-  L.batch.clear();
-  L.busy = false;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(S->d_in + slot, in, sizeof(RingIn), cudaMemcpyHostToDevice, S->sc);
+  long long *pub = (long long *)(S->hstage + (size_t)S->cap * S->stage_slot) + slot;
+  *pub = r->seq + 1;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(S->d_pub, pub, sizeof(long long), cudaMemcpyHostToDevice, S->sc);
+  return e;
+}
+
+void serve_fail_all(nuppn_server *S, const std::string &why) {
+  std::lock_guard<std::mutex> lk(S->mu);
+  S->fatal = why;
+  for (ServeReq *r : S->pending) { r->status = 2; r->err = why; S->completed++; S->queued--; }
+  S->pending.clear();
+  for (ServeReq *&r : S->in_slot)
+    if (r) { r->status = 2; r->err = why; S->completed++; S->in_flight--; r = nullptr; }
 }
 
 void serve_loop(nuppn_server *S) {
   cudaSetDevice(S->net->device);
+  const int nsp = S->net->H.nsp;
   for (;;) {
-    bool did = false, busy = false;
-    for (ServeLane &L : S->lanes) {
-      if (!L.busy) continue;
-      const cudaError_t q = cudaEventQuery(L.done);
-      if (q == cudaErrorNotReady) { busy = true; continue; }
-      lane_finish(S, L, q);
+    bool did = false;
+    // finished requests: RingOut::done = seq + 1 (written after the results)
+    for (int slot = 0; slot < S->cap; ++slot) {
+      ServeReq *r = S->in_slot[slot];
+      if (!r) continue;
+      const volatile long long *done = &S->h_out[slot].done;
+      if (*done != r->seq + 1) continue;
+      std::atomic_thread_fence(std::memory_order_acquire);
+      const RingOut &o = S->h_out[slot];
+      std::lock_guard<std::mutex> lk(S->mu);
+      memcpy(r->X.data(), S->h_xout + (size_t)slot * nsp, (size_t)nsp * 8);
+      r->ye = o.ye; r->bd = o.bd; r->ierr = o.ierr; r->st = o.st; r->fail = r->kind == 1 ? o.fail : -1;
+      r->status = 1;
+      S->in_slot[slot] = nullptr;
+      S->in_flight--;
+      S->completed++;
       did = true;
     }
-    if (S->stop.load() && !busy) break;  // finished what was on the GPU; pending requests are dropped
-    if (!S->stop.load()) {
-      for (ServeLane &L : S->lanes) {
-        if (L.busy) continue;
-        std::vector<ServeReq *> b = take_batch(S);
-        if (b.empty()) break;
-        const std::string err = lane_launch(S, L, b);
-        if (!err.empty()) {
-          cudaStreamSynchronize(L.stream);  // copies of the failed batch may still be queued
-          L.batch.clear();
-          L.busy = false;
-          fail_batch(S, b, err);
+    // publish pending requests in order while their queue slot is free
+    if (!S->stop.load() && S->fatal.empty()) {
+      for (;;) {
+        ServeReq *r = nullptr;
+        {
+          std::lock_guard<std::mutex> lk(S->mu);
+          if (S->pending.empty() || S->in_slot[(int)(S->published % S->cap)]) break;
+          r = S->pending.front();
+          S->pending.pop_front();
+          r->seq = S->published++;
+          S->in_slot[(int)(r->seq % S->cap)] = r;
+          S->queued--;
+          S->in_flight++;
+        }
+        const cudaError_t e = serve_publish(S, r);
+        if (e != cudaSuccess) {
+          serve_fail_all(S, std::string("serve: ") + cudaGetErrorString(e));
+          break;
         }
         did = true;
       }
     }
+    // the loop on the device: note when it has left, relaunch it while published requests wait
+    if (S->running) {
+      const cudaError_t q = cudaEventQuery(S->kdone);
+      if (q == cudaSuccess) {
+        S->running = false;
+        unsigned long long c = 0;
+        if (cudaMemcpy(&c, S->d_claimed, sizeof(c), cudaMemcpyDeviceToHost) == cudaSuccess) S->claimed = (long long)c;
+      } else if (q != cudaErrorNotReady) {
+        S->running = false;
+        serve_fail_all(S, std::string("serve loop: ") + cudaGetErrorString(q));
+      }
+    }
+    if (!S->running && S->published > S->claimed && S->fatal.empty()) {  // published requests always run
+      const cudaError_t e = serve_launch(S);
+      if (e != cudaSuccess) serve_fail_all(S, std::string("serve launch: ") + cudaGetErrorString(e));
+      did = true;
+    }
+    if (S->stop.load()) {
+      bool busy = false;
+      for (ServeReq *r : S->in_slot) busy |= r != nullptr;
+      if (!busy || !S->fatal.empty()) break;  // what was on the GPU has finished; pending requests are dropped
+    }
     if (!did) {
       std::unique_lock<std::mutex> lk(S->mu);
-      S->cv.wait_for(lk, std::chrono::microseconds(100));
+      S->cv.wait_for(lk, std::chrono::microseconds(50));
     }
   }
+  // ask the loop to leave and wait for it
+  *S->h_stop = 1;
+  cudaMemcpyAsync(S->d_stop, S->h_stop, sizeof(int), cudaMemcpyHostToDevice, S->sc);
+  cudaStreamSynchronize(S->sc);
+  cudaStreamSynchronize(S->sk);
 }
 
 }  // namespace
 
 extern "C" {
 
-nuppn_status nuppn_serve_open(nuppn_net *net, int32_t lanes, int32_t max_batch, nuppn_server **out) {
+nuppn_status nuppn_serve_open(nuppn_net *net, int32_t slots, int32_t queue, nuppn_server **out) {
   if (!net || !out) { set_error("null argument"); return NUPPN_ERR_ARG; }
-  if (lanes < 0 || max_batch < 0) { set_error("lanes and max_batch must be >= 0"); return NUPPN_ERR_ARG; }
+  if (slots < 0 || queue < 0) { set_error("slots and queue must be >= 0"); return NUPPN_ERR_ARG; }
   *out = nullptr;
   CK(cudaSetDevice(net->device));
   size_t free_b = 0, total_b = 0;
@@ -1171,32 +1162,65 @@ nuppn_status nuppn_serve_open(nuppn_net *net, int32_t lanes, int32_t max_batch, 
   nuppn_server *S = new (std::nothrow) nuppn_server();
   if (!S) return NUPPN_ERR_NOMEM;
   S->net = net;
-  S->slots = resident_slots(net);
-  const int want = lanes > 0 ? lanes : 4;
-  S->max_batch = max_batch > 0 ? max_batch : S->slots;
-  ServeLane probe;
-  const size_t per_lane = (size_t)S->slots * net->L.bytes + probe.layout(S->max_batch, net->H.nsp, 256);
-  const int fit = (int)std::min<size_t>((size_t)want, (free_b / 2) / std::max<size_t>(per_lane, 1));
-  if (fit < 1) {
+  // zones in flight: whole CTAs of the kernel shape, at most the GPU's resident ones and the slabs
+  // that fit in half of the free device memory (admission by free HBM)
+  const int zpc = zones_per_cta(net), resident = resident_slots(net);
+  const int by_mem = (int)std::min<size_t>((size_t)resident, (free_b / 2) / std::max<size_t>(net->L.bytes, 1));
+  int want = slots > 0 ? std::min<int>(slots, resident) : resident;
+  want = std::min(want, by_mem);
+  S->grid = want / zpc;
+  S->slots = S->grid * zpc;
+  if (S->grid < 1) {
     delete S;
-    set_error("nuppn_serve_open: one lane needs " + std::to_string(per_lane) + " bytes, more than half of the " +
-              std::to_string(free_b) + " bytes free");
+    set_error("nuppn_serve_open: not even one CTA of workspace slabs (" + std::to_string((size_t)zpc * net->L.bytes) +
+              " bytes) fits in half of the " + std::to_string(free_b) + " bytes free, or slots < zones per CTA");
     return NUPPN_ERR_NOMEM;
   }
-  S->lanes.resize(fit);
-  for (ServeLane &L : S->lanes) {
-    cudaError_t e = cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = L.ws.ensure((size_t)S->slots * net->L.bytes);
-    if (e == cudaSuccess) e = lane_alloc(L, net, S->max_batch, 256);
-    if (e != cudaSuccess) {
-      for (ServeLane &M : S->lanes) lane_free(M);
-      delete S;
-      set_error(std::string("nuppn_serve_open: ") + cudaGetErrorString(e));
-      return NUPPN_ERR_NOMEM;
+  S->cap = queue > 0 ? std::max<int>(queue, S->slots) : 4 * S->slots;
+  const int nsp = net->H.nsp, cap = S->cap;
+  // device queue: RingIn[cap], x_in[cap][nsp], grid[cap][3][max points], published, claimed, stop
+  const size_t o_in = 0, o_x = align256((size_t)cap * sizeof(RingIn)), o_g = o_x + align256((size_t)cap * nsp * 8);
+  const size_t o_pub = o_g + align256((size_t)cap * 3 * kServeMaxPoints * 8), o_cl = o_pub + 256, o_st = o_cl + 256;
+  const size_t dq_bytes = o_st + 256;
+  const size_t map_bytes = align256((size_t)cap * sizeof(RingOut)) + (size_t)cap * nsp * 8;
+  S->stage_slot = a16(sizeof(RingIn)) + (size_t)nsp * 8 + (size_t)3 * kServeMaxPoints * 8;
+  const size_t stage_bytes = (size_t)cap * S->stage_slot + (size_t)cap * sizeof(long long) + 64;
+  cudaError_t e = cudaStreamCreateWithFlags(&S->sk, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->sc, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->kdone, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = S->ws.ensure((size_t)S->slots * net->L.bytes);
+  if (e == cudaSuccess) e = S->dq.ensure(dq_bytes);
+  if (e == cudaSuccess) e = cudaHostAlloc((void **)&S->hmap, map_bytes, cudaHostAllocMapped | cudaHostAllocPortable);
+  if (e == cudaSuccess) e = cudaHostAlloc((void **)&S->hstage, stage_bytes, cudaHostAllocPortable);
+  if (e == cudaSuccess) e = cudaMemset(S->dq.p, 0, dq_bytes);
+  if (e == cudaSuccess) {
+    memset(S->hmap, 0, map_bytes);
+    memset(S->hstage, 0, stage_bytes);
+    char *dq = (char *)S->dq.p;
+    S->d_in = (RingIn *)(dq + o_in);
+    S->d_xin = (double *)(dq + o_x);
+    S->d_grid = (double *)(dq + o_g);
+    S->d_pub = (long long *)(dq + o_pub);
+    S->d_claimed = (unsigned long long *)(dq + o_cl);
+    S->d_stop = (int *)(dq + o_st);
+    S->h_out = (RingOut *)S->hmap;
+    S->h_xout = (double *)(S->hmap + align256((size_t)cap * sizeof(RingOut)));
+    S->h_stop = (int *)(S->hstage + (size_t)cap * S->stage_slot + (size_t)cap * sizeof(long long));
+    void *dp = nullptr;
+    e = cudaHostGetDevicePointer(&dp, S->hmap, 0);
+    if (e == cudaSuccess) {
+      S->d_out = (RingOut *)dp;
+      S->d_xout = (double *)((char *)dp + align256((size_t)cap * sizeof(RingOut)));
     }
-    S->device_bytes += (int64_t)(L.ws.n + L.dev.n);
   }
+  if (e != cudaSuccess) {
+    serve_free(S);
+    delete S;
+    set_error(std::string("nuppn_serve_open: ") + cudaGetErrorString(e));
+    return NUPPN_ERR_NOMEM;
+  }
+  S->in_slot.assign(cap, nullptr);
+  S->device_bytes = (int64_t)(S->ws.n + S->dq.n);
   S->worker = std::thread(serve_loop, S);
   *out = S;
   return NUPPN_OK;
@@ -1205,9 +1229,15 @@ nuppn_status nuppn_serve_open(nuppn_net *net, int32_t lanes, int32_t max_batch, 
 static nuppn_status serve_enqueue(nuppn_server *S, ServeReq *r, int64_t *id) {
   {
     std::lock_guard<std::mutex> lk(S->mu);
+    if (!S->fatal.empty()) {
+      set_error(S->fatal);
+      delete r;
+      return NUPPN_ERR_CUDA;
+    }
     r->id = S->next_id++;
     S->reqs[r->id] = r;
     S->pending.push_back(r);
+    S->queued++;
   }
   S->cv.notify_one();
   *id = r->id;
@@ -1230,6 +1260,10 @@ nuppn_status nuppn_serve_submit_trajectory(nuppn_server *srv, const double *X, i
                                            const double *t9, const double *rho, int64_t *id) {
   if (!srv || !X || !time || !t9 || !rho || !id) { set_error("null argument"); return NUPPN_ERR_ARG; }
   if (npts < 2) { set_error("npts < 2"); return NUPPN_ERR_ARG; }
+  if (npts > kServeMaxPoints) {
+    set_error("a served trajectory has at most " + std::to_string(kServeMaxPoints) + " points");
+    return NUPPN_ERR_LIMIT;
+  }
   ServeReq *r = new (std::nothrow) ServeReq();
   if (!r) return NUPPN_ERR_NOMEM;
   r->kind = 1;
@@ -1272,13 +1306,13 @@ nuppn_status nuppn_serve_poll(nuppn_server *srv, int64_t id, int32_t *done, doub
 nuppn_status nuppn_serve_info(nuppn_server *srv, nuppn_serve_stats *out) {
   if (!srv || !out) { set_error("null argument"); return NUPPN_ERR_ARG; }
   std::lock_guard<std::mutex> lk(srv->mu);
-  out->lanes = (int32_t)srv->lanes.size();
-  out->max_batch = srv->max_batch;
-  out->slots_per_lane = srv->slots;
-  out->pending = (int32_t)srv->pending.size();
+  out->slots = srv->slots;
+  out->queue = srv->cap;
+  out->ctas = srv->grid;
+  out->pending = srv->queued.load();
   out->in_flight = srv->in_flight.load();
   out->launches = srv->launches.load();
-  out->batches = srv->batches.load();
+  out->published = srv->published;
   out->completed = srv->completed.load();
   out->device_bytes = srv->device_bytes;
   return NUPPN_OK;
@@ -1290,7 +1324,7 @@ nuppn_status nuppn_serve_close(nuppn_server *srv) {
   srv->cv.notify_all();
   if (srv->worker.joinable()) srv->worker.join();
   cudaSetDevice(srv->net->device);
-  for (ServeLane &L : srv->lanes) lane_free(L);
+  serve_free(srv);
   for (auto &kv : srv->reqs) delete kv.second;
   delete srv;
   return NUPPN_OK;

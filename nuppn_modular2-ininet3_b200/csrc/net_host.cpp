@@ -2,6 +2,7 @@
 #include "net_host.h"
 
 #include <algorithm>
+#include <cstdio>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -95,6 +96,51 @@ int group_for(double avg) {
 }
 
 }  // namespace
+
+std::string read_isotope_database(const char *path, int nnn, std::vector<IsotopeEntry> &out) {
+  out.clear();
+  if (!path || nnn < 0) return "isotope database: bad argument";
+  FILE *f = std::fopen(path, "r");
+  if (!f) return std::string("isotope database: cannot open ") + path;
+  char line[512];
+  int header = 0, lineno = 0;
+  std::string err;
+  while ((int)out.size() < nnn && std::fgets(line, sizeof line, f)) {
+    ++lineno;
+    if (header < 3) {  // the reference skips three lines (nuc_data.F90:60-62)
+      ++header;
+      continue;
+    }
+    IsotopeEntry e;
+    char el[16] = {0}, fl[16] = {0};
+    if (std::sscanf(line, "%d %d %15s %lf %15s", &e.z, &e.a, el, &e.amin, fl) != 5) {
+      // a blank line ends the list as an end of file would (nuc_data.F90:64-65, end=98778)
+      bool blank = true;
+      for (const char *c = line; *c; ++c) blank &= (*c == ' ' || *c == '\t' || *c == '\n' || *c == '\r');
+      if (!blank) err = "isotope database: cannot parse line " + std::to_string(lineno);
+      break;
+    }
+    if (std::strlen(el) > 2) {
+      err = "isotope database: element symbol longer than 2 characters on line " + std::to_string(lineno);
+      break;
+    }
+    std::memcpy(e.elem, el, std::strlen(el));
+    const char c = fl[0];
+    if (c == 'T' || c == 't') e.consider = true;
+    else if (c == 'F' || c == 'f') e.consider = false;
+    else {
+      err = "isotope database: flag is not T or F on line " + std::to_string(lineno);
+      break;
+    }
+    out.push_back(e);
+  }
+  std::fclose(f);
+  if (!err.empty()) return err;
+  if ((int)out.size() < nnn)
+    return "isotope database: " + std::to_string(out.size()) + " entries, fewer than the " + std::to_string(nnn) +
+           " requested";
+  return "";
+}
 
 void bd_constants(HostNet &H) {  // bader_deuflhard.F90:66-124
   const double cf = 1, cj = 0.0, cs = 10, clr = cj, safe1 = 0.25, alpha = 5.0 / 7.0;

@@ -71,4 +71,17 @@ struct HostNet {
 std::string build_host_net(const nuppn_net_desc &d, const nuppn_knobs &kn, HostNet &H);
 void bd_constants(HostNet &H);
 
+// One entry of an isotope database file (physics/run_template/isotopedatabase*.txt).
+struct IsotopeEntry {
+  int z = 0, a = 0;
+  char elem[3] = {0, 0, 0};
+  double amin = 0.0;  // the fourth column, a reference mass number
+  bool consider = false;
+};
+// The first nnn entries of an isotope database file (read_isotopedatabase, nuc_data.F90:50-95):
+// three header lines, then per line Z, A, element symbol, the reference mass number and a T/F flag,
+// separated by blanks or tabs. Returns "" or what went wrong (the file cannot be opened, a line does
+// not parse, or the file has fewer than nnn entries, where the reference stops the run).
+std::string read_isotope_database(const char *path, int nnn, std::vector<IsotopeEntry> &out);
+
 }  // namespace nuppn

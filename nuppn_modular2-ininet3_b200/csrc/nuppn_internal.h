@@ -155,6 +155,37 @@ NUPPN_HD inline size_t rhs_bytes(int na, int ngi) {
   return a16((size_t)(na + 1) * 4) + 2 * a16((size_t)ngi * 4) + 2 * a16((size_t)ngi * 8);
 }
 
+// Serving queue of the device-resident request loop (nuppn_serve_*). Request seq uses slot
+// seq % nslots. The host writes its inputs into that slot of device memory (RingIn, x_in, grid) with
+// asynchronous copies on one stream, then advances `published` (a device counter) with a copy on the
+// same stream, so a request is complete in device memory before it is published. Groups of the
+// persistent kernel claim requests in order (claimed, an atomic counter), integrate them and write
+// the results to host-mapped memory (RingOut, x_out); RingOut::done = seq + 1 tells the host that
+// they are there. The host reuses a slot only after its request is done.
+struct RingIn {
+  long long seq;       // request number
+  int kind, npts, bd, pad;  // kind 0: one integrate_network interval, 1: a tppnp trajectory
+  double t9_0, t9_1, rho_0, rho_1, ye, dtwant;
+};
+struct RingOut {
+  long long done;      // seq + 1 once the outputs are written
+  int ierr, fail, bd, pad;
+  double ye;
+  nuppn_zone_stats st;
+};
+struct ServeQueue {
+  const RingIn *in;              // [nslots] device
+  RingOut *out;                  // [nslots] host-mapped
+  const double *x_in;            // [nslots][nsp] device
+  double *x_out;                 // [nslots][nsp] host-mapped
+  const double *grid;            // [nslots][3][npts_max] device: time, T9, rho
+  const long long *published;    // device: requests published so far
+  unsigned long long *claimed;   // device: requests claimed so far
+  const int *stop;               // device: nonzero = leave when idle
+  int nslots, npts_max;
+  int idle_polls;                // empty polls (with a growing sleep, up to ~8 us) before a group leaves
+};
+
 // arguments of the persistent integration kernel
 struct IntegrateArgs {
   int nz, ldx;
@@ -172,6 +203,9 @@ struct IntegrateArgs {
   int npts;
   const double *tr_time, *tr_t9, *tr_rho;
   int *tr_fail;
+  // serving (queue.in != nullptr, trajectory instantiation): requests come from the queue instead of
+  // the arrays above, each a single interval or a trajectory
+  ServeQueue queue;
 };
 
 // arguments of the single-phase parity kernel

@@ -561,44 +561,104 @@ NUPPN_END
 NUPPN_BEGIN
 
 // ---------------------------------------------------------------------------------------------
-// kernels: persistent CTAs, one zone at a time, workspace slab per CTA; dynamic shared memory holds
-// the active-subsystem LU when it fits (act_smem bytes).
-// kTraj: tppnp's trajectory loop per zone (IntegrateArgs::npts > 0); a separate instantiation so the
-// single-interval kernel keeps its own register allocation.
-// One zone per group: a CTA of the cta variant (3 resident per SM), a warp of the warp variant (8
-// per CTA, one CTA per SM: the groups' shares of shared memory set the residency). Each group owns
-// workspace slab blockIdx.x * groups + GID and act_smem bytes of the dynamic shared memory.
+// kernels: persistent groups, one zone at a time, workspace slab per group; dynamic shared memory
+// holds the active-subsystem LU when it fits (act_smem bytes per group).
+constexpr int kQueueSpinLimit = 1 << 24;  // polls of the serving queue per claim, whatever the queue does
 #if NUPPN_GROUP_WARP
 #define NUPPN_INTEGRATE_BOUNDS __launch_bounds__(256, 1)
 #else
 #define NUPPN_INTEGRATE_BOUNDS __launch_bounds__(256, 3)
 #endif
+
+// Next request of the serving queue for the calling thread's group, or -1 once the queue has stayed
+// empty for Q.idle_polls polls (the group then leaves and the host relaunches the loop when requests
+// come again) or the host has asked the loop to stop. Requests are claimed in publication order.
+// Every wait is bounded.
+__device__ long long queue_claim(const ServeQueue &Q) {
+  unsigned ns = 128;
+  int idle = 0;
+  for (int it = 0; it < kQueueSpinLimit; ++it) {
+    const long long p = *(const volatile long long *)Q.published;
+    const unsigned long long c = *(volatile unsigned long long *)Q.claimed;
+    if ((long long)c < p) {
+      if (atomicCAS(Q.claimed, c, c + 1ull) == c) return (long long)c;
+      continue;  // another group took request c
+    }
+    if (*(const volatile int *)Q.stop || ++idle > Q.idle_polls) return -1;
+    __nanosleep(ns);
+    if (ns < 8192) ns <<= 1;
+  }
+  return -1;
+}
+
+// One zone per group: a CTA of the cta variant (3 resident per SM), a warp of the warp variant (8
+// per CTA, one CTA per SM: the groups' shares of shared memory set the residency). Each group owns
+// workspace slab blockIdx.x * groups + GID and act_smem bytes of the dynamic shared memory.
+// kTraj: tppnp's trajectory loop per zone (IntegrateArgs::npts > 0); a separate instantiation so the
+// single-interval kernel keeps its own register allocation. The trajectory instantiation also runs
+// the serving loop (IntegrateArgs::queue), whose requests are single intervals or trajectories.
 template <bool kTraj>
 __global__ void NUPPN_INTEGRATE_BOUNDS k_integrate(const __grid_constant__ DevNet N, const __grid_constant__ WsLayout L,
                                                    char *ws, const __grid_constant__ IntegrateArgs A, int act_smem) {
   extern __shared__ __align__(16) char smem_dyn[];
   __shared__ double sred_g[NUPPN_MAX_GROUPS][32];
   __shared__ int sint_g[NUPPN_MAX_GROUPS][32];
-  __shared__ int zsh_g[NUPPN_MAX_GROUPS];
+  __shared__ long long zsh_g[NUPPN_MAX_GROUPS];
   double *sred = sred_g[GID];
   int *sint = sint_g[GID];
-  int &zsh = zsh_g[GID];
+  long long &zsh = zsh_g[GID];
   const int groups = (int)blockDim.x / GN;
   const Ws W = ws_bind(ws + ((size_t)blockIdx.x * groups + GID) * L.bytes, L);
+  const bool queue = kTraj && A.queue.in != nullptr;
+  const ServeQueue &Q = A.queue;
   for (;;) {
     GSYNC();
     if (GT == 0) {
-      const int k = atomicAdd(A.counter, 1);
-      zsh = (k < A.nz && A.order) ? A.order[k] : k;
+      if (queue) {
+        zsh = queue_claim(Q);
+      } else {
+        const int k = atomicAdd(A.counter, 1);
+        zsh = (k < A.nz && A.order) ? A.order[k] : k;
+      }
     }
     GSYNC();
-    const int z = zsh;
-    if (z >= A.nz) break;
-    for (int s = GT; s < N.nsp; s += GN) W.y[s] = A.X[(size_t)z * A.ldx + s];
+    const long long zq = zsh;
+    if (queue ? zq < 0 : zq >= A.nz) break;
+    // the zone's inputs: arrays indexed by zone, or a queue slot (rewritten by copies between
+    // requests, so read around L1)
+    int z = 0, slot = 0, kind = kTraj ? 1 : 0, npts = A.npts, st = 0;
+    double t9_0 = 0, t9_1 = 0, rho_0 = 0, rho_1 = 0, ye = 0, dtwant = 0;
+    const double *tt = nullptr, *tp = nullptr, *tr = nullptr;
+    bool seq_ok = true;
+    if (queue) {
+      slot = (int)(zq % Q.nslots);
+      const RingIn *in = Q.in + slot;
+      for (int it = 0; __ldcg(&in->seq) != zq; ++it)
+        if (it > kSpinLimit) { seq_ok = false; break; }
+      kind = __ldcg(&in->kind);
+      npts = __ldcg(&in->npts);
+      st = __ldcg(&in->bd);
+      t9_0 = __ldcg(&in->t9_0); t9_1 = __ldcg(&in->t9_1);
+      rho_0 = __ldcg(&in->rho_0); rho_1 = __ldcg(&in->rho_1);
+      ye = __ldcg(&in->ye); dtwant = __ldcg(&in->dtwant);
+      const double *g = Q.grid + (size_t)slot * 3 * Q.npts_max;
+      tt = g; tp = g + Q.npts_max; tr = g + 2 * Q.npts_max;
+      const double *x = Q.x_in + (size_t)slot * N.nsp;
+      for (int s = GT; s < N.nsp; s += GN) W.y[s] = __ldcg(x + s);
+    } else {
+      z = (int)zq;
+      st = A.bd_state ? A.bd_state[z] : 0;
+      ye = A.ye[z];
+      if (kTraj) {
+        tt = A.tr_time + (size_t)z * A.npts; tp = A.tr_t9 + (size_t)z * A.npts; tr = A.tr_rho + (size_t)z * A.npts;
+      } else {
+        t9_0 = A.t9_0[z]; t9_1 = A.t9_1[z]; rho_0 = A.rho_0[z]; rho_1 = A.rho_1[z]; dtwant = A.dtwant[z];
+      }
+      for (int s = GT; s < N.nsp; s += GN) W.y[s] = A.X[(size_t)z * A.ldx + s];
+    }
     GSYNC();
     ZoneCtl C;
     memset(&C.st, 0, sizeof(C.st));
-    int st = A.bd_state ? A.bd_state[z] : 0;
     C.kopt = (st >= 2 && st <= N.kmax) ? st : N.kopt0;
     C.reduce = false;
     C.sumerr = 0.0;
@@ -606,18 +666,18 @@ __global__ void NUPPN_INTEGRATE_BOUNDS k_integrate(const __grid_constant__ DevNe
     C.smem_bytes = act_smem;
     C.sint = sint;
     nse_reset(C.nse);
-    double ye = A.ye[z];
     int ierr, fail = -1;
-    if (kTraj) {
+    if (!seq_ok) {
+      ierr = NUPPN_BAD_INPUT;
+    } else if (kTraj && kind == 1) {
       // the trajectory loop of tppnp (tppnp.F90:131-168) for this zone
-      const double *tt = A.tr_time + (size_t)z * A.npts, *tp = A.tr_t9 + (size_t)z * A.npts;
-      const double *tr = A.tr_rho + (size_t)z * A.npts;
       if (fabs(1.0 - vsum(W.y, N.nsp, sred)) > 1.e-8) dev_renorm_ksum(W.y, N.nsp, sred);
       bool frst = st <= 0;
       ierr = 0;
-      for (int i = 1; i < A.npts; ++i) {
+      for (int i = 1; i < npts; ++i) {
         ye = dev_ye(N, W.y, sred);
-        ierr = dev_integrate_zone(N, W, C, tp[i - 1], tp[i], tr[i - 1], tr[i], ye, tt[i] - tt[i - 1], frst, sred);
+        ierr = dev_integrate_zone(N, W, C, __ldcg(tp + i - 1), __ldcg(tp + i), __ldcg(tr + i - 1), __ldcg(tr + i), ye,
+                                  __ldcg(tt + i) - __ldcg(tt + i - 1), frst, sred);
         frst = false;
         if (ierr != 0) {
           fail = i - 1;
@@ -626,7 +686,24 @@ __global__ void NUPPN_INTEGRATE_BOUNDS k_integrate(const __grid_constant__ DevNe
         if (fabs(1.0 - vsum(W.y, N.nsp, sred)) > 5.e-7) dev_renorm_ksum(W.y, N.nsp, sred);
       }
     } else {
-      ierr = dev_integrate_zone(N, W, C, A.t9_0[z], A.t9_1[z], A.rho_0[z], A.rho_1[z], ye, A.dtwant[z], st <= 0, sred);
+      ierr = dev_integrate_zone(N, W, C, t9_0, t9_1, rho_0, rho_1, ye, dtwant, st <= 0, sred);
+    }
+    if (queue) {
+      // results to host-mapped memory, made visible to the host before `done`
+      double *xo = Q.x_out + (size_t)slot * N.nsp;
+      for (int s = GT; s < N.nsp; s += GN) xo[s] = W.y[s];
+      RingOut *o = Q.out + slot;
+      if (GT == 0) {
+        o->ierr = ierr;
+        o->fail = fail;
+        o->bd = C.kopt;
+        o->ye = ye;
+        o->st = C.st;
+      }
+      __threadfence_system();
+      GSYNC();
+      if (GT == 0) *(volatile long long *)&o->done = zq + 1;
+      continue;
     }
     for (int s = GT; s < N.nsp; s += GN) A.X[(size_t)z * A.ldx + s] = W.y[s];
     if (GT == 0) {
@@ -774,8 +851,14 @@ cudaError_t configure_kernels(int dyn_smem) {
 
 // CTAs of `block` threads resident per SM when every group has act_smem bytes of shared memory
 cudaError_t occupancy_integrate(int block, int act_smem, int *per_sm) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_integrate<false>, block,
-                                                       (size_t)act_smem * NUPPN_GROUPS_PER_CTA(block));
+  // the smaller of the two instantiations' residencies, so that a grid sized by it is resident with
+  // either (the serving loop runs the trajectory instantiation)
+  const size_t dyn = (size_t)act_smem * NUPPN_GROUPS_PER_CTA(block);
+  int a = 0, b = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_integrate<false>, block, dyn);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_integrate<true>, block, dyn);
+  *per_sm = a < b ? a : b;
+  return e;
 }
 
 NUPPN_END

@@ -257,15 +257,16 @@ class NetworkSolver:
 
 
 class Server:
-    """Continuous batching of independent requests (nuppn_serve_*): each request is one zone
-    (integrate_network's arguments) or one trajectory; the library's worker thread launches pending
-    requests on any idle lane while other lanes' batches run. Submit, poll and close from one thread;
-    do not change the solver's knobs while the server is open."""
+    """A device-resident request loop (nuppn_serve_*): each request is one zone (integrate_network's
+    arguments) or one trajectory; a persistent launch takes requests from a device queue as they are
+    submitted, one per zone group, and returns each result as soon as it is done. `slots` = zones
+    integrated at once (0: all the GPU holds), `queue` = requests on the device at once (0: 4 x slots).
+    Submit, poll and close from one thread; do not change the solver's knobs while the server is open."""
 
-    def __init__(self, solver: NetworkSolver, lanes: int = 0, max_batch: int = 0):
+    def __init__(self, solver: NetworkSolver, slots: int = 0, queue: int = 0):
         self.solver, self.L = solver, solver.L
         h = C.c_void_p()
-        solver._check(self.L.nuppn_serve_open(solver.h, lanes, max_batch, C.byref(h)))
+        solver._check(self.L.nuppn_serve_open(solver.h, int(slots), int(queue), C.byref(h)))
         self.h = h
 
     def submit(self, X, t9_0, t9_1, rho_0, rho_1, ye, dtwant, bd_state=0) -> int:
