@@ -269,7 +269,29 @@ nuppn_status nuppn_integrate_device(nuppn_net *net, int32_t nz, double *d_X, int
                                     int32_t *d_ierr, nuppn_zone_stats *d_stats, int32_t *d_bd_state,
                                     void *stream);
 
-/* The trajectory loop of tppnp (frames/tppnp/source/tppnp.F90:131-168), batched: every zone z follows
+/* integrate_network for zones of several networks in one launch: zone z uses nets[net_of_zone[z]]
+ * (all handles on one device, at most 16), with that network's knobs; X rows have ldx >= the largest
+ * nsp and zone z uses its first nsp entries. No counterpart routine in the reference, whose frames
+ * run one network per process (NNN in ppn_physics.input); this is the uneven-size batch in which
+ * zones of ~200-, ~1100- and ~2500-species networks advance together: one persistent launch of one
+ * zone per CTA, every CTA's workspace sized for the largest network, zones taken hottest first, so
+ * small and large systems share the GPU instead of running as separate waves. Other arguments and
+ * outputs as for nuppn_integrate; a zone whose network index is out of range gets NUPPN_BAD_INPUT
+ * (the host-buffer form rejects the call instead). */
+nuppn_status nuppn_integrate_multi(nuppn_net *const *nets, int32_t nnets, int32_t nz, const int32_t *net_of_zone,
+                                   double *X, int32_t ldx, const double *t9_0, const double *t9_1,
+                                   const double *rho_0, const double *rho_1, double *ye, const double *dtwant,
+                                   int32_t *ierr, nuppn_zone_stats *stats, int32_t *bd_state);
+
+/* Same on device-resident buffers (d_net_of_zone included), asynchronous on the given stream. */
+nuppn_status nuppn_integrate_multi_device(nuppn_net *const *nets, int32_t nnets, int32_t nz,
+                                          const int32_t *d_net_of_zone, double *d_X, int32_t ldx,
+                                          const double *d_t9_0, const double *d_t9_1, const double *d_rho_0,
+                                          const double *d_rho_1, double *d_ye, const double *d_dtwant,
+                                          int32_t *d_ierr, nuppn_zone_stats *d_stats, int32_t *d_bd_state,
+                                          void *stream);
+
+/* The trajectory loop of tppnp/* The trajectory loop of tppnp (frames/tppnp/source/tppnp.F90:131-168), batched: every zone z follows
  * its own trajectory of npts points time[z*npts + i], t9[...], rho[...]. The starting composition is
  * renormalised (Kahan sum) if |1 - sum X| > 1e-8; then for each interval i: Ye from the composition
  * (calculate_ye), integrate_network from point i to i+1, stop at the first interval with a non-zero

@@ -39,6 +39,10 @@ cudaError_t launch_integrate(const DevNet &N, const WsLayout &L, char *ws, int g
 cudaError_t configure_kernels(int dyn_smem);
 cudaError_t occupancy_integrate(int block, int act_smem, int *per_sm);
 }  // namespace warp
+namespace cta {
+cudaError_t launch_integrate_multi(const IntegrateArgs &A, char *ws, int grid, int act_smem, cudaStream_t st);
+cudaError_t occupancy_integrate_multi(int act_smem, int *per_sm);
+}  // namespace cta
 using cta::launch_phase;
 using cta::launch_zone_order;
 }  // namespace nuppn
@@ -83,6 +87,8 @@ struct nuppn_net {
   size_t arena_bytes = 0;
   WsLayout L;
   DevBuf ws, stage, counter, order;  // order: the zone schedule of the allocating entry points
+  DevBuf multi;                      // networks' DevNet and WsLayout for nuppn_integrate_multi_device
+  char *multi_host = nullptr;        // their pinned staging
   int ws_slots = 0;
   // integration kernel: one zone per CTA of `block` threads (warp_zones = 0), or one zone per warp
   // with `block` / 32 zones per CTA (warp_zones = 1); act_smem = shared memory of each zone's group
@@ -453,6 +459,8 @@ nuppn_status nuppn_net_destroy(nuppn_net *net) {
   net->stage.release();
   net->counter.release();
   net->order.release();
+  net->multi.release();
+  if (net->multi_host) cudaFreeHost(net->multi_host);
   delete net;
   return NUPPN_OK;
 }
@@ -865,6 +873,116 @@ nuppn_status nuppn_autotune(nuppn_net *net, int32_t nz, const double *X, int32_t
     if (nreport) *nreport = k;
   }
   return out;
+}
+
+// ---- several networks in one launch ------------------------------------------------------------
+constexpr int kMaxMultiNets = 16;
+
+nuppn_status nuppn_integrate_multi_device(nuppn_net *const *nets, int32_t nnets, int32_t nz, const int32_t *d_net_of,
+                                          double *d_X, int32_t ldx, const double *d_t9_0, const double *d_t9_1,
+                                          const double *d_rho_0, const double *d_rho_1, double *d_ye,
+                                          const double *d_dtwant, int32_t *d_ierr, nuppn_zone_stats *d_stats,
+                                          int32_t *d_bd_state, void *stream) {
+  if (!nets || nnets < 1 || nnets > kMaxMultiNets) {
+    set_error("nnets must be 1.." + std::to_string(kMaxMultiNets));
+    return NUPPN_ERR_ARG;
+  }
+  nuppn_net *net = nets[0];
+  size_t slab = 0;
+  int nsp_max = 0;
+  for (int i = 0; i < nnets; ++i) {
+    if (!nets[i]) { set_error("null network handle"); return NUPPN_ERR_ARG; }
+    if (nets[i]->device != net->device) { set_error("the networks are on different devices"); return NUPPN_ERR_ARG; }
+    slab = std::max(slab, nets[i]->L.bytes);
+    nsp_max = std::max(nsp_max, nets[i]->H.nsp);
+  }
+  if (nz < 0) { set_error("nz < 0"); return NUPPN_ERR_ARG; }
+  if (ldx < nsp_max) { set_error("ldx < the largest network's nsp"); return NUPPN_ERR_ARG; }
+  if (nz == 0) return NUPPN_OK;
+  if (!d_net_of || !d_X || !d_t9_0 || !d_t9_1 || !d_rho_0 || !d_rho_1 || !d_ye || !d_dtwant || !d_ierr) {
+    set_error("null device argument");
+    return NUPPN_ERR_ARG;
+  }
+  CK(cudaSetDevice(net->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  // one zone per CTA of 256 threads, 72 KB of shared memory each (3 CTAs per SM)
+  const int act_smem = 72 * 1024;
+  CK(cta::configure_kernels(std::max(act_smem, net->phase_smem)));
+  int per = 0;
+  if (cta::occupancy_integrate_multi(act_smem, &per) != cudaSuccess || per <= 0) per = 1;
+  const int grid = std::min(nz, per * net->nsm);
+  CK(net->ws.ensure((size_t)grid * slab));
+  net->ws_slots = (int)(net->ws.n / std::max<size_t>(net->L.bytes, 1));
+  const size_t desc = a16(sizeof(DevNet)) * kMaxMultiNets, lay = a16(sizeof(WsLayout)) * kMaxMultiNets;
+  CK(net->multi.ensure(desc + lay));
+  if (!net->multi_host) CK(cudaHostAlloc((void **)&net->multi_host, desc + lay, cudaHostAllocPortable));
+  CK(cudaStreamSynchronize(s));  // the staging buffer may still feed the previous call's copy
+  DevNet *hn = (DevNet *)net->multi_host;
+  WsLayout *hl = (WsLayout *)(net->multi_host + desc);
+  for (int i = 0; i < nnets; ++i) { hn[i] = nets[i]->D; hl[i] = nets[i]->L; }
+  CK(cudaMemcpyAsync(net->multi.p, net->multi_host, desc + lay, cudaMemcpyHostToDevice, s));
+  CK(net->order.ensure((size_t)nz * 4));
+  CK(cudaMemsetAsync(net->counter.p, 0, sizeof(int), s));
+  CK(launch_zone_order(d_t9_0, d_t9_1, 1, nz, (int *)net->order.p, s));
+  IntegrateArgs A = {};
+  A.nz = nz; A.ldx = ldx; A.X = d_X; A.t9_0 = d_t9_0; A.t9_1 = d_t9_1; A.rho_0 = d_rho_0; A.rho_1 = d_rho_1;
+  A.dtwant = d_dtwant; A.ye = d_ye; A.ierr = d_ierr; A.stats = d_stats; A.bd_state = d_bd_state;
+  A.counter = (int *)net->counter.p;
+  A.order = (const int *)net->order.p;
+  A.nets = (const DevNet *)net->multi.p;
+  A.lays = (const WsLayout *)((char *)net->multi.p + desc);
+  A.net_of = d_net_of;
+  A.nnets = nnets;
+  A.slab = slab;
+  CK(cta::launch_integrate_multi(A, (char *)net->ws.p, grid, act_smem, s));
+  net->launches += 2;  // k_zone_order, k_integrate_multi
+  return NUPPN_OK;
+}
+
+nuppn_status nuppn_integrate_multi(nuppn_net *const *nets, int32_t nnets, int32_t nz, const int32_t *net_of, double *X,
+                                   int32_t ldx, const double *t9_0, const double *t9_1, const double *rho_0,
+                                   const double *rho_1, double *ye, const double *dtwant, int32_t *ierr,
+                                   nuppn_zone_stats *stats, int32_t *bd_state) {
+  if (!nets || nnets < 1 || nnets > kMaxMultiNets || !nets[0]) { set_error("bad network list"); return NUPPN_ERR_ARG; }
+  if (nz < 0) { set_error("nz < 0"); return NUPPN_ERR_ARG; }
+  if (nz == 0) return NUPPN_OK;
+  if (!net_of || !X || !t9_0 || !t9_1 || !rho_0 || !rho_1 || !ye || !dtwant || !ierr) {
+    set_error("null argument");
+    return NUPPN_ERR_ARG;
+  }
+  for (int z = 0; z < nz; ++z)
+    if (net_of[z] < 0 || net_of[z] >= nnets) { set_error("net_of[" + std::to_string(z) + "] out of range"); return NUPPN_ERR_ARG; }
+  nuppn_net *net = nets[0];
+  CK(cudaSetDevice(net->device));
+  Stager S;
+  size_t oX = S.add((size_t)nz * ldx * 8), o1 = S.add(nz * 8), o2 = S.add(nz * 8), o3 = S.add(nz * 8);
+  size_t o4 = S.add(nz * 8), o5 = S.add(nz * 8), o6 = S.add(nz * 8), oi = S.add(nz * 4), on = S.add(nz * 4);
+  size_t os = S.add((size_t)nz * sizeof(nuppn_zone_stats)), ob = S.add(nz * 4);
+  CK(net->stage.ensure(S.total));
+  char *sb = (char *)net->stage.p;
+  CK(cudaMemcpy(sb + oX, X, (size_t)nz * ldx * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + o1, t9_0, nz * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + o2, t9_1, nz * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + o3, rho_0, nz * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + o4, rho_1, nz * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + o5, ye, nz * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + o6, dtwant, nz * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sb + on, net_of, nz * 4, cudaMemcpyHostToDevice));
+  if (bd_state) CK(cudaMemcpy(sb + ob, bd_state, nz * 4, cudaMemcpyHostToDevice));
+  else CK(cudaMemset(sb + ob, 0, nz * 4));
+  nuppn_status st = nuppn_integrate_multi_device(nets, nnets, nz, (const int *)(sb + on), (double *)(sb + oX), ldx,
+                                                 (double *)(sb + o1), (double *)(sb + o2), (double *)(sb + o3),
+                                                 (double *)(sb + o4), (double *)(sb + o5), (double *)(sb + o6),
+                                                 (int *)(sb + oi), (nuppn_zone_stats *)(sb + os), (int *)(sb + ob),
+                                                 nullptr);
+  if (st != NUPPN_OK) return st;
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(X, sb + oX, (size_t)nz * ldx * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ye, sb + o5, nz * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ierr, sb + oi, nz * 4, cudaMemcpyDeviceToHost));
+  if (stats) CK(cudaMemcpy(stats, sb + os, (size_t)nz * sizeof(nuppn_zone_stats), cudaMemcpyDeviceToHost));
+  if (bd_state) CK(cudaMemcpy(bd_state, sb + ob, nz * 4, cudaMemcpyDeviceToHost));
+  return NUPPN_OK;
 }
 
 nuppn_status nuppn_integrate_trajectories_device(nuppn_net *net, int32_t nz, int32_t npts, double *d_X, int32_t ldx,

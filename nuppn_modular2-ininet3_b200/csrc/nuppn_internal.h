@@ -206,6 +206,12 @@ struct IntegrateArgs {
   // serving (queue.in != nullptr, trajectory instantiation): requests come from the queue instead of
   // the arrays above, each a single interval or a trajectory
   ServeQueue queue;
+  // several networks in one launch (k_integrate_multi): zone z uses nets[net_of[z]], lays[net_of[z]]
+  const DevNet *nets;
+  const WsLayout *lays;
+  const int *net_of;
+  int nnets;
+  size_t slab;                   // bytes of each CTA's workspace slab
 };
 
 // arguments of the single-phase parity kernel

@@ -597,6 +597,109 @@ __device__ long long queue_claim(const ServeQueue &Q) {
 // kTraj: tppnp's trajectory loop per zone (IntegrateArgs::npts > 0); a separate instantiation so the
 // single-interval kernel keeps its own register allocation. The trajectory instantiation also runs
 // the serving loop (IntegrateArgs::queue), whose requests are single intervals or trajectories.
+// One zone (or one served request) for the calling group: inputs from the arrays of A indexed by
+// zone zq, or from the serving queue's slot of request zq; integrate; write the outputs back.
+template <bool kTraj>
+__device__ __forceinline__ void run_zone(const DevNet &N, const Ws &W, const IntegrateArgs &A, bool queue,
+                                         long long zq, char *smem, int act_smem, double *sred, int *sint) {
+  const ServeQueue &Q = A.queue;
+  // the zone's inputs: arrays indexed by zone, or a queue slot (rewritten by copies between
+  // requests, so read around L1)
+  int z = 0, slot = 0, kind = kTraj ? 1 : 0, npts = A.npts, st = 0;
+  double t9_0 = 0, t9_1 = 0, rho_0 = 0, rho_1 = 0, ye = 0, dtwant = 0;
+  const double *tt = nullptr, *tp = nullptr, *tr = nullptr;
+  bool seq_ok = true;
+  if (queue) {
+    slot = (int)(zq % Q.nslots);
+    const RingIn *in = Q.in + slot;
+    for (int it = 0; __ldcg(&in->seq) != zq; ++it)
+      if (it > kSpinLimit) { seq_ok = false; break; }
+    kind = __ldcg(&in->kind);
+    npts = __ldcg(&in->npts);
+    st = __ldcg(&in->bd);
+    t9_0 = __ldcg(&in->t9_0); t9_1 = __ldcg(&in->t9_1);
+    rho_0 = __ldcg(&in->rho_0); rho_1 = __ldcg(&in->rho_1);
+    ye = __ldcg(&in->ye); dtwant = __ldcg(&in->dtwant);
+    const double *g = Q.grid + (size_t)slot * 3 * Q.npts_max;
+    tt = g; tp = g + Q.npts_max; tr = g + 2 * Q.npts_max;
+    const double *x = Q.x_in + (size_t)slot * N.nsp;
+    for (int s = GT; s < N.nsp; s += GN) W.y[s] = __ldcg(x + s);
+  } else {
+    z = (int)zq;
+    st = A.bd_state ? A.bd_state[z] : 0;
+    ye = A.ye[z];
+    if (kTraj) {
+      tt = A.tr_time + (size_t)z * A.npts; tp = A.tr_t9 + (size_t)z * A.npts; tr = A.tr_rho + (size_t)z * A.npts;
+    } else {
+      t9_0 = A.t9_0[z]; t9_1 = A.t9_1[z]; rho_0 = A.rho_0[z]; rho_1 = A.rho_1[z]; dtwant = A.dtwant[z];
+    }
+    for (int s = GT; s < N.nsp; s += GN) W.y[s] = A.X[(size_t)z * A.ldx + s];
+  }
+  GSYNC();
+  ZoneCtl C;
+  memset(&C.st, 0, sizeof(C.st));
+  C.kopt = (st >= 2 && st <= N.kmax) ? st : N.kopt0;
+  C.reduce = false;
+  C.sumerr = 0.0;
+  C.smem = smem;
+  C.smem_bytes = act_smem;
+  C.sint = sint;
+  nse_reset(C.nse);
+  int ierr, fail = -1;
+  if (!seq_ok) {
+    ierr = NUPPN_BAD_INPUT;
+  } else if (kTraj && kind == 1) {
+    // the trajectory loop of tppnp (tppnp.F90:131-168) for this zone
+    if (fabs(1.0 - vsum(W.y, N.nsp, sred)) > 1.e-8) dev_renorm_ksum(W.y, N.nsp, sred);
+    bool frst = st <= 0;
+    ierr = 0;
+    for (int i = 1; i < npts; ++i) {
+      ye = dev_ye(N, W.y, sred);
+      ierr = dev_integrate_zone(N, W, C, __ldcg(tp + i - 1), __ldcg(tp + i), __ldcg(tr + i - 1), __ldcg(tr + i), ye,
+                                __ldcg(tt + i) - __ldcg(tt + i - 1), frst, sred);
+      frst = false;
+      if (ierr != 0) {
+        fail = i - 1;
+        break;
+      }
+      if (fabs(1.0 - vsum(W.y, N.nsp, sred)) > 5.e-7) dev_renorm_ksum(W.y, N.nsp, sred);
+    }
+  } else {
+    ierr = dev_integrate_zone(N, W, C, t9_0, t9_1, rho_0, rho_1, ye, dtwant, st <= 0, sred);
+  }
+  if (queue) {
+    // results to host-mapped memory, made visible to the host before `done`
+    double *xo = Q.x_out + (size_t)slot * N.nsp;
+    for (int s = GT; s < N.nsp; s += GN) xo[s] = W.y[s];
+    RingOut *o = Q.out + slot;
+    if (GT == 0) {
+      o->ierr = ierr;
+      o->fail = fail;
+      o->bd = C.kopt;
+      o->ye = ye;
+      o->st = C.st;
+    }
+    __threadfence_system();
+    GSYNC();
+    if (GT == 0) *(volatile long long *)&o->done = zq + 1;
+    return;
+  }
+  for (int s = GT; s < N.nsp; s += GN) A.X[(size_t)z * A.ldx + s] = W.y[s];
+  if (GT == 0) {
+    A.ye[z] = ye;
+    A.ierr[z] = ierr;
+    if (A.stats) A.stats[z] = C.st;
+    if (A.bd_state) A.bd_state[z] = C.kopt;
+    if (A.tr_fail) A.tr_fail[z] = fail;
+  }
+}
+
+// One zone per group: a CTA of the cta variant (3 resident per SM), a warp of the warp variant (8
+// per CTA, one CTA per SM: the groups' shares of shared memory set the residency). Each group owns
+// workspace slab blockIdx.x * groups + GID and act_smem bytes of the dynamic shared memory.
+// kTraj: tppnp's trajectory loop per zone (IntegrateArgs::npts > 0); a separate instantiation so the
+// single-interval kernel keeps its own register allocation. The trajectory instantiation also runs
+// the serving loop (IntegrateArgs::queue), whose requests are single intervals or trajectories.
 template <bool kTraj>
 __global__ void NUPPN_INTEGRATE_BOUNDS k_integrate(const __grid_constant__ DevNet N, const __grid_constant__ WsLayout L,
                                                    char *ws, const __grid_constant__ IntegrateArgs A, int act_smem) {
@@ -610,12 +713,11 @@ __global__ void NUPPN_INTEGRATE_BOUNDS k_integrate(const __grid_constant__ DevNe
   const int groups = (int)blockDim.x / GN;
   const Ws W = ws_bind(ws + ((size_t)blockIdx.x * groups + GID) * L.bytes, L);
   const bool queue = kTraj && A.queue.in != nullptr;
-  const ServeQueue &Q = A.queue;
   for (;;) {
     GSYNC();
     if (GT == 0) {
       if (queue) {
-        zsh = queue_claim(Q);
+        zsh = queue_claim(A.queue);
       } else {
         const int k = atomicAdd(A.counter, 1);
         zsh = (k < A.nz && A.order) ? A.order[k] : k;
@@ -624,97 +726,51 @@ __global__ void NUPPN_INTEGRATE_BOUNDS k_integrate(const __grid_constant__ DevNe
     GSYNC();
     const long long zq = zsh;
     if (queue ? zq < 0 : zq >= A.nz) break;
-    // the zone's inputs: arrays indexed by zone, or a queue slot (rewritten by copies between
-    // requests, so read around L1)
-    int z = 0, slot = 0, kind = kTraj ? 1 : 0, npts = A.npts, st = 0;
-    double t9_0 = 0, t9_1 = 0, rho_0 = 0, rho_1 = 0, ye = 0, dtwant = 0;
-    const double *tt = nullptr, *tp = nullptr, *tr = nullptr;
-    bool seq_ok = true;
-    if (queue) {
-      slot = (int)(zq % Q.nslots);
-      const RingIn *in = Q.in + slot;
-      for (int it = 0; __ldcg(&in->seq) != zq; ++it)
-        if (it > kSpinLimit) { seq_ok = false; break; }
-      kind = __ldcg(&in->kind);
-      npts = __ldcg(&in->npts);
-      st = __ldcg(&in->bd);
-      t9_0 = __ldcg(&in->t9_0); t9_1 = __ldcg(&in->t9_1);
-      rho_0 = __ldcg(&in->rho_0); rho_1 = __ldcg(&in->rho_1);
-      ye = __ldcg(&in->ye); dtwant = __ldcg(&in->dtwant);
-      const double *g = Q.grid + (size_t)slot * 3 * Q.npts_max;
-      tt = g; tp = g + Q.npts_max; tr = g + 2 * Q.npts_max;
-      const double *x = Q.x_in + (size_t)slot * N.nsp;
-      for (int s = GT; s < N.nsp; s += GN) W.y[s] = __ldcg(x + s);
-    } else {
-      z = (int)zq;
-      st = A.bd_state ? A.bd_state[z] : 0;
-      ye = A.ye[z];
-      if (kTraj) {
-        tt = A.tr_time + (size_t)z * A.npts; tp = A.tr_t9 + (size_t)z * A.npts; tr = A.tr_rho + (size_t)z * A.npts;
-      } else {
-        t9_0 = A.t9_0[z]; t9_1 = A.t9_1[z]; rho_0 = A.rho_0[z]; rho_1 = A.rho_1[z]; dtwant = A.dtwant[z];
-      }
-      for (int s = GT; s < N.nsp; s += GN) W.y[s] = A.X[(size_t)z * A.ldx + s];
-    }
-    GSYNC();
-    ZoneCtl C;
-    memset(&C.st, 0, sizeof(C.st));
-    C.kopt = (st >= 2 && st <= N.kmax) ? st : N.kopt0;
-    C.reduce = false;
-    C.sumerr = 0.0;
-    C.smem = smem_dyn + (size_t)GID * act_smem;
-    C.smem_bytes = act_smem;
-    C.sint = sint;
-    nse_reset(C.nse);
-    int ierr, fail = -1;
-    if (!seq_ok) {
-      ierr = NUPPN_BAD_INPUT;
-    } else if (kTraj && kind == 1) {
-      // the trajectory loop of tppnp (tppnp.F90:131-168) for this zone
-      if (fabs(1.0 - vsum(W.y, N.nsp, sred)) > 1.e-8) dev_renorm_ksum(W.y, N.nsp, sred);
-      bool frst = st <= 0;
-      ierr = 0;
-      for (int i = 1; i < npts; ++i) {
-        ye = dev_ye(N, W.y, sred);
-        ierr = dev_integrate_zone(N, W, C, __ldcg(tp + i - 1), __ldcg(tp + i), __ldcg(tr + i - 1), __ldcg(tr + i), ye,
-                                  __ldcg(tt + i) - __ldcg(tt + i - 1), frst, sred);
-        frst = false;
-        if (ierr != 0) {
-          fail = i - 1;
-          break;
-        }
-        if (fabs(1.0 - vsum(W.y, N.nsp, sred)) > 5.e-7) dev_renorm_ksum(W.y, N.nsp, sred);
-      }
-    } else {
-      ierr = dev_integrate_zone(N, W, C, t9_0, t9_1, rho_0, rho_1, ye, dtwant, st <= 0, sred);
-    }
-    if (queue) {
-      // results to host-mapped memory, made visible to the host before `done`
-      double *xo = Q.x_out + (size_t)slot * N.nsp;
-      for (int s = GT; s < N.nsp; s += GN) xo[s] = W.y[s];
-      RingOut *o = Q.out + slot;
-      if (GT == 0) {
-        o->ierr = ierr;
-        o->fail = fail;
-        o->bd = C.kopt;
-        o->ye = ye;
-        o->st = C.st;
-      }
-      __threadfence_system();
-      GSYNC();
-      if (GT == 0) *(volatile long long *)&o->done = zq + 1;
-      continue;
-    }
-    for (int s = GT; s < N.nsp; s += GN) A.X[(size_t)z * A.ldx + s] = W.y[s];
-    if (GT == 0) {
-      A.ye[z] = ye;
-      A.ierr[z] = ierr;
-      if (A.stats) A.stats[z] = C.st;
-      if (A.bd_state) A.bd_state[z] = C.kopt;
-      if (A.tr_fail) A.tr_fail[z] = fail;
-    }
+    run_zone<kTraj>(N, W, A, queue, zq, smem_dyn + (size_t)GID * act_smem, act_smem, sred, sint);
   }
 }
+
+#if !NUPPN_GROUP_WARP
+// Zones of several networks in one launch (one zone per CTA): zone z uses network A.net_of[z], whose
+// DevNet and workspace layout the CTA copies from A.nets / A.lays into shared memory when it takes
+// the zone; every CTA's slab is A.slab bytes, the largest of the networks' slabs.
+__global__ void __launch_bounds__(256, 3) k_integrate_multi(const __grid_constant__ IntegrateArgs A, char *ws,
+                                                            int act_smem) {
+  extern __shared__ __align__(16) char smem_dyn[];
+  __shared__ double sred[32];
+  __shared__ int sint[32];
+  __shared__ long long zsh;
+  __shared__ __align__(16) DevNet sN;
+  __shared__ __align__(16) WsLayout sL;
+  char *slab = ws + (size_t)blockIdx.x * A.slab;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int k = atomicAdd(A.counter, 1);
+      zsh = (k < A.nz && A.order) ? A.order[k] : k;
+    }
+    __syncthreads();
+    const long long zq = zsh;
+    if (zq >= A.nz) break;
+    const int nid = A.net_of[zq];
+    if (nid < 0 || nid >= A.nnets) {  // no such network: the zone is left as it is
+      if (threadIdx.x == 0) A.ierr[zq] = NUPPN_BAD_INPUT;
+      continue;
+    }
+    {  // the zone's network description (8-byte words; both structs are 8-byte aligned)
+      const unsigned long long *src = (const unsigned long long *)(A.nets + nid);
+      unsigned long long *dst = (unsigned long long *)&sN;
+      for (int i = threadIdx.x; i < (int)(sizeof(DevNet) / 8); i += blockDim.x) dst[i] = src[i];
+      const unsigned long long *srl = (const unsigned long long *)(A.lays + nid);
+      unsigned long long *dl = (unsigned long long *)&sL;
+      for (int i = threadIdx.x; i < (int)(sizeof(WsLayout) / 8); i += blockDim.x) dl[i] = srl[i];
+    }
+    __syncthreads();
+    const Ws W = ws_bind(slab, sL);
+    run_zone<false>(sN, W, A, false, zq, smem_dyn, act_smem, sred, sint);
+  }
+}
+#endif
 
 #if !NUPPN_GROUP_WARP
 __global__ void __launch_bounds__(256) k_phase(const __grid_constant__ DevNet N, const __grid_constant__ WsLayout L,
@@ -830,6 +886,15 @@ cudaError_t launch_integrate(const DevNet &N, const WsLayout &L, char *ws, int g
 }
 
 #if !NUPPN_GROUP_WARP
+cudaError_t launch_integrate_multi(const IntegrateArgs &A, char *ws, int grid, int act_smem, cudaStream_t st) {
+  k_integrate_multi<<<grid, 256, act_smem, st>>>(A, ws, act_smem);
+  return cudaGetLastError();
+}
+
+cudaError_t occupancy_integrate_multi(int act_smem, int *per_sm) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_integrate_multi, 256, act_smem);
+}
+
 cudaError_t launch_phase(const DevNet &N, const WsLayout &L, char *ws, int grid, int block, int act_smem,
                          const PhaseArgs &A, cudaStream_t st) {
   k_phase<<<grid, block, act_smem, st>>>(N, L, ws, A, act_smem);
@@ -845,6 +910,8 @@ cudaError_t configure_kernels(int dyn_smem) {
 #if !NUPPN_GROUP_WARP
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_phase, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_smem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_integrate_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_smem);
 #endif
   return e;
 }

@@ -54,6 +54,8 @@ def load_library():
     L.nuppn_integrate.argtypes = [vp, i32, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.nuppn_integrate_device.argtypes = [vp, i32, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.nuppn_autotune.argtypes = [vp, i32, vp, i32, vp, vp, vp, vp, vp, vp, i32, vp, i32, vp]
+    L.nuppn_integrate_multi.argtypes = [vp, i32, i32, vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.nuppn_integrate_multi_device.argtypes = [vp, i32, i32, vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.nuppn_launch_count.argtypes = [vp]
     L.nuppn_launch_count.restype = i64
     L.nuppn_nse.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp]
@@ -71,7 +73,8 @@ def load_library():
                  "nuppn_solve_reduced", "nuppn_integrate", "nuppn_integrate_device", "nuppn_nse",
                  "nuppn_integrate_trajectories", "nuppn_integrate_trajectories_device",
                  "nuppn_serve_open", "nuppn_serve_submit", "nuppn_serve_submit_trajectory", "nuppn_serve_poll",
-                 "nuppn_serve_info", "nuppn_serve_close", "nuppn_autotune"):
+                 "nuppn_serve_info", "nuppn_serve_close", "nuppn_autotune", "nuppn_integrate_multi",
+                 "nuppn_integrate_multi_device"):
         getattr(L, name).restype = i32
     _LIB = L
     return L
@@ -254,6 +257,42 @@ class NetworkSolver:
         self._check(self.L.nuppn_integrate_device(
             self.h, X.shape[0], ptr(X), X.shape[1], ptr(t9_0), ptr(t9_1), ptr(rho_0), ptr(rho_1), ptr(ye),
             ptr(dtwant), ptr(ierr), ptr(stats), ptr(bd_state), C.c_void_p(stream)))
+
+
+def _handles(solvers):
+    arr = (C.c_void_p * len(solvers))(*[s.h.value for s in solvers])
+    return arr
+
+
+def integrate_multi(solvers, net_of, X, t9_0, t9_1, rho_0, rho_1, ye, dtwant, bd_state=None):
+    """nuppn_integrate_multi: zones of several networks (solvers[net_of[z]]) in one launch. X rows have
+    the largest network's nsp entries (zone z uses the first nsp of its own). Returns (X, ye, ierr,
+    stats, bd_state); X is not modified."""
+    X = np.array(np.atleast_2d(X), dtype=np.float64, order="C", copy=True)
+    nz = X.shape[0]
+    net_of = np.ascontiguousarray(net_of, dtype=np.int32)
+    t9_0, t9_1, rho_0, rho_1 = _f64(t9_0, nz), _f64(t9_1, nz), _f64(rho_0, nz), _f64(rho_1, nz)
+    ye = np.array(_f64(ye, nz), copy=True)
+    dtwant = _f64(dtwant, nz)
+    ierr = np.zeros(nz, np.int32)
+    stats = (abi.ZoneStats * nz)()
+    bd = np.zeros(nz, np.int32) if bd_state is None else np.array(bd_state, dtype=np.int32, copy=True)
+    s0 = solvers[0]
+    s0._check(s0.L.nuppn_integrate_multi(_handles(solvers), len(solvers), nz, _p(net_of), _p(X), X.shape[1],
+                                         _p(t9_0), _p(t9_1), _p(rho_0), _p(rho_1), _p(ye), _p(dtwant), _p(ierr),
+                                         stats, _p(bd)))
+    return X, ye, ierr, stats, bd
+
+
+def integrate_multi_device(solvers, net_of, X, t9_0, t9_1, rho_0, rho_1, ye, dtwant, ierr, stats=None,
+                           bd_state=None, stream=0):
+    """Device-resident form of integrate_multi: torch CUDA tensors (or objects with data_ptr())."""
+    ptr = lambda t: None if t is None else C.c_void_p(t.data_ptr())
+    s0 = solvers[0]
+    s0._check(s0.L.nuppn_integrate_multi_device(
+        _handles(solvers), len(solvers), int(X.shape[0]), ptr(net_of), ptr(X), int(X.shape[1]), ptr(t9_0),
+        ptr(t9_1), ptr(rho_0), ptr(rho_1), ptr(ye), ptr(dtwant), ptr(ierr), ptr(stats), ptr(bd_state),
+        C.c_void_p(stream)))
 
 
 class Server:

@@ -212,10 +212,28 @@ _VITAL_SPECIES = [(0, 1), (1, 1), (1, 2), (2, 3), (2, 4), (4, 7), (5, 8), (3, 7)
                   (4, 8), (-1, 0)]          # (-1, 0) marks the gamma slot OOOOO
 
 
-def build_network(nnn: int = 1107, seed: int = 20240611, name: str | None = None) -> Network:
-    """Build a synthetic network with ``nnn`` isotope-database entries (the reference's NNN)."""
+def database_isotopes(database: str, nnn: int):
+    """(Z, A) of the network isotopes that networkI (``ppn_physics.F90:40-130``) takes from the first
+    ``nnn`` lines of the reference's isotope database ``database`` (``"isotopedatabase"``, 1107
+    entries, or ``"isotopedatabase_all"``, 5234): the entries flagged T, in file order. (networkI also
+    drops isotopes whose NETGEN beta or EC rate at the set-up T9/rho beats ln 2 / tbetamin; that
+    needs the real NETGEN tables and is not applied here.) The tables come from
+    data/isotope_databases.npz, written by data/make_isotope_tables.py with the library's reader."""
+    import os
+    t = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "isotope_databases.npz"))
+    z, a, f = t[database + "_z"], t[database + "_a"], t[database + "_flag"]
+    if nnn > z.size:
+        raise ValueError(f"{database} has {z.size} entries, fewer than nnn = {nnn}")
+    return [(int(z[i]), int(a[i])) for i in range(nnn) if f[i]]
+
+
+def build_network(nnn: int = 1107, seed: int = 20240611, name: str | None = None,
+                  database: str | None = None) -> Network:
+    """Build a synthetic network with ``nnn`` isotope-database entries (the reference's NNN). With
+    ``database`` the isotopes are the reference database's (database_isotopes), else a synthetic band
+    around the valley of stability in the same Z-then-A order."""
     rng = np.random.default_rng(seed)
-    isos = _isotope_list(nnn)
+    isos = database_isotopes(database, nnn) if database else _isotope_list(nnn)
 
     # ---- species -------------------------------------------------------------------------
     zis, A, Z = [], [], []
@@ -518,7 +536,7 @@ def build_network(nnn: int = 1107, seed: int = 20240611, name: str | None = None
         ng_l10v[:, i, :ndat] = tab
 
     return Network(
-        name=name or f"synth{nnn}", zis=zis, anetw=A, znetw=Z, considerisotope=considerisotope,
+        name=name or (f"{database}{nnn}" if database else f"synth{nnn}"), zis=zis, anetw=A, znetw=Z, considerisotope=considerisotope,
         exmass=exmass, gspin=gspin, spec_part=spec_part, k=K, ilabb=ILABB,
         considerreaction=CONS, rfac=np.ones(nre), src=SRC, src_idx=SIDX, irev=irev,
         nvcp=nvcp, nrcp=nrcp, igamma=igamma,

@@ -46,10 +46,10 @@ def _ye_of(net: sn.Network, X: np.ndarray) -> np.ndarray:
 _NETS: dict = {}
 
 
-def network(nnn: int, seed: int = 20240611) -> sn.Network:
-    key = (nnn, seed)
+def network(nnn: int, seed: int = 20240611, database: str | None = None) -> sn.Network:
+    key = (nnn, seed, database)
     if key not in _NETS:
-        _NETS[key] = sn.build_network(nnn, seed)
+        _NETS[key] = sn.build_network(nnn, seed, database=database)
     return _NETS[key]
 
 
@@ -157,3 +157,36 @@ def hburn_zone(net: sn.Network | None = None) -> tuple[ZoneBatch, np.ndarray]:
     zb = ZoneBatch(X=X, t9_0=np.array([0.020]), t9_1=np.array([0.020]), rho_0=np.array([100.0]),
                    rho_1=np.array([100.0]), ye=_ye_of(net, X), dtwant=np.array([dts[0]]))
     return zb, dts
+
+
+def mixed_networks():
+    """The three networks of the uneven-size batch: ~200 species (the Z <= 30 part of the reference's
+    isotopedatabase.txt, its first 201 lines), the ~1100-species network of the He-shell batch, and
+    ~2500 species (the first 2500 lines of isotopedatabase_all.txt)."""
+    return network(201, database="isotopedatabase"), network(1107), network(2500, database="isotopedatabase_all")
+
+
+def mixed_batch(nz: int, seed: int = 4, dtwant: float = 1.0e10):
+    """Uneven-size batch: 40 % H-burning zones on the ~200-species network (T9 U[0.015, 0.08], rho
+    log-U[1, 1e3], X(H1) = 0.70, X(He4) = 0.28, Z = 0.02 over the stable species), 50 % He-shell
+    zones on the ~1100-species network (as heshell_batch), 10 % zones on the ~2500-species network
+    (T9 U[0.3, 1.0], rho log-U[1e4, 1e6], the He-shell composition), each one integrate_network call
+    of dtwant. Returns (networks, [(network index, ZoneBatch)]), the zones of each network together,
+    and the network index of every zone in batch order."""
+    nets = mixed_networks()
+    rng = np.random.default_rng(seed)
+    counts = [int(round(0.4 * nz)), 0, int(round(0.1 * nz))]
+    counts[1] = nz - counts[0] - counts[2]
+    hb, _ = hburn_zone(nets[0])
+    X0 = np.repeat(hb.X, counts[0], axis=0)
+    t9 = rng.uniform(0.015, 0.08, counts[0])
+    rho = 10.0 ** rng.uniform(0.0, 3.0, counts[0])
+    small = ZoneBatch(X=X0, t9_0=t9.copy(), t9_1=t9.copy(), rho_0=rho.copy(), rho_1=rho.copy(),
+                      ye=_ye_of(nets[0], X0), dtwant=np.full(counts[0], dtwant))
+    mid = heshell_batch(counts[1], net=nets[1], seed=seed + 1, dtwant=dtwant)
+    big = heshell_batch(counts[2], net=nets[2], seed=seed + 2, dtwant=dtwant)
+    t9b = rng.uniform(0.3, 1.0, counts[2])
+    rhob = 10.0 ** rng.uniform(4.0, 6.0, counts[2])
+    big.t9_0[:], big.t9_1[:], big.rho_0[:], big.rho_1[:] = t9b, t9b, rhob, rhob
+    net_of = np.concatenate([np.full(c, i, np.int32) for i, c in enumerate(counts)])
+    return nets, [(0, small), (1, mid), (2, big)], net_of
