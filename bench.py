@@ -540,22 +540,164 @@ def run_serve(args, rank, world):
                       "gpu_launches": batched["loop_launches"], "clocks": batched["clocks"]}), flush=True)
 
 
+def run_mixed(args, rank, world):
+    """The uneven-size batch: 4096 zones (args.nz) of three networks in one launch
+    (nuppn_integrate_multi), 40 % H-burning zones on the ~200-species network, 50 % He-shell zones on
+    the ~1100-species network, 10 % hot zones on the ~2500-species network (workloads.mixed_batch),
+    one integrate_network call of 1e10 s each. A step is one call over the batch from the same state.
+    Beside the one-launch FP64 form (value) the line gives the same zones as three separate launches
+    (one per network, back to back on one stream) and the one-launch form with the FP32 factor and
+    FP64 refinement (lu_precision = 1)."""
+    if rank != 0:
+        return
+    wl = importlib.import_module(PKG + ".workloads")
+    abi = importlib.import_module(PKG + ".abi")
+    nets, parts, net_of = wl.mixed_batch(args.nz)
+    ldx = max(n.nsp for n in nets)
+    nz = args.nz
+    X0 = np.full((nz, ldx), 1e-99)
+    cols = {f: np.zeros(nz) for f in ("t9_0", "t9_1", "rho_0", "rho_1", "ye", "dtwant")}
+    z = 0
+    for i, zb in parts:
+        X0[z:z + zb.nz, :nets[i].nsp] = zb.X
+        for f in cols:
+            cols[f][z:z + zb.nz] = getattr(zb, f)
+        z += zb.nz
+    cfg = {"workload": "mixed networks: 40% hburn-200, 50% heshell-1107, 10% hot-2500, BD 1e10 s",
+           "zones": nz, "network_species": [int(n.nsp) for n in nets], "integrator": "bader-deuflhard",
+           "arithmetic": "fp64"}
+    if args.impl == "reference":
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        cores = os.cpu_count() or 1
+        take = {0: 16, 1: 16, 2: 8}  # a bounded sample: the 2500-species zones take seconds each
+        times, steps = [], []
+        for it in range(args.warmup + args.steps):
+            t, n = 0.0, 0
+            for i, zb in parts:
+                sub = zb.take(np.arange(min(take[i], zb.nz)))
+                ref = orc.Oracle(nets[i], abi.default_knobs(integration_method=1))
+                t0 = time.perf_counter()
+                _, _, _, st, _ = ref.integrate_network(sub.X, sub.t9_0, sub.t9_1, sub.rho_0, sub.rho_1, sub.ye,
+                                                       sub.dtwant, nthreads=cores)
+                t += time.perf_counter() - t0
+                n += sum(s.nsucc for s in st)
+            if it >= args.warmup:
+                times.append(t)
+                steps.append(n)
+        v = sum(steps) / sum(times)
+        print(json.dumps({"impl": "reference", "metric": "zone-timesteps/s", "value": v, "unit": "zone-timesteps/s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+                          "cpu_baseline": {"value": v, "unit": "zone-timesteps/s", "cores": cores, "kind": "port",
+                                           "sample": "16 + 16 + 8 zones of the three networks per step"},
+                          "e2e": {"value": v, "unit": "zone-timesteps/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import torch
+    solver = importlib.import_module(PKG + ".solver")
+    dev = torch.cuda.current_device()
+    cu = lambda a, dt=torch.float64: torch.tensor(np.ascontiguousarray(a), dtype=dt, device="cuda")
+    X0d = cu(X0)
+    d = {f: cu(v) for f, v in cols.items()}
+    nof = cu(net_of, torch.int32)
+    X = X0d.clone()
+    ye = d["ye"].clone()
+    ierr = torch.zeros(nz, dtype=torch.int32, device="cuda")
+    stats = torch.zeros((nz, 8), dtype=torch.int32, device="cuda")
+    bd = torch.zeros(nz, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    offs = np.concatenate([[0], np.cumsum([zb.nz for _, zb in parts])])
+
+    def form(lu_precision, one_launch):
+        sv = [solver.NetworkSolver(n, abi.default_knobs(integration_method=1, lu_precision=lu_precision), device=dev)
+              for n in nets]
+
+        def step():
+            X.copy_(X0d); ye.copy_(d["ye"]); bd.zero_()
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            if one_launch:
+                solver.integrate_multi_device(sv, nof, X, d["t9_0"], d["t9_1"], d["rho_0"], d["rho_1"], ye,
+                                              d["dtwant"], ierr, stats, bd, stream=stream)
+            else:
+                for i in range(3):
+                    a, b = int(offs[i]), int(offs[i + 1])
+                    sl = lambda t: t[a:b]
+                    sv[i].integrate_device(X[a:b], *(sl(d[f]) for f in ("t9_0", "t9_1", "rho_0", "rho_1")),
+                                           ye[a:b], d["dtwant"][a:b], ierr[a:b], stats[a:b], bd[a:b], stream=stream)
+            e1.record()
+            return e0, e1
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        launches0 = sum(s.launches() for s in sv)
+        ev = [step() for _ in range(args.steps)]
+        torch.cuda.synchronize()
+        ms = float(sum(a.elapsed_time(b) for a, b in ev)) / args.steps
+        st = stats.cpu().numpy()
+        res = {"ms_per_call": ms, "value": float(st[:, 0].sum()) / (ms * 1e-3),
+               "failed_zones": int((ierr.cpu().numpy() != 0).sum()),
+               "gpu_launches": int(sum(s.launches() for s in sv) - launches0),
+               "X": X.cpu().numpy(), "stats": st}
+        for s in sv:
+            s.close()
+        return res
+
+    with ClockSampler(dev) as clk:
+        clk.mark()
+        one = form(0, True)
+        clocks = clk.summary()
+    sep = form(0, False)
+    mixp = form(1, True)
+    rel_mixed = parity_rel(mixp["X"], one["X"])
+    per_net = {}
+    for i, n in enumerate(nets):
+        rows = np.nonzero(net_of == i)[0]
+        per_net[n.name] = {"zones": int(rows.size), "accepted_steps": int(one["stats"][rows, 0].sum()),
+                           "max_active_species": int(one["stats"][rows, 7].max())}
+    line = {"metric": "zone-timesteps/s", "value": one["value"], "unit": "zone-timesteps/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": one["ms_per_call"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "run": {"l2": "flushed: 256 MiB written before each timed call", "per_network": per_net,
+                    "failed_zones": one["failed_zones"]},
+            "gpu_launches": one["gpu_launches"],
+            "separate_launches": {k: sep[k] for k in ("ms_per_call", "value", "failed_zones")},
+            "one_launch_over_separate": one["value"] / sep["value"],
+            "mixed_precision": {k: mixp[k] for k in ("ms_per_call", "value", "failed_zones")},
+            "mixed_over_fp64": mixp["value"] / one["value"],
+            "mixed_max_rel_dev_vs_fp64": rel_mixed, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+
+
+def parity_rel(X, Xr):
+    """Largest relative difference over entries with Xr > 1e-12 (other entries: ignored)."""
+    big = Xr > 1e-12
+    return float((np.abs(X - Xr)[big] / Xr[big]).max(initial=0.0))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--nz", type=int, default=1024)
+    ap.add_argument("--nz", type=int, default=None, help="zones (trajectories) per GPU: 4096 for mixed, else 1024")
     ap.add_argument("--cpu-zones", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="heshell", choices=["heshell", "traj", "serve", "hburn"],
+    ap.add_argument("--workload", default="heshell", choices=["heshell", "traj", "serve", "hburn", "mixed"],
                     help="heshell: 1024 He-shell zones (the headline); traj: tppnp-style trajectories; "
                          "serve: Poisson request stream through nuppn_serve_*; hburn: the ppn frame of one "
                          "H-burning zone (200 backward-Euler frame steps)")
     ap.add_argument("--rate", type=float, default=2000.0, help="serve: mean requests per second")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="serve: arrival window (s)")
     args = ap.parse_args()
+    if args.nz is None:
+        args.nz = 4096 if args.workload == "mixed" else 1024
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -568,6 +710,9 @@ def main():
         return
     if args.workload == "hburn":
         run_hburn(args, rank, world)
+        return
+    if args.workload == "mixed":
+        run_mixed(args, rank, world)
         return
     if args.impl == "reference":
         run_reference(args, rank, world)

@@ -216,6 +216,38 @@ nuppn_status nuppn_set_knobs(nuppn_net *net, const nuppn_knobs *knobs);
 nuppn_status nuppn_isotopedatabase_read(const char *path, int32_t nnn, int32_t *z, int32_t *a, uint8_t *consider,
                                         char *elem);
 
+/* The network of a networksetup.txt file (physics/source/networksetup.F90): what write_networksetup
+ * (:55-115, output_network) writes and read_networksetup (:140-260) reads, in the reference's slot
+ * order. Names and labels are 5 characters each, blank padded, without NUL. k holds k1..k8 per
+ * reaction: k1, k3, k5, k7 are 0-based species indices (-1 for a name not in the list), k2, k4, k6,
+ * k8 the counts. Arrays are the caller's: sized nsp (species) and nre (reactions). */
+typedef struct nuppn_netsetup {
+  int32_t nsp, nre;                   /* NGIS species, NGIR reactions                                 */
+  int32_t nisomers, nreac_isomers;    /* inumer, inumerr                                              */
+  double t9, rho;                     /* set-up temperature and density of the header                 */
+  char *zis;                          /* [nsp][5] species names                                       */
+  uint8_t *considerisotope;           /* [nsp]                                                        */
+  double *anetw, *znetw;              /* [nsp]                                                        */
+  int32_t *isomeric_state;            /* [nsp] 1 ground, 2 isomer                                     */
+  uint8_t *considerreaction;          /* [nre]                                                        */
+  int32_t *k;                         /* [nre][8]                                                     */
+  double *v;                          /* [nre] rate at the set-up T9 and rho                          */
+  char *lab, *labb;                   /* [nre][5] rate reference and reaction type labels             */
+  int32_t *ilabb;                     /* [nre] reaction type 1..22                                    */
+  double *rfac, *bind_energy_diff;    /* [nre]                                                        */
+} nuppn_netsetup;
+
+/* write_networksetup: the file in the reference's fixed-column format (the lines
+ * read_networksetup reads with its formats '(7x,I5,16x,I5)', fmtspecies and fmtreactionread). */
+nuppn_status nuppn_networksetup_write(const char *path, const nuppn_netsetup *ns);
+
+/* read_networksetup: with every array pointer NULL, fills only nsp, nre, nisomers, nreac_isomers,
+ * t9 and rho (to size the arrays); otherwise also the arrays, which must hold ns->nsp species and
+ * ns->nre reactions as set by the first call. NUPPN_ERR_ARG if the file cannot be read or a line does
+ * not parse. Like the reference (:226-240), reactions with a participant whose considerisotope is
+ * false are marked not considered. */
+nuppn_status nuppn_networksetup_read(const char *path, nuppn_netsetup *ns);
+
 /* Static Jacobian pattern of makemap (jac_rhs.F90:461-540): row/col (0-based) of each COO entry in
  * the reference's row-major numbering, and dns2csr_map[nre][8] (entry index per slot, -1 if the
  * reaction is not considered). Sizes: row/col [nnz_jac]. */

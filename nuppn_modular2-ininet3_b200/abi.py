@@ -106,6 +106,16 @@ class ServeStats(C.Structure):
                 ("published", C.c_int64), ("completed", C.c_int64), ("device_bytes", C.c_int64)]
 
 
+class NetSetup(C.Structure):
+    """nuppn_netsetup (include/nuppn.h)."""
+    _fields_ = [("nsp", C.c_int32), ("nre", C.c_int32), ("nisomers", C.c_int32), ("nreac_isomers", C.c_int32),
+                ("t9", C.c_double), ("rho", C.c_double), ("zis", C.c_void_p), ("considerisotope", C.c_void_p),
+                ("anetw", C.c_void_p), ("znetw", C.c_void_p), ("isomeric_state", C.c_void_p),
+                ("considerreaction", C.c_void_p), ("k", C.c_void_p), ("v", C.c_void_p), ("lab", C.c_void_p),
+                ("labb", C.c_void_p), ("ilabb", C.c_void_p), ("rfac", C.c_void_p),
+                ("bind_energy_diff", C.c_void_p)]
+
+
 class TuneResult(C.Structure):
     _fields_ = [("threads_per_zone", C.c_int32), ("zones_per_cta", C.c_int32), ("zone_smem", C.c_int32),
                 ("zones_per_sm", C.c_int32), ("ms", C.c_double), ("zone_steps_per_s", C.c_double),

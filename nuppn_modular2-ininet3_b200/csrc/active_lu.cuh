@@ -46,6 +46,7 @@ struct Act {
   double *anc;       // [na] mass number of active row c
   double *xnc;       // [na+1] molar abundances of the active rows; xnc[na] = 1 (gamma)
   double *T, *rinv;  // tile: T[c*tile_rows + r] = entry (r, c) of L\U; rinv[r] = 1 / U(r, r)
+  int *perm;         // tile: original row at each position of the pivoted factor (P b = b[perm])
   // mixed precision (lu_precision = 1, tile systems): T keeps I - hJ unfactored in FP64 for the
   // refinement residuals; T32 / rinv32 hold the FP32 factor of diag(srow) (I - hJ) diag(scol)
   bool mixed;        // the tile has the mixed-precision arrays
@@ -98,9 +99,11 @@ __device__ __forceinline__ void act_bind(Act &A, char *base, int na, int nnz, in
   if (A.tile) {
     A.T = (double *)p; p += (size_t)na * tile_rows * 8;
     A.rinv = (double *)p; p += (size_t)tile_rows * 8;
+    A.perm = (int *)p; p += a16((size_t)tile_rows * 4);
   } else {
     A.T = nullptr;
     A.rinv = nullptr;
+    A.perm = nullptr;
   }
   A.mixed = mixed && A.tile;
   A.mixed_now = false;
@@ -447,19 +450,57 @@ __device__ __forceinline__ double assemble_entry(Act &A, int p, double h) {
 __device__ __forceinline__ bool pivot_ok(double d) { return d != 0.0 && isfinite(d); }
 __device__ __forceinline__ bool pivot_ok(float d) { return d != 0.0f && isfinite(d); }
 
-// Right-looking elimination of a dense tile by all warps of the CTA. At pivot k every warp forms
-// the multipliers l_r = a_rk / a_kk of the rows below in registers (lane l owns rows l + 32 i) and
-// updates its share of the trailing columns (m = k+1+w, step nw); one barrier per pivot. Column k is
-// left unscaled during the elimination and scaled at the end by the stored reciprocal, the same
-// product a_rk * (1 / a_kk) that SuperLU forms (dpivotL.c:178-180). Returns false on a zero or
-// non-finite pivot.
+// Right-looking elimination of a dense tile by all warps of the group, with row pivoting. At pivot k
+// every warp finds the pivot row of column k by SuperLU's threshold rule with u = 1 (dpivotL.c:
+// the diagonal when no entry below it is larger in magnitude, else the first largest), the rows are
+// exchanged across all columns (perm tracks which original row sits at each position, so that a
+// right-hand side b is solved as P b), then every warp forms the multipliers l_r = a_rk / a_kk of the
+// rows below in registers (lane l owns rows l + 32 i) and updates its share of the trailing columns
+// (m = k+1+w, step nw). Column k is left unscaled during the elimination and scaled at the end by the
+// stored reciprocal, the same product a_rk * (1 / a_kk) that SuperLU forms (dpivotL.c:178-180).
+// Without pivoting, I - hJ of a large step is not diagonally dominant, and the small components of
+// the solution (species depleted by many orders of magnitude) lose their relative accuracy.
+// Returns false on a zero or non-finite pivot.
 // F = double for the FP64 factor; F = float for the FP32 factor of the mixed-precision mode.
 template <int R, typename F = double>
-__device__ bool tile_factor_block(F *T, F *rinv, int na) {
+__device__ bool tile_factor_block(F *T, F *rinv, int *perm, int na) {
   constexpr int S = 32 * R;
   const int lane = GT & 31, w = GT >> 5, nw = GN >> 5;
   int bad = 0;
+  for (int r = GT; r < na; r += GN) perm[r] = r;
+  GSYNC();
   for (int k = 0; k < na; ++k) {
+    // pivot row: the same search in every warp (rows k .. na-1 of column k)
+    F best = F(-1);
+    int bi = k;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int r = lane + 32 * i;
+      if (r >= k && r < na) {
+        const F a = fabs(T[k * S + r]);
+        if (a > best) { best = a; bi = r; }
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const F ob = __shfl_xor_sync(NUPPN_FULL, best, o);
+      const int oi = __shfl_xor_sync(NUPPN_FULL, bi, o);
+      if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+    }
+    const int pr = fabs(T[k * (S + 1)]) >= best ? k : bi;
+    GSYNC();  // every warp has read column k (so every warp found the same pivot row) before any swap
+    if (pr != k) {  // exchange rows k and pr in every column
+      for (int c = GT; c < na; c += GN) {
+        const F t = T[c * S + k];
+        T[c * S + k] = T[c * S + pr];
+        T[c * S + pr] = t;
+      }
+      if (GT == 0) {
+        const int t = perm[k];
+        perm[k] = perm[pr];
+        perm[pr] = t;
+      }
+      GSYNC();
+    }
     const F piv = T[k * (S + 1)];
     bad |= !pivot_ok(piv);
     const F rp = F(1) / piv;
@@ -497,6 +538,22 @@ __device__ bool tile_factor_block(F *T, F *rinv, int na) {
   return g_or(bad) == 0;
 }
 
+// Right-hand side of the calling warp (rows lane + 32 i in x) into the factor's row order: x_r becomes
+// b_perm[r] (P b). scratch: na doubles no one else uses meanwhile.
+template <int R, typename F>
+__device__ __forceinline__ void tile_permute_rhs(F (&x)[R], const int *perm, int na, double *scratch, int lane) {
+#pragma unroll
+  for (int i = 0; i < R; ++i)
+    if (lane + 32 * i < na) scratch[lane + 32 * i] = (double)x[i];
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int r = lane + 32 * i;
+    x[i] = r < na ? (F)scratch[perm[r]] : F(0);
+  }
+  __syncwarp();
+}
+
 // Power of two that brings |m| into [1, 2) (1 for 0 or non-finite m).
 __device__ __forceinline__ double pow2_scale(double m) {
   return (m > 0.0 && isfinite(m)) ? ldexp(1.0, -ilogb(m)) : 1.0;
@@ -530,7 +587,7 @@ __device__ bool tile_factor_mixed(Act &A, int na) {
     A.T32[i] = r < na ? (float)(T[i] * A.scol[c] * A.srow[r]) : 0.0f;
   }
   GSYNC();
-  return tile_factor_block<R, float>(A.T32, A.rinv32, na);
+  return tile_factor_block<R, float>(A.T32, A.rinv32, A.perm, na);
 }
 
 // Forward and backward substitution of a factored tile by one warp, x[i] holding row lane + 32 i.
@@ -707,6 +764,7 @@ __device__ int tile_solve_mixed(const Act &A, double (&x)[R], int lane) {
     float f[R];
 #pragma unroll
     for (int i = 0; i < R; ++i) f[i] = (float)ldexp(r[i] * sr[i], -e);
+    tile_permute_rhs<R>(f, A.perm, na, A.xs, lane);  // the FP32 factor is of P diag(srow) (I - hJ) diag(scol)
     int bad = 0;
     tile_solve_core<R, false, float>(A.T32, A.rinv32, na, f, ri, lane, bad);
     double dm = 0.0, xm = 0.0;
@@ -731,16 +789,19 @@ __device__ int tile_solve_mixed(const Act &A, double (&x)[R], int lane) {
   return sweeps;
 }
 
-// Tile solve in place on A.xs by the calling warp.
+// Tile solve in place on A.xs by the calling warp. The FP64 factor is of P (I - hJ): its right-hand
+// side is read in the factor's row order; the mixed-precision solve permutes its own FP32 right-hand
+// sides (its residuals are formed in the original row order).
 template <int R>
 __device__ void tile_solve_xs(const Act &A, int lane) {
   double x[R], ri[R];
 #pragma unroll
   for (int i = 0; i < R; ++i) {
     const int r = lane + 32 * i;
-    x[i] = r < A.na ? A.xs[r] : 0.0;
+    x[i] = r < A.na ? A.xs[A.mixed_now ? r : A.perm[r]] : 0.0;
     ri[i] = r < A.na ? A.rinv[r] : 0.0;
   }
+  __syncwarp();  // every lane has read A.xs before any lane writes it (in the mixed solve or below)
   if (A.mixed_now) tile_solve_mixed<R>(A, x, lane);
   else tile_solve_regs<R>(A.T, A.rinv, A.na, x, ri, lane);
 #pragma unroll
@@ -748,7 +809,8 @@ __device__ void tile_solve_xs(const Act &A, int lane) {
     if (lane + 32 * i < A.na) A.xs[lane + 32 * i] = x[i];
 }
 
-// I - hJ on the active subsystem and its factorization in the static order, no pivoting.
+// I - hJ on the active subsystem and its factorization in the static order: dense tiles with row
+// pivoting (tile_factor_block), larger systems with diagonal pivots.
 // Returns false on a zero or non-finite pivot, or if a dependency wait timed out.
 __device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h) {
   const int tid = GT, nt = GN, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
@@ -766,7 +828,7 @@ __device__ bool dev_factor_active(const DevNet &N, const Ws &W, Act &A, double h
       A.mixed_now = S == 32 ? tile_factor_mixed<1>(A, na) : tile_factor_mixed<2>(A, na);
       if (A.mixed_now) return true;  // otherwise factor in FP64 (T is still unfactored)
     }
-    return S == 32 ? tile_factor_block<1>(T, A.rinv, na) : tile_factor_block<2>(T, A.rinv, na);
+    return S == 32 ? tile_factor_block<1>(T, A.rinv, A.perm, na) : tile_factor_block<2>(T, A.rinv, A.perm, na);
   }
   for (int p = tid; p < A.nnz; p += nt) A.cval[p] = assemble_entry(A, p, h);
   GSYNC();

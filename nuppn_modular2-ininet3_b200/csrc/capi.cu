@@ -518,6 +518,20 @@ nuppn_status nuppn_isotopedatabase_read(const char *path, int32_t nnn, int32_t *
   return NUPPN_OK;
 }
 
+nuppn_status nuppn_networksetup_write(const char *path, const nuppn_netsetup *ns) {
+  if (!ns) { set_error("null argument"); return NUPPN_ERR_ARG; }
+  const std::string err = write_networksetup(path, *ns);
+  if (!err.empty()) { set_error(err); return NUPPN_ERR_ARG; }
+  return NUPPN_OK;
+}
+
+nuppn_status nuppn_networksetup_read(const char *path, nuppn_netsetup *ns) {
+  if (!ns) { set_error("null argument"); return NUPPN_ERR_ARG; }
+  const std::string err = read_networksetup(path, *ns);
+  if (!err.empty()) { set_error(err); return NUPPN_ERR_ARG; }
+  return NUPPN_OK;
+}
+
 nuppn_status nuppn_jac_pattern(const nuppn_net *net, int32_t *row, int32_t *col, int32_t *map) {
   if (!net) return NUPPN_ERR_ARG;
   const HostNet &H = net->H;
@@ -794,11 +808,13 @@ nuppn_status nuppn_autotune(nuppn_net *net, int32_t nz, const double *X, int32_t
   CK(cudaMemcpy(b + o4, rho_1, vb, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(b + oy0, ye, vb, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(b + odt, dtwant, vb, cudaMemcpyHostToDevice));
-  // candidates: one zone per CTA of 256 threads (3 per SM); one zone per warp with 8 zones per CTA,
-  // 4 per CTA at the same share of shared memory (two CTAs per SM), and 4 per CTA with twice the
-  // share (64-row tiles of the hottest zones fit in shared memory, one CTA per SM)
+  // candidates: one zone per CTA of 256 threads and 72 KB (3 per SM), of 128 threads and 36 KB (6 per
+  // SM) and of 64 threads and 24 KB (9 per SM): fewer threads for the wide phases, more zones whose
+  // one-warp dependency chains share the SM; one zone per warp with 8 zones per CTA, 4 per CTA at the
+  // same share of shared memory (two CTAs per SM), and 4 per CTA with twice the share (64-row tiles
+  // of the hottest zones fit in shared memory, one CTA per SM)
   struct Cand { int tpz, zpc, smem; };
-  const Cand cands[] = {{0, 0, 0}, {32, 8, 0}, {32, 4, 27648}, {32, 4, 0}};
+  const Cand cands[] = {{0, 0, 0}, {128, 0, 36864}, {64, 0, 24576}, {32, 8, 0}, {32, 4, 27648}, {32, 4, 0}};
   const int nc = (int)(sizeof(cands) / sizeof(cands[0]));
   const nuppn_knobs base = net->H.kn;
   cudaEvent_t e0 = nullptr, e1 = nullptr;

@@ -235,8 +235,12 @@ __device__ int bd_level_tile(const Act &A, const BdVec &B, double h, int nseq, b
           x[i] = stage == 1 ? h * dx : h * dx - d[i];
         }
       }
-      if (A.mixed_now) sweeps += tile_solve_mixed<R>(A, x, lane);
-      else tile_solve_regs<R>(A.T, A.rinv, na, x, ri, lane);
+      if (A.mixed_now) {
+        sweeps += tile_solve_mixed<R>(A, x, lane);
+      } else {
+        tile_permute_rhs<R>(x, A.perm, na, A.xs, lane);  // the factor is of P (I - hJ)
+        tile_solve_regs<R>(A.T, A.rinv, na, x, ri, lane);
+      }
       bool huge = false;
 #pragma unroll
       for (int i = 0; i < R; ++i) {

@@ -84,4 +84,8 @@ struct IsotopeEntry {
 // not parse, or the file has fewer than nnn entries, where the reference stops the run).
 std::string read_isotope_database(const char *path, int nnn, std::vector<IsotopeEntry> &out);
 
+// networksetup.txt (netsetup.cpp): write_networksetup / read_networksetup of networksetup.F90.
+std::string write_networksetup(const char *path, const nuppn_netsetup &ns);
+std::string read_networksetup(const char *path, nuppn_netsetup &ns);
+
 }  // namespace nuppn

@@ -129,7 +129,7 @@ NUPPN_HD inline int tile_rows_for(int na, int limit) {
 // rows (see active_lu.cuh): int crp[na+1], cdiag[na], arow[na], flagF[na], flagS[na], ccol[nnz],
 // csrc[nnz]; without a tile double cval[nnz], wbuf[nwarps*na], rdg[na]; double xs[na], jval[nnz], anc[na],
 // xnc[na+1]; uint8 jflag[nnz]; with a tile double T[na * tile_rows] (na columns of tile_rows rows),
-// rinv[tile_rows]; a mixed-precision tile adds float T32[na * tile_rows], rinv32[tile_rows] and double
+// rinv[tile_rows], int perm[tile_rows]; a mixed-precision tile adds float T32[na * tile_rows], rinv32[tile_rows] and double
 // srow[tile_rows], scol[tile_rows]. Every array 16-byte aligned.
 NUPPN_HD inline size_t act_bytes(int na, int nnz, int nwarps, int tile_rows, bool mixed = false) {
   size_t b = a16((size_t)(na + 1) * 4) + 4 * a16((size_t)na * 4) + 2 * a16((size_t)nnz * 4);
@@ -137,6 +137,7 @@ NUPPN_HD inline size_t act_bytes(int na, int nnz, int nwarps, int tile_rows, boo
   b += a16((size_t)na * 8);
   b += a16((size_t)nnz * 8) + a16((size_t)na * 8) + a16((size_t)(na + 1) * 8) + a16((size_t)nnz);
   b += (size_t)na * tile_rows * 8 + (size_t)tile_rows * 8;
+  if (tile_rows > 0) b += a16((size_t)tile_rows * 4);  // row permutation of the pivoted tile
   if (mixed && tile_rows > 0) b += (size_t)na * tile_rows * 4 + a16((size_t)tile_rows * 4) + 2 * (size_t)tile_rows * 8;
   return b;
 }

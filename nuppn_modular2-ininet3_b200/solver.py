@@ -56,6 +56,9 @@ def load_library():
     L.nuppn_autotune.argtypes = [vp, i32, vp, i32, vp, vp, vp, vp, vp, vp, i32, vp, i32, vp]
     L.nuppn_integrate_multi.argtypes = [vp, i32, i32, vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.nuppn_integrate_multi_device.argtypes = [vp, i32, i32, vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.nuppn_networksetup_write.argtypes = [C.c_char_p, vp]
+    L.nuppn_networksetup_read.argtypes = [C.c_char_p, vp]
+    L.nuppn_isotopedatabase_read.argtypes = [C.c_char_p, i32, vp, vp, vp, C.c_char_p]
     L.nuppn_launch_count.argtypes = [vp]
     L.nuppn_launch_count.restype = i64
     L.nuppn_nse.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp]
@@ -74,7 +77,8 @@ def load_library():
                  "nuppn_integrate_trajectories", "nuppn_integrate_trajectories_device",
                  "nuppn_serve_open", "nuppn_serve_submit", "nuppn_serve_submit_trajectory", "nuppn_serve_poll",
                  "nuppn_serve_info", "nuppn_serve_close", "nuppn_autotune", "nuppn_integrate_multi",
-                 "nuppn_integrate_multi_device"):
+                 "nuppn_integrate_multi_device", "nuppn_networksetup_write", "nuppn_networksetup_read",
+                 "nuppn_isotopedatabase_read"):
         getattr(L, name).restype = i32
     _LIB = L
     return L
@@ -243,9 +247,9 @@ class NetworkSolver:
         nz = X.shape[0]
         f = lambda a: _f64(a, nz)
         args = [f(a) for a in (t9_0, t9_1, rho_0, rho_1, ye, dtwant)]
-        rep = (abi.TuneResult * 8)()
+        rep = (abi.TuneResult * 16)()
         n = C.c_int32(0)
-        self._check(self.L.nuppn_autotune(self.h, nz, _p(X), X.shape[1], *[_p(a) for a in args], int(sample), rep, 8,
+        self._check(self.L.nuppn_autotune(self.h, nz, _p(X), X.shape[1], *[_p(a) for a in args], int(sample), rep, 16,
                                           C.byref(n)))
         return [{k: getattr(rep[i], k) for k, _ in abi.TuneResult._fields_ if k != "reserved"}
                 for i in range(n.value)]
@@ -257,6 +261,62 @@ class NetworkSolver:
         self._check(self.L.nuppn_integrate_device(
             self.h, X.shape[0], ptr(X), X.shape[1], ptr(t9_0), ptr(t9_1), ptr(rho_0), ptr(rho_1), ptr(ye),
             ptr(dtwant), ptr(ierr), ptr(stats), ptr(bd_state), C.c_void_p(stream)))
+
+
+# rate-source labels written to networksetup.txt's lab column, by descriptor source (NUPPN_SRC_*)
+_SRC_LABEL = {0: "OOOOO", 1: "VITAL", 2: "JINAC", 3: "NETB1", 4: "FFW85", 5: "KADON", 6: "ALPHA"}
+
+
+def _str5(items):
+    return b"".join(s.encode()[:5].ljust(5) for s in items)
+
+
+def networksetup_write(path, net, t9=0.0, rho=0.0, v=None):
+    """write_networksetup (networksetup.F90:55-115) for a network description: its species, their
+    switches, A and Z, and every reaction slot with k1..k8, the reaction type label and the rate
+    factor; v (the rates at t9, rho) is written as 0 if not given. Host only."""
+    L = load_library()
+    nsp, nre = net.nsp, net.nre
+    zis = C.create_string_buffer(_str5(net.zis), 5 * nsp)
+    labb = C.create_string_buffer(_str5([sn.RLABELS.get(int(t), "     ") for t in net.ilabb]), 5 * nre)
+    lab = C.create_string_buffer(_str5([_SRC_LABEL.get(int(x), "     ") for x in net.src]), 5 * nre)
+    arr = {"considerisotope": np.ascontiguousarray(net.considerisotope, np.uint8),
+           "anetw": np.ascontiguousarray(net.anetw, np.float64), "znetw": np.ascontiguousarray(net.znetw, np.float64),
+           "isomeric_state": np.ones(nsp, np.int32),
+           "considerreaction": np.ascontiguousarray(net.considerreaction, np.uint8),
+           "k": np.ascontiguousarray(net.k, np.int32),
+           "v": np.zeros(nre) if v is None else np.ascontiguousarray(v, np.float64),
+           "ilabb": np.ascontiguousarray(net.ilabb, np.int32), "rfac": np.ascontiguousarray(net.rfac, np.float64),
+           "bind_energy_diff": np.zeros(nre)}
+    ns = abi.NetSetup(nsp=nsp, nre=nre, nisomers=0, nreac_isomers=0, t9=float(t9), rho=float(rho),
+                      zis=C.cast(zis, C.c_void_p), lab=C.cast(lab, C.c_void_p), labb=C.cast(labb, C.c_void_p),
+                      **{k: a.ctypes.data for k, a in arr.items()})
+    if L.nuppn_networksetup_write(str(path).encode(), C.byref(ns)) != 0:
+        raise NuppnError(L.nuppn_last_error().decode())
+
+
+def networksetup_read(path):
+    """read_networksetup (networksetup.F90:140-260): a dict of the file's arrays (zis, lab, labb as
+    lists of 5-character strings; k as [nre, 8] with 0-based species indices) and its header."""
+    L = load_library()
+    ns = abi.NetSetup()
+    if L.nuppn_networksetup_read(str(path).encode(), C.byref(ns)) != 0:
+        raise NuppnError(L.nuppn_last_error().decode())
+    nsp, nre = ns.nsp, ns.nre
+    zis, lab, labb = (C.create_string_buffer(5 * max(n, 1)) for n in (nsp, nre, nre))
+    arr = {"considerisotope": np.zeros(nsp, np.uint8), "anetw": np.zeros(nsp), "znetw": np.zeros(nsp),
+           "isomeric_state": np.zeros(nsp, np.int32), "considerreaction": np.zeros(nre, np.uint8),
+           "k": np.zeros((nre, 8), np.int32), "v": np.zeros(nre), "ilabb": np.zeros(nre, np.int32),
+           "rfac": np.zeros(nre), "bind_energy_diff": np.zeros(nre)}
+    for k, a in arr.items():
+        setattr(ns, k, a.ctypes.data)
+    ns.zis, ns.lab, ns.labb = (C.cast(b, C.c_void_p) for b in (zis, lab, labb))
+    if L.nuppn_networksetup_read(str(path).encode(), C.byref(ns)) != 0:
+        raise NuppnError(L.nuppn_last_error().decode())
+    split = lambda b, n: [b.raw[5 * i:5 * i + 5].decode() for i in range(n)]
+    arr.update(zis=split(zis, nsp), lab=split(lab, nre), labb=split(labb, nre), t9=ns.t9, rho=ns.rho,
+               nisomers=ns.nisomers, nreac_isomers=ns.nreac_isomers)
+    return arr
 
 
 def _handles(solvers):

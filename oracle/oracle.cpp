@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <tuple>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -953,8 +954,65 @@ struct SluFactors {
   bool live = false;
 };
 
+// Experiment hook for the tests (environment ORACLE_LU_PERMUTE=<seed>): hand SuperLU the reduced
+// system under a seeded symmetric permutation P A P^T (and P b, the solution permuted back). The
+// system is the same; only the elimination order, and so the rounding, changes. This measures how far
+// the checker's own results depend on the LU's elimination order.
+static int lu_permute_seed() {
+  static int seed = -2;
+  if (seed == -2) {
+    const char *e = getenv("ORACLE_LU_PERMUTE");
+    seed = e ? atoi(e) : -1;
+  }
+  return seed;
+}
+
+static vector<int> lu_permutation(int n, int seed) {
+  vector<int> p(n);
+  for (int i = 0; i < n; ++i) p[i] = i;
+  unsigned long long st = 0x9E3779B97F4A7C15ull * (unsigned long long)(seed + 1) + (unsigned long long)n;
+  for (int i = n - 1; i > 0; --i) {  // Fisher-Yates with a 64-bit LCG
+    st = st * 6364136223846793005ull + 1442695040888963407ull;
+    const int j = (int)((st >> 33) % (unsigned long long)(i + 1));
+    std::swap(p[i], p[j]);
+  }
+  return p;
+}
+
+// CSC (1-based, as the shim takes it) of P A P^T: entry (i, j) moves to (p[i], p[j]).
+static void permute_csc(int n, const vector<double> &val, const vector<int> &row, const vector<int> &col,
+                        const vector<int> &p, vector<double> &pv, vector<int> &pr, vector<int> &pc) {
+  vector<std::tuple<int, int, double>> e;
+  for (int j = 0; j < n; ++j)
+    for (int q = col[j] - 1; q < col[j + 1] - 1; ++q) e.emplace_back(p[j], p[row[q] - 1], val[q]);
+  std::sort(e.begin(), e.end(), [](const auto &a, const auto &b) {
+    return std::get<0>(a) != std::get<0>(b) ? std::get<0>(a) < std::get<0>(b) : std::get<1>(a) < std::get<1>(b);
+  });
+  pv.resize(e.size());
+  pr.resize(e.size());
+  pc.assign(n + 1, 0);
+  for (size_t q = 0; q < e.size(); ++q) {
+    pv[q] = std::get<2>(e[q]);
+    pr[q] = std::get<1>(e[q]) + 1;
+    pc[std::get<0>(e[q]) + 1]++;
+  }
+  for (int j = 0; j < n; ++j) pc[j + 1] += pc[j];
+  for (int j = 0; j <= n; ++j) pc[j] += 1;
+}
+
 int bd_step(Zone &Z, vector<double> &y_k, vector<double> &delta_k, double h, int nvar1, int stage,
-            const vector<double> &cval, vector<int> &crow, vector<int> &ccol, SluFactors &F) {
+            const vector<double> &cval_in, vector<int> &crow_in, vector<int> &ccol_in, SluFactors &F) {
+  const int pseed = lu_permute_seed();
+  vector<int> perm;
+  vector<double> pval;
+  vector<int> prow, pcol;
+  if (pseed >= 0 && nvar1 > 0) {
+    perm = lu_permutation(nvar1, pseed);
+    permute_csc(nvar1, cval_in, crow_in, ccol_in, perm, pval, prow, pcol);
+  }
+  const vector<double> &cval = perm.empty() ? cval_in : pval;
+  vector<int> &crow = perm.empty() ? crow_in : prow;
+  vector<int> &ccol = perm.empty() ? ccol_in : pcol;
   const Net &N = *Z.N;
   enum { FIRST = 1, MID = 2, LAST = 3 };
   int ierr = 0;
@@ -976,7 +1034,17 @@ int bd_step(Zone &Z, vector<double> &y_k, vector<double> &delta_k, double h, int
   }
   if (n > 0) {
     iopt = 2;
+    if (!perm.empty()) {
+      vector<double> t(n);
+      for (int i = 0; i < n; ++i) t[perm[i]] = rr[i];
+      rr = t;
+    }
     g_dgssv(&iopt, &n, &nnz, &nrhs, vals.data(), crow.data(), ccol.data(), rr.data(), &ldb, &F.h, &info);
+    if (!perm.empty()) {
+      vector<double> t(n);
+      for (int i = 0; i < n; ++i) t[i] = rr[perm[i]];
+      rr = t;
+    }
   }
   Z.st.nsolve++;
   int icons = 0;

@@ -122,3 +122,50 @@ def test_serve_rejects_bad_arguments(solver_mod, abi, wl):
             srv.submit_trajectory(np.zeros(net.nsp), np.linspace(0, 1, n), np.ones(n), np.ones(n))
     finally:
         srv.close()
+
+
+def test_serve_small_dt_outcomes_match_checker(solver_mod, abi, orc, wl):
+    """48 H-burning zones of the serving stream (300 species, T9 U[0.015, 0.08], rho log-U[1, 1e3],
+    1e10 s, Bader-Deuflhard) through the server: each zone's outcome (success or SMALL_DT, the step
+    falling below 1e-30 s) equals the checker's on every zone whose checker outcome stays the same
+    under two draws of 1-ulp input changes (on the others the reference's own outcome is not
+    determined by its input), and successful zones meet the parity bar."""
+    import parity
+
+    net = wl.network(300)
+    hb, _ = wl.hburn_zone(net)
+    rng = np.random.default_rng(11)
+    n = 48
+    t9 = rng.uniform(0.015, 0.08, n)
+    rho = 10.0 ** rng.uniform(0.0, 3.0, n)
+    X = np.repeat(hb.X, n, axis=0)
+    ye = np.repeat(hb.ye, n)
+    kn = abi.default_knobs(integration_method=1)
+    ref = orc.Oracle(net, kn)
+    Xr, _, ierr_r, _, _ = ref.integrate_network(X, t9, t9, rho, rho, ye, np.full(n, 1e10), nthreads=8)
+    stable = np.ones(n, bool)
+    for trial in (1, 2):
+        Xp = X * (1.0 + np.random.default_rng(trial).choice([-1.0, 0.0, 1.0], size=X.shape) * 2.2e-16)
+        ie = ref.integrate_network(Xp, t9, t9, rho, rho, ye, np.full(n, 1e10), nthreads=8)[2]
+        stable &= ie == ierr_r
+    assert (ierr_r == 11).sum() >= 5 and stable.sum() >= 32
+    dev = solver_mod.NetworkSolver(net, kn, device=0)
+    srv = solver_mod.Server(dev)
+    try:
+        ids = [srv.submit(X[z], t9[z], t9[z], rho[z], rho[z], ye[z], 1.0e10) for z in range(n)]
+        res = [srv.wait(i) for i in ids]
+    finally:
+        srv.close()
+    ierr = np.array([r[2] for r in res])
+    Xd = np.array([r[0] for r in res])
+    assert (ierr[stable] == ierr_r[stable]).all(), (ierr[stable], ierr_r[stable])
+    assert set(np.unique(ierr)) <= {0, 11}
+    ok = stable & (ierr == 0)
+    rel, ab = parity.zone_errors(Xd[ok], Xr[ok])
+    off = (rel > 1e-6) | (ab > 1e-15)
+    if off.any():  # only zones the checker itself cannot pin to 1e-6
+        sub = np.nonzero(ok)[0][off]
+        spread = parity.checker_spread(ref, wl.ZoneBatch(X=X[sub], t9_0=t9[sub], t9_1=t9[sub], rho_0=rho[sub],
+                                                        rho_1=rho[sub], ye=ye[sub], dtwant=np.full(sub.size, 1e10)),
+                                       Xr[sub], nthreads=8)
+        assert (rel[off] <= 2.0 * spread).all(), (rel[off], spread)

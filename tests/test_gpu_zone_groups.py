@@ -158,7 +158,7 @@ def test_autotune_picks_a_shape_and_keeps_results(solver_mod, abi, orc, wl):
     assert len(rep) >= 2 and sum(r["chosen"] for r in rep) == 1
     best = max((r for r in rep if r["zone_steps_per_s"] > 0), key=lambda r: r["zone_steps_per_s"])
     assert best["chosen"] == 1 and best["ms"] > 0 and best["zones_per_sm"] >= 1
-    assert {r["threads_per_zone"] for r in rep} == {0, 32}
+    assert {0, 64, 128, 32} <= {r["threads_per_zone"] for r in rep}
     X, ye, ierr, st, _ = dev.integrate_network(*args)
     ref = orc.Oracle(net, abi.default_knobs(integration_method=1))
     Xr, _, ierr_r, str_, _ = ref.integrate_network(*args, nthreads=8)
