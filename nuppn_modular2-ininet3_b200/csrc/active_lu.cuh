@@ -11,7 +11,7 @@
 // Per Jacobian (dev_jacobian_mask, then):
 //   dev_compact          active rows and the restricted filled pattern
 //   dev_jacobian_active  Jacobian values and entry flags of the active entries (all reactions)
-//   dev_compact_rhs      per-species gather items of the right-hand side
+//   dev_compact_rhs      per-species gather items of the right-hand side (all reactions)
 // Per factorization / right-hand side / solve: dev_factor_active, dev_dxdt_active, dev_solve_active,
 // all on compact vectors indexed by the active row number c. Systems of up to kTileMax rows (the
 // usual case: a few tens of species) are factored as a dense tile and solved with rows held in the
@@ -57,16 +57,12 @@ struct Act {
   double ir_rtol;
   int genF, genS;
   bool in_smem;
-  // reactions of the step (see dev_active_reactions), in the CTA's workspace
-  int nK, nP;
-  int *Klist;        // [nK] kept: first reactant masked, second masked or gamma
-  int *Plist;        // [nP] passing the rate test of dev_jacobian_mask (a subset of the kept)
   // right-hand side restricted to the dynamic network (see dev_compact_rhs)
   int ngi;
   int *gptr;         // [na+1] gather items of active row c: gptr[c] .. gptr[c+1]-1
   float *gcoef;      // [ngi] term coefficient (-k2, -1, k6 or k8)
   uint32_t *grpk;    // [ngi] compact index of reactant 1 | reactant 2 (na = gamma) << 14 | k2 << 28
-  double *grcv;      // [ngi] (1/k2!) * rate of the term's reaction
+  double *grcv;      // [ngi] (1/k2!) * rate of the term's reaction (a group's constant: see below)
   double *gterm;     // [ngi] term values of the current sub-step
   bool rhs_in_smem;
 };
@@ -271,142 +267,105 @@ __device__ __forceinline__ double jac_contrib(const DevNet &N, const Ws &W, int 
   return d;
 }
 
-// Reactions of the step, found through the active species' lists of the reactions they lead (k1):
-// every considered reaction whose first reactant is masked, in one flattened pass. K (kept) = those
-// whose second reactant is masked or gamma, the terms of the restricted right-hand side. P (passing)
-// = those that passed the rate test of dev_jacobian_mask, the only reactions that contribute to the
-// Jacobian (jac_rhs.F90:350-392); a passing reaction masks all its participants, so P is part of K.
-// Both lists are in flattened order (active row, then reaction index).
-__device__ void dev_active_reactions(const DevNet &N, const Ws &W, Act &A, int *sint) {
-  const int tid = GT, nt = GN, na = A.na, g = N.ig;
-  int *off = W.rx;                  // [na+1]
-  int *ra = off + (N.nsys + 1);     // [T] reaction of each flattened position
-  int *kf = ra + (N.nact + 1);      // [T+1] kept flags, then their positions
-  int *pf = kf + (N.nact + 1);      // [T+1] passing flags, then their positions
-  A.Klist = pf + (N.nact + 1);
-  A.Plist = A.Klist + (N.nact + 1);
-  for (int c = tid; c < na; c += nt) {
-    const int s = N.sp_of_sys[A.arow[c]];
-    off[c] = N.k1_ptr[s + 1] - N.k1_ptr[s];
-  }
-  GSYNC();
-  const int T = block_scan_excl(off, na, sint);
-  if (tid == 0) off[na] = T;
-  GSYNC();
-  for (int t = tid; t < T; t += nt) {
-    const int c = seg_of(off, na, t);
-    const int a = N.k1_list[N.k1_ptr[N.sp_of_sys[A.arow[c]]] + (t - off[c])];
-    const int k3 = N.act_k[(size_t)a * 8 + 2];
-    ra[t] = a;
-    kf[t] = (k3 == g || W.mask[k3]) ? 1 : 0;
-    pf[t] = W.flux[a] != 0.0 ? 1 : 0;
-  }
-  GSYNC();
-  const int nK = block_scan_excl(kf, T, sint);
-  const int nP = block_scan_excl(pf, T, sint);
-  if (tid == 0) {
-    kf[T] = nK;
-    pf[T] = nP;
-  }
-  GSYNC();
-  for (int t = tid; t < T; t += nt) {
-    if (kf[t + 1] > kf[t]) A.Klist[kf[t]] = ra[t];
-    if (pf[t + 1] > pf[t]) A.Plist[pf[t]] = ra[t];
-  }
-  A.nK = nK;
-  A.nP = nP;
-  GSYNC();
-}
-
-// Jacobian values (1e-99 + the contributions of every passing reaction, as in the reference) and
-// entry flags for the positions of the active subsystem. Entries with a short static gather list
-// evaluate it as one flattened, block-parallel list; the few entries with long lists (among n, p
-// and alpha) take their contributions from the passing reactions P. Each entry is summed by a warp.
+// Jacobian values (1e-99 + the contributions of every reaction that passes the rate test, masked
+// reactants or not, as in the reference) and entry flags for the positions of the active subsystem.
+// Entries with short static gather lists are evaluated as one flattened, block-parallel list and
+// summed by one thread each in the list's order from 1e-99 (the reference's accumulation: jac =
+// 1e-99, then += each contribution in reaction order, jac_rhs.F90:309-392). The few with long lists
+// (among n, p and alpha: every capture on every nucleus, frozen or not) are cut into pieces of
+// kRhsPiece items; a warp sums a piece (lane-strided, then a fixed butterfly) and each entry adds
+// its pieces' sums in piece order, so the result does not depend on which warp took which piece.
 __device__ void dev_jacobian_active(const DevNet &N, const Ws &W, Act &A, int *sint) {
-  const int tid = GT, nt = GN, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
-  int *off = W.act_otmp;  // [nnz+1] <= nnzLU + 1
-  for (int p = tid; p < A.nnz; p += nt) {
+  const int tid = GT, nt = GN, lane = tid & 31, w = tid >> 5, nw = nt >> 5, nnz = A.nnz;
+  int *off = W.act_otmp;                  // [nnz+1] short entries' items, then offsets
+  int *lfl = W.jac_long;                  // [nnz+1] long-entry flags, then their ranks
+  int *lst = W.jac_long + (N.nnzLU + 1);  // [nlong] positions of the long entries, in order
+  int *poff = lst + N.nnzLU;              // [nlong+1] their first pieces
+  for (int p = tid; p < nnz; p += nt) {
     const int e = N.lu_src[A.csrc[p]];
     const int len = e >= 0 ? N.jg_ptr[e + 1] - N.jg_ptr[e] : 0;
-    off[p] = len <= kLongList ? len : 0;
+    const bool lng = len > kLongList;
+    off[p] = lng ? 0 : len;
+    lfl[p] = lng ? 1 : 0;
   }
   GSYNC();
-  const int T = block_scan_excl(off, A.nnz, sint);
-  if (tid == 0) off[A.nnz] = T;
+  const int T = block_scan_excl(off, nnz, sint);  // <= the network's jg items: distinct entries
+  const int nlong = block_scan_excl(lfl, nnz, sint);
+  if (tid == 0) {
+    off[nnz] = T;
+    lfl[nnz] = nlong;
+  }
   GSYNC();
-  double *dv = W.act_dtmp;
-  uint8_t *sf = W.act_btmp;
+  for (int p = tid; p < nnz; p += nt) {
+    if (lfl[p + 1] == lfl[p]) continue;
+    const int e = N.lu_src[A.csrc[p]];
+    lst[lfl[p]] = p;
+    poff[lfl[p]] = (N.jg_ptr[e + 1] - N.jg_ptr[e] + kRhsPiece - 1) / kRhsPiece;
+  }
+  GSYNC();
+  const int NPc = block_scan_excl(poff, nlong, sint);
+  if (tid == 0) poff[nlong] = NPc;
+  GSYNC();
+  double *dv = W.act_dtmp;   // [T] short entries' contributions, then [NPc] long pieces' sums
+  uint8_t *sf = W.act_btmp;  // their entry-set flags
   for (int t = tid; t < T; t += nt) {
-    const int p = seg_of(off, A.nnz, t);
+    const int p = seg_of(off, nnz, t);
     const int e = N.lu_src[A.csrc[p]];
     const int it = N.jg_item[N.jg_ptr[e] + (t - off[p])];
     bool set;
     dv[t] = jac_contrib(N, W, it >> 3, it & 7, set);
     sf[t] = set ? 1 : 0;
   }
-  GSYNC();
-  // Short entries: one thread each, summed in the static list's order from 1e-99 (the reference's
-  // accumulation: jac = 1e-99, then += each contribution in reaction order, jac_rhs.F90:309-392).
-  // Long entries (a few: among n, p, alpha) are listed and summed by a warp each from P.
-  constexpr int kMaxLong = 128;
-  __shared__ int s_nlong_g[NUPPN_MAX_GROUPS];
-  __shared__ int s_longp_g[NUPPN_MAX_GROUPS][kMaxLong];
-  int &s_nlong = s_nlong_g[GID];
-  int *s_longp = s_longp_g[GID];
-  if (tid == 0) s_nlong = 0;
-  GSYNC();
-  for (int p = tid; p < A.nnz; p += nt) {
-    const int e = N.lu_src[A.csrc[p]];
-    if (e < 0) {
-      A.jval[p] = 0.0;
-      A.jflag[p] = JF_FILL;
-      continue;
-    }
-    if (N.jg_ptr[e + 1] - N.jg_ptr[e] > kLongList) {
-      const int k = atomicAdd(&s_nlong, 1);
-      if (k < kMaxLong) s_longp[k] = p;
-      continue;
-    }
-    double acc = 1.e-99;
-    int set = 0;
-    for (int t = off[p]; t < off[p + 1]; ++t) {
-      acc = acc + dv[t];
-      set |= sf[t];
-    }
-    A.jval[p] = acc;
-    A.jflag[p] = (uint8_t)((set ? JF_SET : 0) | (N.jdiag[N.jrow[e]] == e ? JF_DIAG : 0));
-  }
-  GSYNC();
-  const int nlong = s_nlong;
-  const int nwork = nlong <= kMaxLong ? nlong : A.nnz;  // more than kMaxLong: scan every position
-  for (int k = w; k < nwork; k += nw) {
-    const int p = nlong <= kMaxLong ? s_longp[k] : k;
-    const int e = N.lu_src[A.csrc[p]];
-    if (e < 0 || N.jg_ptr[e + 1] - N.jg_ptr[e] <= kLongList) continue;
+  for (int Q = w; Q < NPc; Q += nw) {
+    const int L = seg_of(poff, nlong, Q);
+    const int e = N.lu_src[A.csrc[lst[L]]];
+    const int *items = N.jg_item + N.jg_ptr[e];
+    const int t0 = (Q - poff[L]) * kRhsPiece, t1 = min(t0 + kRhsPiece, N.jg_ptr[e + 1] - N.jg_ptr[e]);
     double acc = 0.0;
     int set = 0;
-    for (int i = lane; i < A.nP; i += 32) {  // a lane takes whole reactions: their 8 targets in 2 loads
-      const int a = A.Plist[i];
-      const int4 *ice = reinterpret_cast<const int4 *>(N.act_ice + (size_t)a * 8);
-      const int4 u = ice[0], v = ice[1];
-      const int tg[8] = {u.x, u.y, u.z, u.w, v.x, v.y, v.z, v.w};
-#pragma unroll
-      for (int sl = 0; sl < 8; ++sl) {
-        if (tg[sl] == e) {
-          bool st;
-          acc += jac_contrib(N, W, a, sl, st);
-          set |= st ? 1 : 0;
-        }
-      }
+#pragma unroll 4
+    for (int t = t0 + lane; t < t1; t += 32) {
+      const int it = items[t];
+      bool st;
+      acc += jac_contrib(N, W, it >> 3, it & 7, st);
+      set |= st ? 1 : 0;
     }
     for (int o = 16; o > 0; o >>= 1) {
       acc += __shfl_xor_sync(NUPPN_FULL, acc, o);
       set |= __shfl_xor_sync(NUPPN_FULL, set, o);
     }
     if (lane == 0) {
-      A.jval[p] = 1.e-99 + acc;
-      A.jflag[p] = (uint8_t)((set ? JF_SET : 0) | (N.jdiag[N.jrow[e]] == e ? JF_DIAG : 0));
+      dv[T + Q] = acc;
+      sf[T + Q] = (uint8_t)set;
     }
+  }
+  GSYNC();
+  for (int p = tid; p < nnz; p += nt) {
+    const int e = N.lu_src[A.csrc[p]];
+    if (e < 0) {
+      A.jval[p] = 0.0;
+      A.jflag[p] = JF_FILL;
+      continue;
+    }
+    double acc;
+    int set = 0;
+    if (lfl[p + 1] > lfl[p]) {
+      const int L = lfl[p];
+      double sum = 0.0;
+      for (int Q = poff[L]; Q < poff[L + 1]; ++Q) {
+        sum += dv[T + Q];
+        set |= sf[T + Q];
+      }
+      acc = 1.e-99 + sum;
+    } else {
+      acc = 1.e-99;
+      for (int t = off[p]; t < off[p + 1]; ++t) {
+        acc = acc + dv[t];
+        set |= sf[t];
+      }
+    }
+    A.jval[p] = acc;
+    A.jflag[p] = (uint8_t)((set ? JF_SET : 0) | (N.jdiag[N.jrow[e]] == e ? JF_DIAG : 0));
   }
   GSYNC();
 }
@@ -982,18 +941,27 @@ __device__ bool dev_solve_species(const DevNet &N, Act &A, const double *rhs, do
 }
 
 // ---------------------------------------------------------------------------------------------
-// Right-hand side restricted to the dynamic network (after dev_compact and dev_active_reactions).
+// Right-hand side restricted to the dynamic network (after dev_compact).
 //
-// Within one step only dX/dt of masked species is used (the rest of the correction is zero, as in
-// ddecompac, jac_rhs.F90:584-608) and unmasked abundances stay frozen. A reaction with an unmasked
-// reactant did not pass the dynamic-network test itself (jac_rhs.F90:350-353: otherwise all its
-// participants would be masked), so its flux is at most y * cyminformal / dt for the frozen
-// reactant's abundance y, and it changes X by at most ~1e-30 over the step; such reactions are left
-// out. Each masked species keeps one gather item per term of a kept reaction: the term's coefficient
-// (-k2, -1, k6 or k8 for its slot k1, k3, k5, k7), the reaction's (1/k2!) * rate and the compact
-// indices of its reactants. Species with a short static list keep the reference's accumulation
-// order (reaction order, then slot); the few with long lists (n, p, alpha) take their terms from the
-// kept reactions K, in K's order. A sub-step recomputes each term's flux from the item.
+// Within one step only dX/dt of masked species is used (the correction is zero elsewhere, as in
+// ddecompac, jac_rhs.F90:584-608) and unmasked abundances stay frozen at the step's values, but
+// calculate_dxdt (jac_rhs.F90:217-278) still sums every considered reaction into the masked rows,
+// those with a frozen reactant included. Such a reaction failed the dynamic-network test at the
+// start of the step, yet its flux can grow within the step with its masked reactant: neutron
+// captures on frozen seed nuclei take up neutrons once a neutron source has switched on. Each masked
+// row therefore gets
+//  - one term per reaction whose reactants are all masked (or gamma): the slot's coefficient (-k2,
+//    -1, k6 or k8 for k1, k3, k5, k7), the reaction's (1/k2!) * rate and the compact indices of its
+//    reactants, evaluated from each sub-step's abundances in the reference's order (reaction, then
+//    slot);
+//  - one term per group of reactions with a frozen reactant that share their varying factor (the
+//    masked reactant's xn to its power, or none when every reactant is frozen or gamma): the
+//    group's constant, the sum over its reactions of coefficient * (1/k2!) * rate * the frozen
+//    reactant's xn (to the power k2 for the first reactant), formed once per step. A group sums in
+//    another order than the reference's loop, which changes the row's sum at the rounding level.
+// Groups are found deterministically: a row's static list is cut into pieces of kRhsPiece items,
+// a warp sums each piece's items per key (a fixed butterfly per key and chunk of 32 items, then the
+// chunks in order), and a warp per row sums its pieces' groups in piece order.
 __device__ __forceinline__ void put_rhs_item(const DevNet &N, const Ws &W, Act &A, const int *sys2c, int q, int a,
                                              int m) {
   const int *k = N.act_k + (size_t)a * 8;
@@ -1004,44 +972,223 @@ __device__ __forceinline__ void put_rhs_item(const DevNet &N, const Ws &W, Act &
   A.grpk[q] = i1 | (i2 << 14) | ((uint32_t)k[1] << 28);
 }
 
+// Item (a, m) of a masked row: -1 if every reactant of reaction a is masked or gamma (a term of
+// its own); otherwise its group key, (compact row of the masked reactant << 3) | its power, or
+// (na << 3) | 1 for a constant flux, and in val its constant coefficient * (1/k2!) v * frozen xn.
+// spc: species -> compact row, -1 if frozen (gamma included).
+__device__ __forceinline__ int rhs_item_key(const DevNet &N, const Ws &W, const int *spc, int na, int a, int m,
+                                            double &val) {
+  const int4 *kp = reinterpret_cast<const int4 *>(N.act_k + (size_t)a * 8);
+  const int4 k0 = kp[0], k1 = kp[1];
+  const int g = N.ig, r1 = k0.x, k2 = k0.y, r2 = k0.z;
+  const int c1 = spc[r1], c2 = r2 == g ? na : spc[r2];
+  const bool m1 = c1 >= 0, m2 = c2 >= 0;
+  if (m1 && m2) return -1;
+  double cf = c_fact[k2] * W.v[N.act_slot[a]];  // the reference's order: ((1/k2!) v) xn1^k2 xn2
+  if (!m1) cf = cf * powi(W.xn[r1], k2);
+  if (!m2) cf = cf * W.xn[r2];
+  const double coef = m == 0 ? (double)(-k2) : m == 1 ? -1.0 : m == 2 ? (double)k1.y : (double)k1.w;
+  val = coef * cf;
+  if (m1) return (c1 << 3) | k2;
+  if (m2 && c2 < na) return (c2 << 3) | 1;  // the second reactant masked (not gamma)
+  return (na << 3) | 1;  // every reactant frozen or gamma: a constant flux
+}
+
+// Register groups of a warp: lane i holds group i (key gk, -1 if unused, and sum gs); ng groups are
+// in use (warp-uniform). The warp's 32 (key, val) pairs (key < 0: none) are added: the values of
+// one key are summed by a butterfly, which gives every lane the same bits whatever their order, then
+// added to their group; keys are taken in the order of their first lane, so the sums and the groups'
+// order depend only on the positions of the items. A 33rd key sets ovf (the caller then groups the
+// same pairs again through the workspace accumulator below).
+__device__ __forceinline__ void group_chunk_reg(int key, double val, int &gk, double &gs, int &ng, bool &ovf) {
+  const int lane = threadIdx.x & 31;
+  unsigned pend = __ballot_sync(NUPPN_FULL, key >= 0);
+  while (pend) {
+    const int k0 = __shfl_sync(NUPPN_FULL, key, __ffs(pend) - 1);
+    const bool mine = key == k0;
+    double v = mine ? val : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(NUPPN_FULL, v, o);
+    const unsigned hit = __ballot_sync(NUPPN_FULL, gk == k0);
+    if (hit) {
+      if (lane == __ffs(hit) - 1) gs += v;
+    } else if (ng < 32) {
+      if (lane == ng) {
+        gk = k0;
+        gs = v;
+      }
+      ++ng;
+    } else {
+      ovf = true;
+    }
+    pend &= ~__ballot_sync(NUPPN_FULL, mine);
+  }
+}
+
+// Per-warp key accumulator in the CTA's workspace: acc[key] the running sum of a key, tag[key] 1 once
+// the key has a value in the current piece or row, list[] the keys in the order they first came.
+// Entries are zero outside the keys in the list, which are cleared when the list is emitted.
+struct KeyAcc {
+  double *acc;
+  int *tag, *list;
+};
+
+// The warp's 32 (key, val) pairs (key < 0: none) added to its accumulator. The values of one key
+// are summed by a butterfly, which gives every lane the same bits whatever their order, then lane 0
+// adds the sum to acc[key]; keys are taken in the order of their first lane, so the sums and the
+// order of the list depend only on the positions of the items. n: keys in the list (warp-uniform).
+__device__ __forceinline__ void group_chunk(int key, double val, const KeyAcc &K, int &n) {
+  const int lane = threadIdx.x & 31;
+  unsigned pend = __ballot_sync(NUPPN_FULL, key >= 0);
+  while (pend) {
+    const int k0 = __shfl_sync(NUPPN_FULL, key, __ffs(pend) - 1);
+    const bool mine = key == k0;
+    double v = mine ? val : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(NUPPN_FULL, v, o);
+    int fresh = 0;
+    if (lane == 0) {
+      if (K.tag[k0] == 0) {
+        K.tag[k0] = 1;
+        K.list[n] = k0;
+        K.acc[k0] = v;
+        fresh = 1;
+      } else {
+        K.acc[k0] = K.acc[k0] + v;
+      }
+    }
+    n += __shfl_sync(NUPPN_FULL, fresh, 0);
+    pend &= ~__ballot_sync(NUPPN_FULL, mine);
+  }
+}
+
+// The accumulator's n keys and sums written to key[i], val[i] (i < n) and cleared.
+__device__ __forceinline__ void group_emit(const KeyAcc &K, int n, int *key, double *val) {
+  __syncwarp();  // lane 0's accumulator writes are visible to the warp
+  for (int i = threadIdx.x & 31; i < n; i += 32) {
+    const int k = K.list[i];
+    key[i] = k;
+    val[i] = K.acc[k];
+    K.acc[k] = 0.0;
+    K.tag[k] = 0;
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ void put_group_item(Act &A, int q, int key, double sum) {
+  A.gcoef[q] = 1.0f;
+  A.grcv[q] = sum;
+  A.grpk[q] = (uint32_t)(key >> 3) | ((uint32_t)A.na << 14) | ((uint32_t)(key & 7) << 28);
+}
+
+// The groups of the items key[0..n) (-1: none), written over key[0..groups) and val[0..groups);
+// returns the number of groups. A first pass groups in registers; if the items hold more than 32
+// keys it only reads, and a second pass groups them through the workspace accumulator instead.
+__device__ __forceinline__ int group_items(int *key, double *val, int n, const KeyAcc &K) {
+  const int lane = threadIdx.x & 31;
+  int gk = -1, ng = 0;
+  double gs = 0.0;
+  bool ovf = false;
+  for (int b = 0; b < n && !ovf; b += 32) {
+    const bool in = b + lane < n;
+    group_chunk_reg(in ? key[b + lane] : -1, in ? val[b + lane] : 0.0, gk, gs, ng, ovf);
+  }
+  __syncwarp();
+  if (!ovf) {
+    if (lane < ng) {
+      key[lane] = gk;
+      val[lane] = gs;
+    }
+    __syncwarp();
+    return ng;
+  }
+  int nk = 0;
+  for (int b = 0; b < n; b += 32) {
+    const bool in = b + lane < n;
+    group_chunk(in ? key[b + lane] : -1, in ? val[b + lane] : 0.0, K, nk);
+  }
+  group_emit(K, nk, key, val);
+  return nk;
+}
+
 __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem, size_t smem_bytes, int *sint) {
   const int tid = GT, nt = GN, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
   const int *sys2c = W.act_tmp;              // system index -> active row (dev_compact), -1 if frozen
-  int *cnt = W.act_tmp + 2 * (N.nsys + 1);   // [na+1] items per row, then row offsets
-  int *off = W.act_tmp + 3 * (N.nsys + 1);   // [na+1] offsets of the short rows' static lists
-  int *flag = W.act_itmp;                    // [T+1] kept flags, then positions
-  const int g = N.ig, na = A.na;
+  int *cnt = W.act_tmp + 2 * (N.nsys + 1);   // [na+1] gather items per row, then row offsets
+  int *off = W.act_tmp + 3 * (N.nsys + 1);   // [na+1] offsets of the rows' static lists
+  int *flag = W.act_itmp;                    // [T+1] own-term flags, then their positions
+  int *fkey = W.rhs_key;                     // [T] group key of each item (-1: own term), then groups
+  double *fval = W.rhs_val;                  // [T] its value, then group sums
+  int *pofs = W.rhs_piece;                   // [na+1] first piece of each row
+  int *pcnt = W.rhs_piece + (N.nsys + 1);    // [pieces] groups of each piece
+  int *spc = W.rhs_spc;                      // [nsp] species -> active row, -1 if frozen
+  const int na = A.na, nkey = (na + 1) << 3;
+  const size_t kw = (size_t)w * kRhsKeysPerRow * (N.nsys + 1);  // this warp's accumulator
+  const KeyAcc K = {W.rhs_acc + kw, W.rhs_tag + kw, W.rhs_list + kw};
+  for (int i = lane; i < nkey; i += 32) {  // the workspace may hold anything: clear the keys of na rows
+    K.acc[i] = 0.0;
+    K.tag[i] = 0;
+  }
+  for (int sp = tid; sp < N.nsp; sp += nt) {
+    const int q = N.sys_of_sp[sp];
+    spc[sp] = q >= 0 ? sys2c[q] : -1;
+  }
   for (int c = tid; c < na; c += nt) {
-    const int s = N.sp_of_sys[A.arow[c]];
-    const int len = N.dg_ptr[s + 1] - N.dg_ptr[s];
-    off[c] = len <= kLongList ? len : 0;
+    const int sp = N.sp_of_sys[A.arow[c]];
+    const int len = N.dg_ptr[sp + 1] - N.dg_ptr[sp];
+    off[c] = len;
+    pofs[c] = (len + kRhsPiece - 1) / kRhsPiece;
   }
   GSYNC();
   const int T = block_scan_excl(off, na, sint);
-  if (tid == 0) off[na] = T;
+  const int NP = block_scan_excl(pofs, na, sint);
+  if (tid == 0) {
+    off[na] = T;
+    pofs[na] = NP;
+  }
   GSYNC();
-  for (int t = tid; t < T; t += nt) {  // flattened static lists of the short rows
-    const int c = seg_of(off, na, t);
-    const int a = N.dg_item[N.dg_ptr[N.sp_of_sys[A.arow[c]]] + (t - off[c])] >> 2;
-    const int *k = N.act_k + (size_t)a * 8;
-    flag[t] = (W.mask[k[0]] && (k[2] == g || W.mask[k[2]])) ? 1 : 0;
+  // each piece (a warp): its items classified, own-term flags set, frozen-reactant items grouped
+  for (int P = w; P < NP; P += nw) {
+    const int c = seg_of(pofs, na, P);
+    const int t0 = off[c] + (P - pofs[c]) * kRhsPiece, t1 = min(t0 + kRhsPiece, off[c + 1]);
+    const int *items = N.dg_item + N.dg_ptr[N.sp_of_sys[A.arow[c]]] - off[c];
+    for (int t = t0 + lane; t < t1; t += 32) {
+      const int it = items[t];
+      double val = 0.0;
+      const int key = rhs_item_key(N, W, spc, na, it >> 2, it & 3, val);
+      flag[t] = key < 0 ? 1 : 0;
+      fkey[t] = key;
+      fval[t] = val;
+    }
+    __syncwarp();
+    const int n = group_items(fkey + t0, fval + t0, t1 - t0, K);
+    if (lane == 0) pcnt[P] = n;
   }
   GSYNC();
   const int nS = block_scan_excl(flag, T, sint);
   if (tid == 0) flag[T] = nS;
   GSYNC();
-  for (int c = tid; c < na; c += nt) cnt[c] = flag[off[c + 1]] - flag[off[c]];  // 0 for long rows
-  GSYNC();
-  for (int c = w; c < na; c += nw) {  // long rows: count their slots among the kept reactions
-    const int s = N.sp_of_sys[A.arow[c]];
-    if (N.dg_ptr[s + 1] - N.dg_ptr[s] <= kLongList) continue;
-    int n = 0;
-    for (int i = lane; i < A.nK; i += 32) {
-      const int *k = N.act_k + (size_t)A.Klist[i] * 8;
-      n += (k[0] == s) + (k[2] == s) + (k[4] == s) + (k[6] == s);
+  for (int c = w; c < na; c += nw) {  // rows of several pieces: their pieces' groups grouped again
+    const int npc = pofs[c + 1] - pofs[c];
+    int n = npc == 1 ? pcnt[pofs[c]] : 0;
+    if (npc > 1) {
+      // move the pieces' groups together at the row's start, in piece order, then group them
+      for (int P = pofs[c]; P < pofs[c + 1]; ++P) {
+        const int s0 = off[c] + (P - pofs[c]) * kRhsPiece, np = pcnt[P];
+        for (int b = 0; b < np; b += 32) {  // s0 >= off[c] + n: moves go down or stay
+          const int i = b + lane;
+          const int k = i < np ? fkey[s0 + i] : -1;
+          const double v = i < np ? fval[s0 + i] : 0.0;
+          __syncwarp();
+          if (i < np) {
+            fkey[off[c] + n + i] = k;
+            fval[off[c] + n + i] = v;
+          }
+          __syncwarp();
+        }
+        n += np;
+      }
+      n = group_items(fkey + off[c], fval + off[c], n, K);
     }
-    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(NUPPN_FULL, n, o);
-    if (lane == 0) cnt[c] = n;
+    if (lane == 0) cnt[c] = (flag[off[c + 1]] - flag[off[c]]) + n;
   }
   GSYNC();
   const int ngi = block_scan_excl(cnt, na, sint);
@@ -1061,31 +1208,16 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
   A.gterm = (double *)base;
   A.ngi = ngi;
   for (int c = tid; c <= na; c += nt) A.gptr[c] = c < na ? cnt[c] : ngi;
-  for (int t = tid; t < T; t += nt) {
+  for (int t = tid; t < T; t += nt) {  // own terms first, in the static list's order
     if (flag[t + 1] == flag[t]) continue;
     const int c = seg_of(off, na, t);
     const int it = N.dg_item[N.dg_ptr[N.sp_of_sys[A.arow[c]]] + (t - off[c])];
     put_rhs_item(N, W, A, sys2c, cnt[c] + flag[t] - flag[off[c]], it >> 2, it & 3);
   }
-  for (int c = w; c < na; c += nw) {  // long rows: their terms in the order of K, then slot
-    const int s = N.sp_of_sys[A.arow[c]];
-    if (N.dg_ptr[s + 1] - N.dg_ptr[s] <= kLongList) continue;
-    int base_q = cnt[c];
-    for (int i0 = 0; i0 < A.nK; i0 += 32) {
-      const int i = i0 + lane;
-      const int a = i < A.nK ? A.Klist[i] : -1;
-      const int *k = N.act_k + (size_t)(a < 0 ? 0 : a) * 8;
-      const int n = a < 0 ? 0 : (k[0] == s) + (k[2] == s) + (k[4] == s) + (k[6] == s);
-      int incl = n;
-      for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(NUPPN_FULL, incl, o);
-        if (lane >= o) incl += v;
-      }
-      int q = base_q + incl - n;
-      for (int m = 0; m < 4 && n > 0; ++m)
-        if (k[2 * m] == s) put_rhs_item(N, W, A, sys2c, q++, a, m);
-      base_q += __shfl_sync(NUPPN_FULL, incl, 31);
-    }
+  for (int c = w; c < na; c += nw) {  // then the row's groups
+    const int own = flag[off[c + 1]] - flag[off[c]];
+    const int q0 = cnt[c] + own, ng = (c + 1 < na ? cnt[c + 1] : ngi) - q0;
+    for (int i = lane; i < ng; i += 32) put_group_item(A, q0 + i, fkey[off[c] + i], fval[off[c] + i]);
   }
   GSYNC();
 }

@@ -232,7 +232,18 @@ WsLayout layout(const HostNet &H) {
     L.act_btmp = take(njg);
     L.bd = take((size_t)(2 * kMaxLevels + 8) * H.nsys * sizeof(double));
   }
-  L.rx = take(((size_t)H.nsys + 1 + 5 * ((size_t)H.nact + 1)) * sizeof(int));
+  {
+    const size_t ngi = H.dg_item.size();
+    L.rhs_key = take(ngi * sizeof(int));
+    L.rhs_val = take(ngi * sizeof(double));
+    L.rhs_piece = take((2 * ((size_t)H.nsys + 1) + ngi / kRhsPiece + 1) * sizeof(int));
+    const size_t keys = (size_t)kRhsWarps * kRhsKeysPerRow * ((size_t)H.nsys + 1);
+    L.rhs_acc = take(keys * sizeof(double));
+    L.rhs_tag = take(keys * sizeof(int));
+    L.rhs_list = take(keys * sizeof(int));
+    L.rhs_spc = take((size_t)H.nsp * sizeof(int));
+    L.jac_long = take(3 * ((size_t)H.nnzLU + 1) * sizeof(int));
+  }
   L.nse = take((5 * (size_t)H.nsp + (size_t)H.nse_p2) * sizeof(double));
   L.nse_stride = (size_t)H.nsp;
   L.bytes = t;

@@ -10,6 +10,9 @@
 namespace nuppn {
 
 constexpr int kMaxLevels = 8;       // Bader-Deuflhard tableau columns (bader_deuflhard.F90:24)
+constexpr int kRhsPiece = 256;      // right-hand side items per piece when grouping frozen-reactant terms
+constexpr int kRhsKeysPerRow = 8;   // group keys per active row: (row << 3) | power of its xn
+constexpr int kRhsWarps = 8;        // warps of a zone group at most (256 threads), one key accumulator each
 constexpr int kPartDim = 24;        // partition-function temperature points (array_sizes.F90:15)
 
 // Network as the device sees it: every pointer is device memory, read-only during solves.
@@ -99,7 +102,10 @@ struct WsLayout {
   size_t act_tmp, act;           // compaction scratch (ints) and the global fallback of the active LU
   size_t act_r;                  // global fall-back of the restricted right-hand side
   size_t act_itmp, act_otmp, act_dtmp, act_btmp, bd;  // flattened-gather scratch, compact BD vectors
-  size_t rx;                     // active-reaction lists: offsets, flags, kept and passing reactions
+  size_t rhs_key, rhs_val, rhs_piece;  // grouping of the right-hand side's frozen-reactant terms
+  size_t rhs_acc, rhs_tag, rhs_list;   // per-warp key accumulators of that grouping
+  size_t rhs_spc;                      // species -> active row of the step
+  size_t jac_long;                     // long Jacobian entries of the step and their pieces
   size_t nse;                    // NSE work arrays [5 * nsp + nse_p2] doubles
   size_t nse_stride;             // nsp: the length of each NSE work array but the last
   size_t bytes;

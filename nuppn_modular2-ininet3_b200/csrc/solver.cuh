@@ -71,7 +71,13 @@ struct Ws {
   int *act_tmp;  // compaction scratch: sys2c, arow, counts
   char *act;     // global fallback of the active-subsystem LU
   char *act_r;   // global fallback of the restricted right-hand side
-  int *rx;       // active-reaction lists [nsys+1 + 5*(nact+1)]
+  int *rhs_key;       // right-hand side items' group keys, then group keys [dg items]
+  double *rhs_val;    // their values, then group sums [dg items]
+  int *rhs_piece;     // first piece of each active row [nsys+1], groups of each piece
+  double *rhs_acc;    // key accumulators of the grouping, one per warp [warps * 8 * (nsys+1)]
+  int *rhs_spc;       // species -> active row of the current step, -1 if frozen [nsp]
+  int *jac_long;      // long Jacobian entries: flags, positions, first pieces [3 * (nnzLU + 1)]
+  int *rhs_tag, *rhs_list;
   double *nse_x, *nse_gtot, *nse_mc, *nse_lm, *nse_y1, *nse_sort;  // NSE work arrays
   int *act_itmp; // flattened-list flags / positions [max(list items) + 1]
   int *act_otmp; // segment offsets of the active Jacobian entries [nnzLU + 1]
@@ -97,7 +103,14 @@ __device__ __forceinline__ Ws ws_bind(char *base, const WsLayout &L) {
   w.act_tmp = (int *)(base + L.act_tmp);
   w.act = base + L.act;
   w.act_r = base + L.act_r;
-  w.rx = (int *)(base + L.rx);
+  w.rhs_key = (int *)(base + L.rhs_key);
+  w.rhs_val = (double *)(base + L.rhs_val);
+  w.rhs_piece = (int *)(base + L.rhs_piece);
+  w.rhs_acc = (double *)(base + L.rhs_acc);
+  w.rhs_spc = (int *)(base + L.rhs_spc);
+  w.jac_long = (int *)(base + L.jac_long);
+  w.rhs_tag = (int *)(base + L.rhs_tag);
+  w.rhs_list = (int *)(base + L.rhs_list);
   w.nse_x = (double *)(base + L.nse);
   w.nse_gtot = w.nse_x + L.nse_stride;
   w.nse_mc = w.nse_gtot + L.nse_stride;

@@ -187,6 +187,7 @@ double akima_eval(const Akima &ai, int npt, const double *xpt, double xx_in) {  
 // ---- network -----------------------------------------------------------------------------------
 struct Net {
   nuppn_knobs kn;
+  int rhs_noise = -1;  // >= 0: seed of the dX/dt rounding perturbation (oracle_set_rhs_noise), else off
   int nsp, nre, ig;
   vector<double> an, zn, exmass, gspin;
   vector<uint8_t> ciso, crea;
@@ -321,6 +322,7 @@ struct Zone {
   vector<double> nse_x, nse_gtot, nse_mucoul, lm_ov_a;
   double mu_p_coul = 0.0, nse_mu[2] = {0.0, 0.0}, nse_mu_last[2] = {-9.0, -9.0}, nse_the = 0.0, nse_phi = 0.0;
   bool nse_first = true;
+  unsigned long long noise = 0;  // generator state of the dX/dt perturbation (oracle_set_rhs_noise)
   // stats
   nuppn_zone_stats st;
   explicit Zone(const Net *n) : N(n) {
@@ -709,6 +711,26 @@ void evaluate_all_rates(Zone &Z, double ye, double rho, double t9, const double 
 // ---- RHS and Jacobian --------------------------------------------------------------------------
 const double fact[5] = {ONE, ONE, HALF, SIXTH, ONE / 24.0};
 
+// Test infrastructure, off unless oracle_set_rhs_noise was called: every dX/dt entry scaled by
+// 1 - 2^-52, 1 or 1 + 2^-52 at random, a change of the size of one rounding of the sum. An
+// implementation that sums the same terms in another order differs from the reference by such
+// amounts; the spread of the checker's results under this perturbation is how far the reference's
+// own answer depends on them. Each zone draws from its own generator (seed, zone), so results do not
+// depend on the thread count.
+static unsigned long long noise_state(int seed, int z) {
+  unsigned long long x = 0x9E3779B97F4A7C15ull * (unsigned long long)(seed + 1) + 0xD1B54A32D192ED03ull * (unsigned long long)(z + 1);
+  x ^= x >> 31;
+  return x | 1ull;
+}
+
+static void rhs_perturb(Zone &Z) {
+  for (int i = 0; i < Z.N->nsp; ++i) {
+    Z.noise = Z.noise * 6364136223846793005ull + 1442695040888963407ull;
+    const int u = (int)((Z.noise >> 33) % 3ull) - 1;
+    Z.dxdt[i] = Z.dxdt[i] * (1.0 + u * 2.220446049250313e-16);
+  }
+}
+
 void calculate_dxdt(Zone &Z, const double *x_in) {  // jac_rhs.F90:217-278
   const Net &N = *Z.N;
   std::fill(Z.dxdt.begin(), Z.dxdt.end(), 0.0);
@@ -730,6 +752,7 @@ void calculate_dxdt(Zone &Z, const double *x_in) {  // jac_rhs.F90:217-278
     if (N.ciso[i]) Z.dxdt[i] = Z.dxdt[i] * N.an[i];
   Z.xn[N.ig] = ZERO;
   Z.dxdt[N.ig] = ZERO;
+  if (N.rhs_noise >= 0) rhs_perturb(Z);
 }
 
 void calculate_jacobian(Zone &Z, double dzeit, const double *x_in) {  // jac_rhs.F90:282-455
@@ -1817,6 +1840,7 @@ int oracle_integrate(void *net, int32_t nz, double *X, int32_t ldx, const double
       int z = next.fetch_add(1);
       if (z >= nz) break;
       Zone Zn(N);
+      if (N->rhs_noise >= 0) Zn.noise = noise_state(N->rhs_noise, z);
       double yez = ye[z];
       ierr[z] = integrate_zone(Zn, X + (size_t)z * ldx, t9_0[z], t9_1[z], rho_0[z], rho_1[z], yez, dtwant[z],
                                bd_state ? bd_state + z : nullptr);
@@ -1856,6 +1880,7 @@ int oracle_integrate_trajectories(void *net, int32_t nz, int32_t npts, double *X
       const int z = next.fetch_add(1);
       if (z >= nz) break;
       Zone Zn(N);
+      if (N->rhs_noise >= 0) Zn.noise = noise_state(N->rhs_noise, z);
       double *y = X + (size_t)z * ldx;
       const double *tt = time + (size_t)z * npts, *tp = t9 + (size_t)z * npts, *tr = rho + (size_t)z * npts;
       if (std::fabs(ONE - sortedsum(y, N->nsp)) > 1.e-8) {  // check_2d_mass_cons(.true.), renorm_2d
@@ -1906,5 +1931,6 @@ int oracle_nse(void *net, int32_t nz, const double *t9, const double *rho, const
   return 0;
 }
 double oracle_sortedsum(const double *a, int32_t n) { return sortedsum(a, n); }
+void oracle_set_rhs_noise(void *net, int32_t seed) { ((Net *)net)->rhs_noise = seed < 0 ? -1 : seed; }
 
 }  // extern "C"

@@ -238,3 +238,33 @@ def test_no_cpu_fallback_in_product(solver_mod):
         if f.endswith(".py"):
             src = open(os.path.join(pkgdir, f)).read()
             assert "oracle" not in src.replace("reference", ""), f
+
+
+def test_oracle_rhs_noise_is_seeded_and_shows_hburn_sensitivity(orc, abi, wl):
+    """The checker's dX/dt perturbation (a rounding-sized change of every entry, the freedom any
+    implementation that sums the terms in another order has): off by default and after it is
+    switched off, deterministic per seed and independent of the thread count. Cool H-burning zones
+    (300 species, T9 0.02-0.05, 1e10 s) move by far more than 1e-6 under it, which is why the
+    parity bar for such zones is the checker's spread under both perturbations."""
+    net = wl.network(300)
+    hb, _ = wl.hburn_zone(net)
+    n = 6
+    t9 = np.linspace(0.02, 0.05, n)
+    rho = np.full(n, 100.0)
+    X = np.repeat(hb.X, n, axis=0)
+    ye = np.repeat(hb.ye, n)
+    ref = orc.Oracle(net, abi.default_knobs(integration_method=1))
+    run = lambda nt: ref.integrate_network(X, t9, t9, rho, rho, ye, np.full(n, 1e10), nthreads=nt)
+    X0, _, ie0, _, _ = run(3)
+    ref.set_rhs_noise(7)
+    Xa, _, iea, _, _ = run(1)
+    Xb, _, ieb, _, _ = run(3)
+    ref.set_rhs_noise(None)
+    Xc, _, _, _, _ = run(2)
+    assert np.array_equal(Xa, Xb) and np.array_equal(iea, ieb)  # per-zone generators
+    assert np.array_equal(Xc, X0)  # off again
+    ok = (ie0 == 0) & (iea == 0)
+    assert ok.sum() >= 3
+    big = X0 > 1e-12
+    rel = np.where(big, np.abs(Xa - X0) / np.where(big, X0, 1.0), 0.0).max(axis=1)
+    assert (rel[ok] > 1e-6).any(), rel
