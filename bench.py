@@ -10,7 +10,8 @@ the same initial state. The metric counts accepted sub-steps (zone-timesteps) pe
 
 --impl reference times the reference's own algorithm on the host cores (the CPU restatement of
 NuPPN's FP64 path, calling the reference's SuperLU) on a bounded sample of the same workload.
-For N > 1 (torchrun) the zones are sharded across ranks; there is no collective on the data path.
+For N > 1 (torchrun) the zones are sharded across ranks, balanced by peak temperature (snake order);
+there is no collective on the data path.
 """
 from __future__ import annotations
 
@@ -224,8 +225,9 @@ def run_traj(args, rank, world, local):
     abi = importlib.import_module(PKG + ".abi")
     net = wl.network(1107)
     tr_all = wl.trajectory_batch(args.nz * world, net=net, npts=201)
-    sel = importlib.import_module(PKG + ".sharding").zone_shard(args.nz, rank)
-    tt, t9, rho = (g[sel] for g in tr_all.grids())
+    grids = tr_all.grids()
+    sel = importlib.import_module(PKG + ".sharding").snake_shards(grids[1].max(axis=1), world)[rank]
+    tt, t9, rho = (g[sel] for g in grids)
     X0, ye0 = tr_all.X0[sel], tr_all.ye0[sel]
     cfg = {"workload": "tppnp-traj-1107 201 points to 10 s", "trajectories": args.nz * world,
            "trajectories_per_gpu": args.nz, "network_species": net.nsp, "integrator": "bader-deuflhard",
@@ -730,7 +732,8 @@ def main():
     solver = importlib.import_module(PKG + ".solver")
     net = wl.network(1107)
     zb_all = wl.heshell_batch(args.nz * world, net=net, seed=2)
-    zb = zb_all.take(importlib.import_module(PKG + ".sharding").zone_shard(args.nz, rank))  # weak scaling
+    hot = np.maximum(zb_all.t9_0, zb_all.t9_1)  # weak scaling, shards balanced by peak temperature
+    zb = zb_all.take(importlib.import_module(PKG + ".sharding").snake_shards(hot, world)[rank])
     knobs = abi.default_knobs(integration_method=1)
     S = solver.NetworkSolver(net, knobs, device=dev_id)
     nz = zb.nz
@@ -826,7 +829,8 @@ def cpu_baseline(net, zb, nzones, dev_out):
     """The checker on the host cores, on a fixed sample of the same workload (the 8 hottest zones and
     evenly spaced others): its throughput, and the device results of those zones against it
     (dev_out = final X, ierr and accepted steps of every zone from the last timed call). Zones beyond
-    1e-6 are also measured against the checker's own spread under 1-ulp changes of their input."""
+    1e-6 are also measured against the checker's own spread under 1-ulp changes of their input and
+    rounding-sized changes of its dX/dt."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
     import parity
@@ -854,7 +858,8 @@ def cpu_baseline(net, zb, nzones, dev_out):
         spread[off] = parity.checker_spread(ref, sub.take(off), Xr[off], nthreads=cores)
     err = parity.summary(X, ierr, nsucc, Xr, ierr_r, nsucc_r, spread)
     err["sample"] = f"{len(idx)} zones: the 8 hottest and evenly spaced others"
-    err["spread"] = "per zone beyond 1e-6: max relative change of the checker under +-1-ulp input changes, 2 draws"
+    err["spread"] = ("per zone beyond 1e-6: max relative change of the checker under +-1-ulp input changes (2 draws) "
+                     "and under +-2^-52 changes of every dX/dt entry (2 draws)")
     return base, err
 
 
