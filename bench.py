@@ -829,8 +829,8 @@ def cpu_baseline(net, zb, nzones, dev_out):
     """The checker on the host cores, on a fixed sample of the same workload (the 8 hottest zones and
     evenly spaced others): its throughput, and the device results of those zones against it
     (dev_out = final X, ierr and accepted steps of every zone from the last timed call). Zones beyond
-    1e-6 are also measured against the checker's own spread under 1-ulp changes of their input and
-    rounding-sized changes of its dX/dt."""
+    1e-6 are also measured against the checker's own spread under 1-ulp changes of their input,
+    rounding-sized changes of its dX/dt and another elimination order of its LU."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
     import parity
@@ -858,8 +858,8 @@ def cpu_baseline(net, zb, nzones, dev_out):
         spread[off] = parity.checker_spread(ref, sub.take(off), Xr[off], nthreads=cores)
     err = parity.summary(X, ierr, nsucc, Xr, ierr_r, nsucc_r, spread)
     err["sample"] = f"{len(idx)} zones: the 8 hottest and evenly spaced others"
-    err["spread"] = ("per zone beyond 1e-6: max relative change of the checker under +-1-ulp input changes (2 draws) "
-                     "and under +-2^-52 changes of every dX/dt entry (2 draws)")
+    err["spread"] = ("per zone beyond 1e-6: max relative change of the checker under +-1-ulp input changes, "
+                     "+-2^-52 changes of every dX/dt entry, and another SuperLU elimination order (2 draws each)")
     return base, err
 
 

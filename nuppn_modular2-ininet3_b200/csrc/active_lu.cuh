@@ -972,55 +972,63 @@ __device__ __forceinline__ void put_rhs_item(const DevNet &N, const Ws &W, Act &
   A.grpk[q] = i1 | (i2 << 14) | ((uint32_t)k[1] << 28);
 }
 
-// Item (a, m) of a masked row: -1 if every reactant of reaction a is masked or gamma (a term of
-// its own); otherwise its group key, (compact row of the masked reactant << 3) | its power, or
-// (na << 3) | 1 for a constant flux, and in val its constant coefficient * (1/k2!) v * frozen xn.
-// spc: species -> compact row, -1 if frozen (gamma included).
-__device__ __forceinline__ int rhs_item_key(const DevNet &N, const Ws &W, const int *spc, int na, int a, int m,
-                                            double &val) {
-  const int4 *kp = reinterpret_cast<const int4 *>(N.act_k + (size_t)a * 8);
-  const int4 k0 = kp[0], k1 = kp[1];
-  const int g = N.ig, r1 = k0.x, k2 = k0.y, r2 = k0.z;
-  const int c1 = spc[r1], c2 = r2 == g ? na : spc[r2];
-  const bool m1 = c1 >= 0, m2 = c2 >= 0;
-  if (m1 && m2) return -1;
-  double cf = c_fact[k2] * W.v[N.act_slot[a]];  // the reference's order: ((1/k2!) v) xn1^k2 xn2
-  if (!m1) cf = cf * powi(W.xn[r1], k2);
-  if (!m2) cf = cf * W.xn[r2];
-  const double coef = m == 0 ? (double)(-k2) : m == 1 ? -1.0 : m == 2 ? (double)k1.y : (double)k1.w;
-  val = coef * cf;
-  if (m1) return (c1 << 3) | k2;
-  if (m2 && c2 < na) return (c2 << 3) | 1;  // the second reactant masked (not gamma)
-  return (na << 3) | 1;  // every reactant frozen or gamma: a constant flux
-}
-
-// Register groups of a warp: lane i holds group i (key gk, -1 if unused, and sum gs); ng groups are
-// in use (warp-uniform). The warp's 32 (key, val) pairs (key < 0: none) are added: the values of
-// one key are summed by a butterfly, which gives every lane the same bits whatever their order, then
-// added to their group; keys are taken in the order of their first lane, so the sums and the groups'
-// order depend only on the positions of the items. A 33rd key sets ovf (the caller then groups the
-// same pairs again through the workspace accumulator below).
-__device__ __forceinline__ void group_chunk_reg(int key, double val, int &gk, double &gs, int &ng, bool &ovf) {
-  const int lane = threadIdx.x & 31;
-  unsigned pend = __ballot_sync(NUPPN_FULL, key >= 0);
-  while (pend) {
-    const int k0 = __shfl_sync(NUPPN_FULL, key, __ffs(pend) - 1);
-    const bool mine = key == k0;
-    double v = mine ? val : 0.0;
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(NUPPN_FULL, v, o);
-    const unsigned hit = __ballot_sync(NUPPN_FULL, gk == k0);
-    if (hit) {
-      if (lane == __ffs(hit) - 1) gs += v;
-    } else if (ng < 32) {
-      if (lane == ng) {
-        gk = k0;
-        gs = v;
-      }
-      ++ng;
-    } else {
-      ovf = true;
+// Items [t0, t1) of a masked row's static list (items[t] = reaction a << 2 | slot m, coefs[t] the
+// slot's coefficient -k2, -1, k6 or k8), classified by one warp, four items per lane at a time with
+// their loads issued together. An item whose reactants are all masked or gamma is a term of its own
+// (flag 1, key -1); otherwise its group key is (compact row of its masked reactant << 3) | that
+// reactant's power, or (na << 3) | 1 when every reactant is frozen or gamma (a constant flux), and
+// its value is coefficient * (1/k2!) v * the frozen reactants' xn (xn1^k2, xn2), in the reference's
+// order of products. spc: species -> compact row, -1 if frozen (gamma included).
+__device__ __forceinline__ void rhs_classify(const DevNet &N, const Ws &W, const int *spc, int na, const int *items,
+                                             const double *coefs, int t0, int t1, int *flag, int *fkey, double *fval) {
+  const int lane = threadIdx.x & 31, g = N.ig;
+  const int4 *kp = reinterpret_cast<const int4 *>(N.act_k);
+  for (int b = t0; b < t1; b += 128) {
+    int it[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int t = b + lane + 32 * i;
+      it[i] = t < t1 ? items[t] : -1;
     }
-    pend &= ~__ballot_sync(NUPPN_FULL, mine);
+    int4 k[4];
+    int sl[4];
+    double co[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int a = it[i] < 0 ? 0 : it[i] >> 2;
+      k[i] = kp[2 * (size_t)a];
+      sl[i] = N.act_slot[a];
+      co[i] = coefs[it[i] < 0 ? t0 : b + lane + 32 * i];
+    }
+    int c1[4], c2[4];
+    double v[4], x1[4], x2[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      c1[i] = spc[k[i].x];
+      c2[i] = k[i].z == g ? na : spc[k[i].z];
+      v[i] = W.v[sl[i]];
+      x1[i] = W.xn[k[i].x];
+      x2[i] = W.xn[k[i].z];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int t = b + lane + 32 * i;
+      if (it[i] < 0) continue;
+      const bool m1 = c1[i] >= 0, m2 = c2[i] >= 0;
+      int key = -1;
+      double val = 0.0;
+      if (!(m1 && m2)) {
+        const int k2 = k[i].y;
+        double cf = c_fact[k2] * v[i];
+        if (!m1) cf = cf * powi(x1[i], k2);
+        if (!m2) cf = cf * x2[i];
+        val = co[i] * cf;
+        key = m1 ? (c1[i] << 3) | k2 : (m2 && c2[i] < na ? (c2[i] << 3) | 1 : (na << 3) | 1);
+      }
+      flag[t] = key < 0 ? 1 : 0;
+      fkey[t] = key;
+      fval[t] = val;
+    }
   }
 }
 
@@ -1080,19 +1088,52 @@ __device__ __forceinline__ void put_group_item(Act &A, int q, int key, double su
 }
 
 // The groups of the items key[0..n) (-1: none), written over key[0..groups) and val[0..groups);
-// returns the number of groups. A first pass groups in registers; if the items hold more than 32
-// keys it only reads, and a second pass groups them through the workspace accumulator instead.
+// returns the number of groups. Up to 32 keys: lane i holds the i-th key (in the order of first
+// appearance), every lane adds its own items (the n items taken 32 at a time, lane l the l-th of
+// each chunk) into a private sum per key, and the 32 private sums of a key are added by a
+// butterfly, which gives every lane the same bits whatever their order. The result depends only on
+// the items' positions. Past 32 keys the items are grouped again through the workspace
+// accumulator (K) instead.
 __device__ __forceinline__ int group_items(int *key, double *val, int n, const KeyAcc &K) {
   const int lane = threadIdx.x & 31;
+  double lacc[32];
   int gk = -1, ng = 0;
-  double gs = 0.0;
   bool ovf = false;
-  for (int b = 0; b < n && !ovf; b += 32) {
-    const bool in = b + lane < n;
-    group_chunk_reg(in ? key[b + lane] : -1, in ? val[b + lane] : 0.0, gk, gs, ng, ovf);
+  int kn = lane < n ? key[lane] : -1;
+  double vn = lane < n ? val[lane] : 0.0;
+  for (int b = 0; b < n; b += 32) {
+    const int k = kn;
+    const double v = vn;
+    const int bn = b + 32 + lane;  // the next chunk's loads go out before this chunk's work
+    kn = bn < n ? key[bn] : -1;
+    vn = bn < n ? val[bn] : 0.0;
+    int slot = -1;
+    for (int j = 0; j < ng; ++j)
+      if (__shfl_sync(NUPPN_FULL, gk, j) == k) slot = j;
+    unsigned pend = __ballot_sync(NUPPN_FULL, k >= 0 && slot < 0);
+    while (pend) {  // keys seen for the first time, in the order of their first lane
+      const int k0 = __shfl_sync(NUPPN_FULL, k, __ffs(pend) - 1);
+      if (ng < 32) {
+        if (lane == ng) gk = k0;
+        lacc[ng] = 0.0;
+        if (k == k0) slot = ng;
+        ++ng;
+      } else {
+        ovf = true;
+      }
+      pend &= ~__ballot_sync(NUPPN_FULL, k == k0);
+    }
+    if (ovf) break;
+    if (slot >= 0) lacc[slot] += v;
   }
-  __syncwarp();
   if (!ovf) {
+    double gs = 0.0;
+    for (int j = 0; j < ng; ++j) {
+      double t = lacc[j];
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(NUPPN_FULL, t, o);
+      if (lane == j) gs = t;
+    }
+    __syncwarp();
     if (lane < ng) {
       key[lane] = gk;
       val[lane] = gs;
@@ -1149,15 +1190,8 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
   for (int P = w; P < NP; P += nw) {
     const int c = seg_of(pofs, na, P);
     const int t0 = off[c] + (P - pofs[c]) * kRhsPiece, t1 = min(t0 + kRhsPiece, off[c + 1]);
-    const int *items = N.dg_item + N.dg_ptr[N.sp_of_sys[A.arow[c]]] - off[c];
-    for (int t = t0 + lane; t < t1; t += 32) {
-      const int it = items[t];
-      double val = 0.0;
-      const int key = rhs_item_key(N, W, spc, na, it >> 2, it & 3, val);
-      flag[t] = key < 0 ? 1 : 0;
-      fkey[t] = key;
-      fval[t] = val;
-    }
+    const int base = N.dg_ptr[N.sp_of_sys[A.arow[c]]] - off[c];
+    rhs_classify(N, W, spc, na, N.dg_item + base, N.dg_coef + base, t0, t1, flag, fkey, fval);
     __syncwarp();
     const int n = group_items(fkey + t0, fval + t0, t1 - t0, K);
     if (lane == 0) pcnt[P] = n;

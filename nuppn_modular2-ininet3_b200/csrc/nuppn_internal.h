@@ -10,7 +10,7 @@
 namespace nuppn {
 
 constexpr int kMaxLevels = 8;       // Bader-Deuflhard tableau columns (bader_deuflhard.F90:24)
-constexpr int kRhsPiece = 256;      // right-hand side items per piece when grouping frozen-reactant terms
+constexpr int kRhsPiece = 1024;     // right-hand side items per piece when grouping frozen-reactant terms
 constexpr int kRhsKeysPerRow = 8;   // group keys per active row: (row << 3) | power of its xn
 constexpr int kRhsWarps = 8;        // warps of a zone group at most (256 threads), one key accumulator each
 constexpr int kPartDim = 24;        // partition-function temperature points (array_sizes.F90:15)

@@ -188,6 +188,7 @@ double akima_eval(const Akima &ai, int npt, const double *xpt, double xx_in) {  
 struct Net {
   nuppn_knobs kn;
   int rhs_noise = -1;  // >= 0: seed of the dX/dt rounding perturbation (oracle_set_rhs_noise), else off
+  int lu_permute = -1; // >= 0: seed of the LU elimination-order permutation (oracle_set_lu_permute), else off
   int nsp, nre, ig;
   vector<double> an, zn, exmass, gspin;
   vector<uint8_t> ciso, crea;
@@ -977,19 +978,11 @@ struct SluFactors {
   bool live = false;
 };
 
-// Experiment hook for the tests (environment ORACLE_LU_PERMUTE=<seed>): hand SuperLU the reduced
-// system under a seeded symmetric permutation P A P^T (and P b, the solution permuted back). The
-// system is the same; only the elimination order, and so the rounding, changes. This measures how far
-// the checker's own results depend on the LU's elimination order.
-static int lu_permute_seed() {
-  static int seed = -2;
-  if (seed == -2) {
-    const char *e = getenv("ORACLE_LU_PERMUTE");
-    seed = e ? atoi(e) : -1;
-  }
-  return seed;
-}
-
+// Test infrastructure, off unless oracle_set_lu_permute was called: hand SuperLU the reduced system
+// of every Bader-Deuflhard level under a seeded symmetric permutation P A P^T (and P b, the solution
+// permuted back). The system is the same; only the elimination order, and so the rounding, changes.
+// The spread of the checker's results under it is how far the reference's answer depends on the
+// LU's rounding, which any other factorization changes.
 static vector<int> lu_permutation(int n, int seed) {
   vector<int> p(n);
   for (int i = 0; i < n; ++i) p[i] = i;
@@ -1025,7 +1018,7 @@ static void permute_csc(int n, const vector<double> &val, const vector<int> &row
 
 int bd_step(Zone &Z, vector<double> &y_k, vector<double> &delta_k, double h, int nvar1, int stage,
             const vector<double> &cval_in, vector<int> &crow_in, vector<int> &ccol_in, SluFactors &F) {
-  const int pseed = lu_permute_seed();
+  const int pseed = Z.N->lu_permute;
   vector<int> perm;
   vector<double> pval;
   vector<int> prow, pcol;
@@ -1932,5 +1925,6 @@ int oracle_nse(void *net, int32_t nz, const double *t9, const double *rho, const
 }
 double oracle_sortedsum(const double *a, int32_t n) { return sortedsum(a, n); }
 void oracle_set_rhs_noise(void *net, int32_t seed) { ((Net *)net)->rhs_noise = seed < 0 ? -1 : seed; }
+void oracle_set_lu_permute(void *net, int32_t seed) { ((Net *)net)->lu_permute = seed < 0 ? -1 : seed; }
 
 }  // extern "C"

@@ -47,6 +47,7 @@ def load():
     L.oracle_sortedsum.argtypes = [vp, i32]
     L.oracle_sortedsum.restype = d
     L.oracle_set_rhs_noise.argtypes = [vp, i32]
+    L.oracle_set_lu_permute.argtypes = [vp, i32]
     L.oracle_nse.argtypes = [vp, i32, vp, vp, vp, vp, i32, vp, vp, vp, vp]
     L.oracle_integrate_trajectories.argtypes = [vp, i32, i32, vp, i32, vp, vp, vp, vp, vp, vp, vp, i32]
     _L = L
@@ -133,6 +134,11 @@ class Oracle:
         """seed >= 0: from now on every dX/dt entry is scaled by 1 - 2^-52, 1 or 1 + 2^-52 at random
         (a rounding-sized change, per zone and seed deterministic); None or < 0: off."""
         self.L.oracle_set_rhs_noise(self.h, -1 if seed is None else int(seed))
+
+    def set_lu_permute(self, seed):
+        """seed >= 0: from now on SuperLU factors every Bader-Deuflhard system under a seeded symmetric
+        permutation (same system, another elimination order and rounding); None or < 0: off."""
+        self.L.oracle_set_lu_permute(self.h, -1 if seed is None else int(seed))
 
     def integrate_network(self, X, t9_0, t9_1, rho_0, rho_1, ye, dtwant, bd_state=None, nthreads=1):
         X = np.array(np.atleast_2d(X), dtype=np.float64, order="C", copy=True)

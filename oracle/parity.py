@@ -3,10 +3,10 @@ checker leg, never by the product).
 
 The reference's FP64 CPU path is restated in oracle.cpp and calls the reference's own SuperLU, so
 the checker's output is the yardstick. Some zones are ill-conditioned in the reference's own
-algorithm: a change of one unit in the last place of the input, or of one rounding in the sums of
-dX/dt, changes their sub-step sequence or their final abundances far beyond 1e-6. For those,
-`checker_spread` measures how far the checker itself moves under both kinds of perturbation, and a
-device result is judged against that spread. (The second kind is what any implementation that does
+algorithm: a change of one unit in the last place of the input, of one rounding in the sums of
+dX/dt, or of the LU's elimination order changes their sub-step sequence or their final abundances
+far beyond 1e-6. For those, `checker_spread` measures how far the checker itself moves under these
+three kinds of perturbation, and a device result is judged against that spread. (The second kind is what any implementation that does
 not add the reference's terms in the reference's order is free to differ by: H-burning zones at
 T9 < 0.08 over 1e10 s move by 1-50 % under it while 1-ulp input changes move them far less.)
 """
@@ -29,26 +29,29 @@ def zone_errors(X, Xr):
     return rel, ab
 
 
-def checker_spread(ref, zb, X0, trials=(1, 2), nthreads=1, rhs_noise=True):
+def checker_spread(ref, zb, X0, trials=(1, 2), nthreads=1, rhs_noise=True, lu_permute=True):
     """Per zone: the largest relative change (species with X0 > 1e-12) of the checker's own final
-    abundances over seeded draws of two perturbations: every initial abundance moved by -1, 0 or
-    +1 ulp at random (one draw per entry of `trials`), and, with rhs_noise, every dX/dt entry of
-    every evaluation scaled by 1 - 2^-52, 1 or 1 + 2^-52 at random (one draw per entry of `trials`).
-    X0 is the checker's unperturbed result for the batch zb; the checker's noise is off afterwards."""
+    abundances over seeded draws of three perturbations, one draw of each per entry of `trials`:
+    every initial abundance moved by -1, 0 or +1 ulp at random; with rhs_noise, every dX/dt entry of
+    every evaluation scaled by 1 - 2^-52, 1 or 1 + 2^-52 at random; with lu_permute, every
+    Bader-Deuflhard system factored by SuperLU in another (seeded) elimination order. X0 is the
+    checker's unperturbed result for the batch zb; the checker's perturbations are off afterwards."""
     args = (zb.t9_0, zb.t9_1, zb.rho_0, zb.rho_1, zb.ye, zb.dtwant)
     spread = np.zeros(zb.nz)
     for t in trials:
         Xp = zb.X * (1.0 + np.random.default_rng(t).choice([-1.0, 0.0, 1.0], size=zb.X.shape) * 2.2e-16)
         X1, _, _, _, _ = ref.integrate_network(Xp, *args, nthreads=nthreads)
         spread = np.maximum(spread, zone_errors(X1, X0)[0])
-    if rhs_noise:
+    for on, setter in ((rhs_noise, ref.set_rhs_noise), (lu_permute, ref.set_lu_permute)):
+        if not on:
+            continue
         try:
             for t in trials:
-                ref.set_rhs_noise(t)
+                setter(t)
                 X1, _, _, _, _ = ref.integrate_network(zb.X, *args, nthreads=nthreads)
                 spread = np.maximum(spread, zone_errors(X1, X0)[0])
         finally:
-            ref.set_rhs_noise(None)
+            setter(None)
     return spread
 
 

@@ -242,10 +242,11 @@ def test_no_cpu_fallback_in_product(solver_mod):
 
 def test_oracle_rhs_noise_is_seeded_and_shows_hburn_sensitivity(orc, abi, wl):
     """The checker's dX/dt perturbation (a rounding-sized change of every entry, the freedom any
-    implementation that sums the terms in another order has): off by default and after it is
-    switched off, deterministic per seed and independent of the thread count. Cool H-burning zones
+    implementation that sums the terms in another order has) and its elimination-order perturbation
+    of the LU: off by default and after they are switched off, deterministic per seed and
+    independent of the thread count. Cool H-burning zones
     (300 species, T9 0.02-0.05, 1e10 s) move by far more than 1e-6 under it, which is why the
-    parity bar for such zones is the checker's spread under both perturbations."""
+    parity bar for such zones is the checker's spread under these perturbations."""
     net = wl.network(300)
     hb, _ = wl.hburn_zone(net)
     n = 6
@@ -263,6 +264,11 @@ def test_oracle_rhs_noise_is_seeded_and_shows_hburn_sensitivity(orc, abi, wl):
     Xc, _, _, _, _ = run(2)
     assert np.array_equal(Xa, Xb) and np.array_equal(iea, ieb)  # per-zone generators
     assert np.array_equal(Xc, X0)  # off again
+    ref.set_lu_permute(3)  # another elimination order: deterministic, off again afterwards
+    Xp1, _, _, _, _ = run(1)
+    Xp2, _, _, _, _ = run(3)
+    ref.set_lu_permute(None)
+    assert np.array_equal(Xp1, Xp2) and np.array_equal(run(2)[0], X0)
     ok = (ie0 == 0) & (iea == 0)
     assert ok.sum() >= 3
     big = X0 > 1e-12

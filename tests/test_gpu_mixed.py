@@ -6,7 +6,9 @@ He-shell zones on the ~1100-species network and hot zones on the ~2500-species n
 Every zone's result must equal, bit for bit, what nuppn_integrate gives for it on its own network
 (the launch only chooses which network description a CTA reads), and lie within the parity bar of
 the checker: 1e-6 relative for X > 1e-12, 1e-15 absolute below, or twice the checker's own spread
-under 1-ulp input changes for zones that the checker itself cannot pin to 1e-6.
+(four draws each of 1-ulp input changes and of rounding-sized dX/dt changes) for zones that the
+checker itself cannot pin to 1e-6 (the H-burning zones of the ~200-species network move by up to
+tens of percent under the latter).
 """
 import numpy as np
 import pytest
@@ -56,7 +58,7 @@ def test_mixed_networks_one_launch(solver_mod, abi, orc, wl):
         off = np.nonzero((rel > 1e-6) | (ab > 1e-15))[0]
         spread = np.zeros(zb.nz)
         if off.size:
-            spread[off] = parity.checker_spread(ref, zb.take(off), Xr[off], nthreads=8)
+            spread[off] = parity.checker_spread(ref, zb.take(off), Xr[off], trials=(1, 2, 3, 4), nthreads=8)
         pinned = spread < 1e-6
         assert (rel[pinned] <= 1e-6).all() and (ab[pinned] <= 1e-15).all(), (nets[i].name, rel, ab)
         assert (rel[~pinned] <= 2.0 * spread[~pinned]).all(), (nets[i].name, rel, spread)

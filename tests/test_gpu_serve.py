@@ -129,7 +129,10 @@ def test_serve_small_dt_outcomes_match_checker(solver_mod, abi, orc, wl):
     1e10 s, Bader-Deuflhard) through the server: each zone's outcome (success or SMALL_DT, the step
     falling below 1e-30 s) equals the checker's on every zone whose checker outcome stays the same
     under two draws of 1-ulp input changes (on the others the reference's own outcome is not
-    determined by its input), and successful zones meet the parity bar."""
+    determined by its input), and successful zones meet the parity bar. These zones move by 1-50 %
+    under rounding-sized changes of dX/dt in the reference's own algorithm, so their bar is twice the
+    checker's spread over four draws of each perturbation (with two draws, the checker itself under
+    another draw falls outside twice the spread on 2 of 32 zones; with four, on none)."""
     import parity
 
     net = wl.network(300)
@@ -167,5 +170,5 @@ def test_serve_small_dt_outcomes_match_checker(solver_mod, abi, orc, wl):
         sub = np.nonzero(ok)[0][off]
         spread = parity.checker_spread(ref, wl.ZoneBatch(X=X[sub], t9_0=t9[sub], t9_1=t9[sub], rho_0=rho[sub],
                                                         rho_1=rho[sub], ye=ye[sub], dtwant=np.full(sub.size, 1e10)),
-                                       Xr[sub], nthreads=8)
+                                       Xr[sub], trials=(1, 2, 3, 4), nthreads=8)
         assert (rel[off] <= 2.0 * spread).all(), (rel[off], spread)
