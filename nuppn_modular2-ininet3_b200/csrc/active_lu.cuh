@@ -32,6 +32,9 @@ constexpr int kOneWarpMax = 512;
 // Flags of a compact LU position (jflag): entry set, diagonal, fill (no Jacobian entry).
 enum : uint8_t { JF_SET = 1, JF_DIAG = 2, JF_FILL = 4 };
 
+// Flag of a right-hand side item (grpk) that is a group of reactions with a frozen reactant.
+constexpr uint32_t kGroupItem = 1u << 31;
+
 struct Act {
   int na, nnz;
   int *crp, *cdiag, *arow, *flagF, *flagS, *ccol, *csrc;
@@ -61,7 +64,7 @@ struct Act {
   int ngi;
   int *gptr;         // [na+1] gather items of active row c: gptr[c] .. gptr[c+1]-1
   float *gcoef;      // [ngi] term coefficient (-k2, -1, k6 or k8)
-  uint32_t *grpk;    // [ngi] compact index of reactant 1 | reactant 2 (na = gamma) << 14 | k2 << 28
+  uint32_t *grpk;    // [ngi] compact index of reactant 1 | reactant 2 (na = gamma) << 14 | k2 << 28 | group flag << 31
   double *grcv;      // [ngi] (1/k2!) * rate of the term's reaction (a group's constant: see below)
   double *gterm;     // [ngi] term values of the current sub-step
   bool rhs_in_smem;
@@ -269,14 +272,20 @@ __device__ __forceinline__ double jac_contrib(const DevNet &N, const Ws &W, int 
 
 // Jacobian values (1e-99 + the contributions of every reaction that passes the rate test, masked
 // reactants or not, as in the reference) and entry flags for the positions of the active subsystem.
-// Entries with short static gather lists are evaluated as one flattened, block-parallel list and
-// summed by one thread each in the list's order from 1e-99 (the reference's accumulation: jac =
-// 1e-99, then += each contribution in reaction order, jac_rhs.F90:309-392). The few with long lists
-// (among n, p and alpha: every capture on every nucleus, frozen or not) are cut into pieces of
-// kRhsPiece items; a warp sums a piece (lane-strided, then a fixed butterfly) and each entry adds
-// its pieces' sums in piece order, so the result does not depend on which warp took which piece.
+// Runs after dev_compact_rhs. Entries with short static gather lists are evaluated as one flattened,
+// block-parallel list and summed by one thread each in the list's order from 1e-99 (the reference's
+// accumulation: jac = 1e-99, then += each contribution in reaction order, jac_rhs.F90:309-392).
+// The few with long lists (among n, p and alpha: every capture on every nucleus) take the reactions
+// whose other reactant is masked or gamma from their list, in pieces of kRhsPiece items (a warp
+// sums a piece, lane-strided and then by a fixed butterfly; each entry adds its pieces in order),
+// and the reactions with a frozen other reactant from the right-hand side's groups: a group of row i
+// with varying factor xn_j^p and constant G contributes d/dxn_j (G xn_j^p) = p G xn_j^(p-1), times
+// A_i / A_j, to entry (i, j), which is the sum of those reactions' contributions in the reference
+// (their stems, jac_rhs.F90:346-353, with k4 = 1 or k3 = gamma), added in another order. Such a
+// reaction never sets an entry (its frozen reactant is never masked, jac_rhs.F90:399-436).
 __device__ void dev_jacobian_active(const DevNet &N, const Ws &W, Act &A, int *sint) {
   const int tid = GT, nt = GN, lane = tid & 31, w = tid >> 5, nw = nt >> 5, nnz = A.nnz;
+  const int *spc = W.rhs_spc;             // species -> active row (dev_compact_rhs), -1 if frozen
   int *off = W.act_otmp;                  // [nnz+1] short entries' items, then offsets
   int *lfl = W.jac_long;                  // [nnz+1] long-entry flags, then their ranks
   int *lst = W.jac_long + (N.nnzLU + 1);  // [nlong] positions of the long entries, in order
@@ -321,10 +330,12 @@ __device__ void dev_jacobian_active(const DevNet &N, const Ws &W, Act &A, int *s
     const int e = N.lu_src[A.csrc[lst[L]]];
     const int *items = N.jg_item + N.jg_ptr[e];
     const int t0 = (Q - poff[L]) * kRhsPiece, t1 = min(t0 + kRhsPiece, N.jg_ptr[e + 1] - N.jg_ptr[e]);
+    const int *oth = N.jg_oth + N.jg_ptr[e];
     double acc = 0.0;
     int set = 0;
-#pragma unroll 4
     for (int t = t0 + lane; t < t1; t += 32) {
+      const int o = oth[t];
+      if (o >= 0 && spc[o] < 0) continue;  // a frozen other reactant: in the groups below
       const int it = items[t];
       bool st;
       acc += jac_contrib(N, W, it >> 3, it & 7, st);
@@ -355,6 +366,14 @@ __device__ void dev_jacobian_active(const DevNet &N, const Ws &W, Act &A, int *s
       for (int Q = poff[L]; Q < poff[L + 1]; ++Q) {
         sum += dv[T + Q];
         set |= sf[T + Q];
+      }
+      const int r = seg_of(A.crp, A.na, p), cj = A.ccol[p];
+      const double y = W.xn[N.sp_of_sys[A.arow[cj]]], ar = A.anc[r], ac = A.anc[cj];
+      for (int q = A.gptr[r]; q < A.gptr[r + 1]; ++q) {  // the row's groups varying with xn_j
+        const uint32_t pk = A.grpk[q];
+        if (!(pk & kGroupItem) || (int)(pk & 0x3fff) != cj) continue;
+        const int pw = (int)((pk >> 28) & 7);
+        sum += (((double)pw * A.grcv[q] * powi(y, pw - 1)) * ar) / ac;
       }
       acc = 1.e-99 + sum;
     } else {
@@ -1084,7 +1103,7 @@ __device__ __forceinline__ void group_emit(const KeyAcc &K, int n, int *key, dou
 __device__ __forceinline__ void put_group_item(Act &A, int q, int key, double sum) {
   A.gcoef[q] = 1.0f;
   A.grcv[q] = sum;
-  A.grpk[q] = (uint32_t)(key >> 3) | ((uint32_t)A.na << 14) | ((uint32_t)(key & 7) << 28);
+  A.grpk[q] = (uint32_t)(key >> 3) | ((uint32_t)A.na << 14) | ((uint32_t)(key & 7) << 28) | kGroupItem;
 }
 
 // The groups of the items key[0..n) (-1: none), written over key[0..groups) and val[0..groups);
@@ -1264,7 +1283,7 @@ __device__ __forceinline__ double powi_small(double x, int m) {  // powi's produ
 
 __device__ __forceinline__ double rhs_term(const Act &A, int q) {
   const uint32_t pk = A.grpk[q];
-  const double flux = A.grcv[q] * powi_small(A.xnc[pk & 0x3fff], (int)(pk >> 28)) * A.xnc[(pk >> 14) & 0x3fff];
+  const double flux = A.grcv[q] * powi_small(A.xnc[pk & 0x3fff], (int)((pk >> 28) & 7)) * A.xnc[(pk >> 14) & 0x3fff];
   return (double)A.gcoef[q] * flux;
 }
 

@@ -144,7 +144,7 @@ nuppn_status upload(nuppn_net *net) {
   P(H.ngt8); P(H.ngl10t8); P(H.ngflag); P(H.ngane); P(H.ngl10v); P(H.ngndata);
   P(H.fft9); P(H.ffrho); P(H.ffl10v); P(H.kdE); P(H.kdcoef); P(H.constr);
   P(H.jrow); P(H.jcol); P(H.jdiag); P(H.jg_ptr); P(H.jg_item); P(H.dg_ptr); P(H.dg_item); P(H.dg_coef);
-  P(H.jg_long); P(H.dg_long);
+  P(H.jg_long); P(H.dg_long); P(H.jg_oth);
   P(H.sys_of_sp); P(H.sp_of_sys); P(H.pos_of_entry); P(H.lu_src); P(H.lu_rowptr); P(H.lu_diag); P(H.lu_col); P(H.upd_start);
   P(H.upd_off); P(H.lvL_ptr); P(H.lvL_rows); P(H.lvL_grp); P(H.lvU_ptr); P(H.lvU_rows); P(H.lvU_grp);
   P(H.k1_ptr); P(H.k1_list);
@@ -177,7 +177,7 @@ nuppn_status upload(nuppn_net *net) {
   D.jrow = (const int *)nx(); D.jcol = (const int *)nx(); D.jdiag = (const int *)nx();
   D.jg_ptr = (const int *)nx(); D.jg_item = (const int *)nx(); D.dg_ptr = (const int *)nx();
   D.dg_item = (const int *)nx(); D.dg_coef = (const double *)nx();
-  D.jg_long = (const int *)nx(); D.dg_long = (const int *)nx();
+  D.jg_long = (const int *)nx(); D.dg_long = (const int *)nx(); D.jg_oth = (const int *)nx();
   D.sys_of_sp = (const int *)nx(); D.sp_of_sys = (const int *)nx(); D.pos_of_entry = (const int *)nx();
   D.lu_src = (const int *)nx();
   D.lu_rowptr = (const int *)nx(); D.lu_diag = (const int *)nx(); D.lu_col = (const int *)nx();

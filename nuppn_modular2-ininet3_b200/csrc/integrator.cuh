@@ -87,8 +87,8 @@ __device__ double dev_ye(const DevNet &N, const double *x, double *sred) {
 __device__ void dev_new_jacobian(const DevNet &N, const Ws &W, ZoneCtl &C, double dt, const double *y) {
   dev_jacobian_mask(N, W, dt, y);
   dev_compact(N, W, C.act, C.smem, C.smem_bytes, C.sint);
-  dev_jacobian_active(N, W, C.act, C.sint);
   dev_compact_rhs(N, W, C.act, C.smem, C.smem_bytes, C.sint);
+  dev_jacobian_active(N, W, C.act, C.sint);
   C.st.nvar1_last = C.act.na;
   C.st.nvar1_max = max(C.st.nvar1_max, C.act.na);
 }

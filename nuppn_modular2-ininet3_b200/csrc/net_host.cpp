@@ -386,6 +386,12 @@ std::string build_host_net(const nuppn_net_desc &d, const nuppn_knobs &kn, HostN
     for (int e = 0; e < H.nnzJ; ++e) H.jg_ptr[e + 1] = H.jg_ptr[e] + (int)lists[e].size();
     H.jg_item.reserve(H.jg_ptr[H.nnzJ]);
     for (auto &L : lists) H.jg_item.insert(H.jg_item.end(), L.begin(), L.end());
+    H.jg_oth.reserve(H.jg_item.size());
+    for (int it : H.jg_item) {
+      const int *k = &H.act_k[(size_t)(it >> 3) * 8];
+      const int o = (it & 7) < 4 ? k[2] : k[0];  // slots 0-3: d/dy(k1), the other is k3; 4-7: d/dy(k3)
+      H.jg_oth.push_back(o == H.ig ? -1 : o);
+    }
   }
   {
     std::vector<std::vector<int>> lists(nsp);

@@ -52,6 +52,7 @@ struct HostNet {
   // pattern
   std::vector<int> jrow, jcol, jdiag, dmap_all;  // dmap_all[nre*8] (-1 for unconsidered)
   std::vector<int> jg_ptr, jg_item, dg_ptr, dg_item, jg_long, dg_long;
+  std::vector<int> jg_oth;        // per jg item: the reaction's other reactant (the one not differentiated), -1 for gamma
   std::vector<int> k1_ptr, k1_list;  // species -> considered reactions it leads as k1, in order
   std::vector<double> dg_coef;
   // system / LU

@@ -66,6 +66,7 @@ struct DevNet {
   // Jacobian pattern and gathers
   const int *jrow, *jcol, *jdiag;          // jdiag[nsp]: entry of (i,i) or -1
   const int *jg_ptr, *jg_item;             // entry -> (a*8 + s) in reference accumulation order
+  const int *jg_oth;                       // per jg item: the other reactant's species, -1 for gamma
   const int *dg_ptr, *dg_item;             // species -> (a*4 + slot) in scatter order
   const double *dg_coef;                   // coefficient of each dg item: -k2, -1, k6, k8
   int njg_long, ndg_long;
