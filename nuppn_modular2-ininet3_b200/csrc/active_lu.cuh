@@ -991,63 +991,46 @@ __device__ __forceinline__ void put_rhs_item(const DevNet &N, const Ws &W, Act &
   A.grpk[q] = i1 | (i2 << 14) | ((uint32_t)k[1] << 28);
 }
 
-// Items [t0, t1) of a masked row's static list (items[t] = reaction a << 2 | slot m, coefs[t] the
-// slot's coefficient -k2, -1, k6 or k8), classified by one warp, four items per lane at a time with
-// their loads issued together. An item whose reactants are all masked or gamma is a term of its own
-// (flag 1, key -1); otherwise its group key is (compact row of its masked reactant << 3) | that
+// Every considered reaction classified once per step, block-parallel and coalesced over reactions:
+// rkey[a] = -1 if its reactants are all masked or gamma (each of its slots in a masked row is then a
+// term of its own); otherwise its group key, (compact row of its masked reactant << 3) | that
 // reactant's power, or (na << 3) | 1 when every reactant is frozen or gamma (a constant flux), and
-// its value is coefficient * (1/k2!) v * the frozen reactants' xn (xn1^k2, xn2), in the reference's
-// order of products. spc: species -> compact row, -1 if frozen (gamma included).
-__device__ __forceinline__ void rhs_classify(const DevNet &N, const Ws &W, const int *spc, int na, const int *items,
-                                             const double *coefs, int t0, int t1, int *flag, int *fkey, double *fval) {
-  const int lane = threadIdx.x & 31, g = N.ig;
+// rcf[a] = (1/k2!) v * the frozen reactants' xn (xn1^k2, xn2) in the reference's order of products.
+// spc: species -> compact row, -1 if frozen (gamma included).
+__device__ __forceinline__ void rhs_classify_reactions(const DevNet &N, const Ws &W, const int *spc, int na, int *rkey,
+                                                       double *rcf) {
+  const int g = N.ig;
   const int4 *kp = reinterpret_cast<const int4 *>(N.act_k);
-  for (int b = t0; b < t1; b += 128) {
-    int it[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int t = b + lane + 32 * i;
-      it[i] = t < t1 ? items[t] : -1;
+#pragma unroll 2
+  for (int a = GT; a < N.nact; a += GN) {
+    const int4 k = kp[2 * (size_t)a];
+    const int c1 = spc[k.x], c2 = k.z == g ? na : spc[k.z];
+    const bool m1 = c1 >= 0, m2 = c2 >= 0;
+    if (m1 && m2) {
+      rkey[a] = -1;
+      continue;
     }
-    int4 k[4];
-    int sl[4];
-    double co[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int a = it[i] < 0 ? 0 : it[i] >> 2;
-      k[i] = kp[2 * (size_t)a];
-      sl[i] = N.act_slot[a];
-      co[i] = coefs[it[i] < 0 ? t0 : b + lane + 32 * i];
-    }
-    int c1[4], c2[4];
-    double v[4], x1[4], x2[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      c1[i] = spc[k[i].x];
-      c2[i] = k[i].z == g ? na : spc[k[i].z];
-      v[i] = W.v[sl[i]];
-      x1[i] = W.xn[k[i].x];
-      x2[i] = W.xn[k[i].z];
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int t = b + lane + 32 * i;
-      if (it[i] < 0) continue;
-      const bool m1 = c1[i] >= 0, m2 = c2[i] >= 0;
-      int key = -1;
-      double val = 0.0;
-      if (!(m1 && m2)) {
-        const int k2 = k[i].y;
-        double cf = c_fact[k2] * v[i];
-        if (!m1) cf = cf * powi(x1[i], k2);
-        if (!m2) cf = cf * x2[i];
-        val = co[i] * cf;
-        key = m1 ? (c1[i] << 3) | k2 : (m2 && c2[i] < na ? (c2[i] << 3) | 1 : (na << 3) | 1);
-      }
-      flag[t] = key < 0 ? 1 : 0;
-      fkey[t] = key;
-      fval[t] = val;
-    }
+    double cf = c_fact[k.y] * W.v[N.act_slot[a]];
+    if (!m1) cf = cf * powi(W.xn[k.x], k.y);
+    if (!m2) cf = cf * W.xn[k.z];
+    rkey[a] = m1 ? (c1 << 3) | k.y : (m2 && c2 < na ? (c2 << 3) | 1 : (na << 3) | 1);
+    rcf[a] = cf;
+  }
+}
+
+// Items [t0, t1) of a masked row's static list (items[t] = reaction a << 2 | slot m, coefs[t] the
+// slot's coefficient -k2, -1, k6 or k8) with their reactions' classes: own-term flag, group key and
+// value coefficient * rcf[a].
+__device__ __forceinline__ void rhs_classify(const int *rkey, const double *rcf, const int *items,
+                                             const double *coefs, int t0, int t1, int *flag, int *fkey, double *fval) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll 4
+  for (int t = t0 + lane; t < t1; t += 32) {
+    const int a = items[t] >> 2;
+    const int key = rkey[a];
+    flag[t] = key < 0 ? 1 : 0;
+    fkey[t] = key;
+    fval[t] = key < 0 ? 0.0 : coefs[t] * rcf[a];
   }
 }
 
@@ -1180,6 +1163,8 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
   int *pofs = W.rhs_piece;                   // [na+1] first piece of each row
   int *pcnt = W.rhs_piece + (N.nsys + 1);    // [pieces] groups of each piece
   int *spc = W.rhs_spc;                      // [nsp] species -> active row, -1 if frozen
+  int *rkey = W.rhs_rkey;                    // [nact] each reaction's class: -1 own terms, else group key
+  double *rcf = W.rhs_rcf;                   // [nact] its frozen factors' constant
   const int na = A.na, nkey = (na + 1) << 3;
   const size_t kw = (size_t)w * kRhsKeysPerRow * (N.nsys + 1);  // this warp's accumulator
   const KeyAcc K = {W.rhs_acc + kw, W.rhs_tag + kw, W.rhs_list + kw};
@@ -1198,6 +1183,7 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
     pofs[c] = (len + kRhsPiece - 1) / kRhsPiece;
   }
   GSYNC();
+  rhs_classify_reactions(N, W, spc, na, rkey, rcf);
   const int T = block_scan_excl(off, na, sint);
   const int NP = block_scan_excl(pofs, na, sint);
   if (tid == 0) {
@@ -1210,7 +1196,7 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
     const int c = seg_of(pofs, na, P);
     const int t0 = off[c] + (P - pofs[c]) * kRhsPiece, t1 = min(t0 + kRhsPiece, off[c + 1]);
     const int base = N.dg_ptr[N.sp_of_sys[A.arow[c]]] - off[c];
-    rhs_classify(N, W, spc, na, N.dg_item + base, N.dg_coef + base, t0, t1, flag, fkey, fval);
+    rhs_classify(rkey, rcf, N.dg_item + base, N.dg_coef + base, t0, t1, flag, fkey, fval);
     __syncwarp();
     const int n = group_items(fkey + t0, fval + t0, t1 - t0, K);
     if (lane == 0) pcnt[P] = n;

@@ -242,6 +242,8 @@ WsLayout layout(const HostNet &H) {
     L.rhs_tag = take(keys * sizeof(int));
     L.rhs_list = take(keys * sizeof(int));
     L.rhs_spc = take((size_t)H.nsp * sizeof(int));
+    L.rhs_rkey = take((size_t)H.nact * sizeof(int));
+    L.rhs_rcf = take((size_t)H.nact * sizeof(double));
     L.jac_long = take(3 * ((size_t)H.nnzLU + 1) * sizeof(int));
   }
   L.nse = take((5 * (size_t)H.nsp + (size_t)H.nse_p2) * sizeof(double));
