@@ -981,24 +981,17 @@ __device__ bool dev_solve_species(const DevNet &N, Act &A, const double *rhs, do
 // Groups are found deterministically: a row's static list is cut into pieces of kRhsPiece items,
 // a warp sums each piece's items per key (a fixed butterfly per key and chunk of 32 items, then the
 // chunks in order), and a warp per row sums its pieces' groups in piece order.
-__device__ __forceinline__ void put_rhs_item(const DevNet &N, const Ws &W, Act &A, const int *sys2c, int q, int a,
-                                             int m) {
-  const int *k = N.act_k + (size_t)a * 8;
-  const uint32_t i1 = (uint32_t)sys2c[N.sys_of_sp[k[0]]];
-  const uint32_t i2 = k[2] == N.ig ? (uint32_t)A.na : (uint32_t)sys2c[N.sys_of_sp[k[2]]];
-  A.gcoef[q] = (float)(m == 0 ? -k[1] : m == 1 ? -1 : m == 2 ? k[5] : k[7]);  // small integers, exact
-  A.grcv[q] = c_fact[k[1]] * W.v[N.act_slot[a]];
-  A.grpk[q] = i1 | (i2 << 14) | ((uint32_t)k[1] << 28);
-}
 
 // Every considered reaction classified once per step, block-parallel and coalesced over reactions:
 // rkey[a] = -1 if its reactants are all masked or gamma (each of its slots in a masked row is then a
 // term of its own); otherwise its group key, (compact row of its masked reactant << 3) | that
 // reactant's power, or (na << 3) | 1 when every reactant is frozen or gamma (a constant flux), and
 // rcf[a] = (1/k2!) v * the frozen reactants' xn (xn1^k2, xn2) in the reference's order of products.
+// For a reaction of the first kind, rcf[a] = (1/k2!) v and rpk[a] packs its term's reactants as the
+// gather items do (compact row of k1 | of k3, na for gamma, << 14 | k2 << 28).
 // spc: species -> compact row, -1 if frozen (gamma included).
 __device__ __forceinline__ void rhs_classify_reactions(const DevNet &N, const Ws &W, const int *spc, int na, int *rkey,
-                                                       double *rcf) {
+                                                       double *rcf, uint32_t *rpk) {
   const int g = N.ig;
   const int4 *kp = reinterpret_cast<const int4 *>(N.act_k);
 #pragma unroll 2
@@ -1006,11 +999,13 @@ __device__ __forceinline__ void rhs_classify_reactions(const DevNet &N, const Ws
     const int4 k = kp[2 * (size_t)a];
     const int c1 = spc[k.x], c2 = k.z == g ? na : spc[k.z];
     const bool m1 = c1 >= 0, m2 = c2 >= 0;
+    double cf = c_fact[k.y] * W.v[N.act_slot[a]];
     if (m1 && m2) {
       rkey[a] = -1;
+      rcf[a] = cf;
+      rpk[a] = (uint32_t)c1 | ((uint32_t)c2 << 14) | ((uint32_t)k.y << 28);
       continue;
     }
-    double cf = c_fact[k.y] * W.v[N.act_slot[a]];
     if (!m1) cf = cf * powi(W.xn[k.x], k.y);
     if (!m2) cf = cf * W.xn[k.z];
     rkey[a] = m1 ? (c1 << 3) | k.y : (m2 && c2 < na ? (c2 << 3) | 1 : (na << 3) | 1);
@@ -1165,6 +1160,7 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
   int *spc = W.rhs_spc;                      // [nsp] species -> active row, -1 if frozen
   int *rkey = W.rhs_rkey;                    // [nact] each reaction's class: -1 own terms, else group key
   double *rcf = W.rhs_rcf;                   // [nact] its frozen factors' constant
+  uint32_t *rpk = W.rhs_rpk;                 // [nact] packed reactants of a reaction of own terms
   const int na = A.na, nkey = (na + 1) << 3;
   const size_t kw = (size_t)w * kRhsKeysPerRow * (N.nsys + 1);  // this warp's accumulator
   const KeyAcc K = {W.rhs_acc + kw, W.rhs_tag + kw, W.rhs_list + kw};
@@ -1183,7 +1179,7 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
     pofs[c] = (len + kRhsPiece - 1) / kRhsPiece;
   }
   GSYNC();
-  rhs_classify_reactions(N, W, spc, na, rkey, rcf);
+  rhs_classify_reactions(N, W, spc, na, rkey, rcf, rpk);
   const int T = block_scan_excl(off, na, sint);
   const int NP = block_scan_excl(pofs, na, sint);
   if (tid == 0) {
@@ -1247,11 +1243,17 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
   A.gterm = (double *)base;
   A.ngi = ngi;
   for (int c = tid; c <= na; c += nt) A.gptr[c] = c < na ? cnt[c] : ngi;
-  for (int t = tid; t < T; t += nt) {  // own terms first, in the static list's order
-    if (flag[t + 1] == flag[t]) continue;
-    const int c = seg_of(off, na, t);
-    const int it = N.dg_item[N.dg_ptr[N.sp_of_sys[A.arow[c]]] + (t - off[c])];
-    put_rhs_item(N, W, A, sys2c, cnt[c] + flag[t] - flag[off[c]], it >> 2, it & 3);
+  for (int P = w; P < NP; P += nw) {  // own terms first, in the static list's order (a warp per piece)
+    const int c = seg_of(pofs, na, P);
+    const int t0 = off[c] + (P - pofs[c]) * kRhsPiece, t1 = min(t0 + kRhsPiece, off[c + 1]);
+    const int base = N.dg_ptr[N.sp_of_sys[A.arow[c]]] - off[c], q0 = cnt[c] - flag[off[c]];
+    for (int t = t0 + lane; t < t1; t += 32) {
+      if (flag[t + 1] == flag[t]) continue;
+      const int a = N.dg_item[base + t] >> 2, q = q0 + flag[t];
+      A.gcoef[q] = (float)N.dg_coef[base + t];  // -k2, -1, k6 or k8: small integers, exact
+      A.grcv[q] = rcf[a];
+      A.grpk[q] = rpk[a];
+    }
   }
   for (int c = w; c < na; c += nw) {  // then the row's groups
     const int own = flag[off[c + 1]] - flag[off[c]];

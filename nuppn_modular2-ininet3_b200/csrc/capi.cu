@@ -242,8 +242,11 @@ WsLayout layout(const HostNet &H) {
     L.rhs_tag = take(keys * sizeof(int));
     L.rhs_list = take(keys * sizeof(int));
     L.rhs_spc = take((size_t)H.nsp * sizeof(int));
+    L.cache_mask = take((size_t)H.nsp);
+    L.cache_xn = take((size_t)H.nsp * sizeof(double));
     L.rhs_rkey = take((size_t)H.nact * sizeof(int));
     L.rhs_rcf = take((size_t)H.nact * sizeof(double));
+    L.rhs_rpk = take((size_t)H.nact * sizeof(uint32_t));
     L.jac_long = take(3 * ((size_t)H.nnzLU + 1) * sizeof(int));
   }
   L.nse = take((5 * (size_t)H.nsp + (size_t)H.nse_p2) * sizeof(double));

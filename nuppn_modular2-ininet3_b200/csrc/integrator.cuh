@@ -25,6 +25,11 @@ struct ZoneCtl {
   int *sint;      // shared scan scratch (>= 32 ints)
   Act act;        // active subsystem of the current Jacobian
   NseCtl nse;     // NSE solver state of the zone (kept across its NSE calls within one call)
+  // The active subsystem's structure and right-hand side items depend only on the mask, the rates
+  // and the frozen species' abundances; when none changed since they were built they are kept.
+  int rates_ver;  // incremented by every rate evaluation
+  int built_ver;  // rates_ver when act was built; act_ok: act's shared memory still holds it
+  bool act_ok;
 };
 
 __device__ void vcopy(double *dst, const double *src, int n) {
@@ -83,11 +88,29 @@ __device__ double dev_ye(const DevNet &N, const double *x, double *sred) {
   return (1.0 - s) * 0.5;
 }
 
-// Jacobian pass, compaction, active Jacobian and restricted right-hand side for abundances y
+// Jacobian pass, compaction, active Jacobian and restricted right-hand side for abundances y. The
+// compaction and the right-hand side items are rebuilt only if the mask, the rates or a frozen
+// species' abundance changed since the last build (about half the Jacobians of a He-shell zone keep
+// all three); the Jacobian values are always new.
 __device__ void dev_new_jacobian(const DevNet &N, const Ws &W, ZoneCtl &C, double dt, const double *y) {
   dev_jacobian_mask(N, W, dt, y);
-  dev_compact(N, W, C.act, C.smem, C.smem_bytes, C.sint);
-  dev_compact_rhs(N, W, C.act, C.smem, C.smem_bytes, C.sint);
+  int same = C.act_ok && C.built_ver == C.rates_ver;
+  if (same) {
+    int diff = 0;
+    for (int s = GT; s < N.nsp; s += GN)
+      diff |= W.mask[s] != W.cache_mask[s] || (!W.mask[s] && W.xn[s] != W.cache_xn[s]);
+    same = !g_or(diff);
+  }
+  if (!same) {
+    dev_compact(N, W, C.act, C.smem, C.smem_bytes, C.sint);
+    dev_compact_rhs(N, W, C.act, C.smem, C.smem_bytes, C.sint);
+    for (int s = GT; s < N.nsp; s += GN) {
+      W.cache_mask[s] = W.mask[s];
+      W.cache_xn[s] = W.xn[s];
+    }
+    C.built_ver = C.rates_ver;
+    C.act_ok = true;
+  }
   dev_jacobian_active(N, W, C.act, C.sint);
   C.st.nvar1_last = C.act.na;
   C.st.nvar1_max = max(C.st.nvar1_max, C.act.na);
@@ -455,6 +478,7 @@ __device__ int dev_integrate_zone(const DevNet &N, const Ws &W, ZoneCtl &C, doub
   double ye_old = ye, dtdone = 0.0, dtrcmd = 0.0, dttry = dtwant;
   double t9_last = 0.5 * (t9_0 + t9_1), rho_last = 0.5 * (rho_0 + rho_1);
   dev_eval_rates(N, W, t9_last, rho_last, ye, yps, sred);  // the frame's evaluate_all_rates
+  C.rates_ver++;
   for (int i = 1; i <= kn.max_sub_steps; ++i) {
     if (i > 1) frst = false;
     double t_0 = dtdone, t_1 = fmin(dtdone + dttry, dtwant);
@@ -480,6 +504,7 @@ __device__ int dev_integrate_zone(const DevNet &N, const Ws &W, ZoneCtl &C, doub
     }
     if (my_t9 != t9_last || my_rho != rho_last) {
       dev_eval_rates(N, W, my_t9, my_rho, ye, yps, sred);
+      C.rates_ver++;
       t9_last = my_t9; rho_last = my_rho;
     }
     // NSE above nse_min_t9 (solver.F90:153-158; do_one_time_step, solver.F90:260-266)
@@ -488,6 +513,7 @@ __device__ int dev_integrate_zone(const DevNet &N, const Ws &W, ZoneCtl &C, doub
     int ierr = 0;
     if (my_t9 >= kn.min_t9_for_slv) {
       if (do_nse) {
+        C.act_ok = false;  // the NSE step works in the same shared memory
         if (kn.nse_weak_method == 0)
           ierr = dev_nse_euler(N, W, C.nse, yps, my_t9, my_rho, ye, dttry, dtrcmd, C.smem, C.smem_bytes, sred);
         else

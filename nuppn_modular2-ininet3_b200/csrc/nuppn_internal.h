@@ -106,7 +106,8 @@ struct WsLayout {
   size_t rhs_key, rhs_val, rhs_piece;  // grouping of the right-hand side's frozen-reactant terms
   size_t rhs_acc, rhs_tag, rhs_list;   // per-warp key accumulators of that grouping
   size_t rhs_spc;                      // species -> active row of the step
-  size_t rhs_rkey, rhs_rcf;            // each reaction's class and constant of the step
+  size_t cache_mask, cache_xn;         // mask and abundances of the last build of the active subsystem
+  size_t rhs_rkey, rhs_rcf, rhs_rpk;   // each reaction's class, constant and packed own term of the step
   size_t jac_long;                     // long Jacobian entries of the step and their pieces
   size_t nse;                    // NSE work arrays [5 * nsp + nse_p2] doubles
   size_t nse_stride;             // nsp: the length of each NSE work array but the last

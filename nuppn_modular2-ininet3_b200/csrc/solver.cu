@@ -644,6 +644,9 @@ __device__ __forceinline__ void run_zone(const DevNet &N, const Ws &W, const Int
   C.smem = smem;
   C.smem_bytes = act_smem;
   C.sint = sint;
+  C.rates_ver = 0;
+  C.built_ver = -1;
+  C.act_ok = false;
   nse_reset(C.nse);
   int ierr, fail = -1;
   if (!seq_ok) {

@@ -76,8 +76,11 @@ struct Ws {
   int *rhs_piece;     // first piece of each active row [nsys+1], groups of each piece
   double *rhs_acc;    // key accumulators of the grouping, one per warp [warps * 8 * (nsys+1)]
   int *rhs_spc;       // species -> active row of the current step, -1 if frozen [nsp]
+  uint8_t *cache_mask;  // mask of the last build of the active subsystem [nsp]
+  double *cache_xn;     // molar abundances it was built with [nsp]
   int *rhs_rkey;      // each reaction's class of the step [nact]
   double *rhs_rcf;    // its constant [nact]
+  uint32_t *rhs_rpk;  // packed reactants of an own-term reaction [nact]
   int *jac_long;      // long Jacobian entries: flags, positions, first pieces [3 * (nnzLU + 1)]
   int *rhs_tag, *rhs_list;
   double *nse_x, *nse_gtot, *nse_mc, *nse_lm, *nse_y1, *nse_sort;  // NSE work arrays
@@ -110,8 +113,11 @@ __device__ __forceinline__ Ws ws_bind(char *base, const WsLayout &L) {
   w.rhs_piece = (int *)(base + L.rhs_piece);
   w.rhs_acc = (double *)(base + L.rhs_acc);
   w.rhs_spc = (int *)(base + L.rhs_spc);
+  w.cache_mask = (uint8_t *)(base + L.cache_mask);
+  w.cache_xn = (double *)(base + L.cache_xn);
   w.rhs_rkey = (int *)(base + L.rhs_rkey);
   w.rhs_rcf = (double *)(base + L.rhs_rcf);
+  w.rhs_rpk = (uint32_t *)(base + L.rhs_rpk);
   w.jac_long = (int *)(base + L.jac_long);
   w.rhs_tag = (int *)(base + L.rhs_tag);
   w.rhs_list = (int *)(base + L.rhs_list);
