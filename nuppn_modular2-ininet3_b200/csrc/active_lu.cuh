@@ -1013,22 +1013,6 @@ __device__ __forceinline__ void rhs_classify_reactions(const DevNet &N, const Ws
   }
 }
 
-// Items [t0, t1) of a masked row's static list (items[t] = reaction a << 2 | slot m, coefs[t] the
-// slot's coefficient -k2, -1, k6 or k8) with their reactions' classes: own-term flag, group key and
-// value coefficient * rcf[a].
-__device__ __forceinline__ void rhs_classify(const int *rkey, const double *rcf, const int *items,
-                                             const double *coefs, int t0, int t1, int *flag, int *fkey, double *fval) {
-  const int lane = threadIdx.x & 31;
-#pragma unroll 4
-  for (int t = t0 + lane; t < t1; t += 32) {
-    const int a = items[t] >> 2;
-    const int key = rkey[a];
-    flag[t] = key < 0 ? 1 : 0;
-    fkey[t] = key;
-    fval[t] = key < 0 ? 0.0 : coefs[t] * rcf[a];
-  }
-}
-
 // Per-warp key accumulator in the CTA's workspace: acc[key] the running sum of a key, tag[key] 1 once
 // the key has a value in the current piece or row, list[] the keys in the order they first came.
 // Entries are zero outside the keys in the list, which are cleared when the list is emitted.
@@ -1147,16 +1131,87 @@ __device__ __forceinline__ int group_items(int *key, double *val, int n, const K
   return nk;
 }
 
+// One piece of a masked row's static list, items [t0, t1) (items[t] = reaction a << 2 | slot m,
+// coefs[t] the slot's coefficient -k2, -1, k6 or k8), taken by one warp 32 at a time: items of
+// reactions whose reactants are all masked or gamma (rkey -1) are counted into own (they become terms
+// of their own), the others are summed per group key (value = coefficient * rcf[a]) straight from
+// registers. Up to 32 keys: lane i holds the i-th key (in the order of first appearance), each lane
+// adds its own items into a private sum per key, and a key's 32 private sums are added by a
+// butterfly, which gives every lane the same bits whatever their order. Past 32 keys the piece is
+// grouped again through the workspace accumulator K. The groups are written to gkey / gval, the
+// number of groups returned.
+__device__ __forceinline__ int rhs_piece(const int *rkey, const double *rcf, const int *items, const double *coefs,
+                                         int t0, int t1, int *gkey, double *gval, const KeyAcc &K, int &own) {
+  const int lane = threadIdx.x & 31;
+  double lacc[32];
+  int gk = -1, ng = 0, nown = 0;
+  bool ovf = false;
+  for (int b = t0; b < t1 && !ovf; b += 32) {
+    const int t = b + lane;
+    const int a = t < t1 ? items[t] >> 2 : 0;
+    const int k = t < t1 ? rkey[a] : -2;
+    const double v = k >= 0 ? coefs[t] * rcf[a] : 0.0;
+    nown += __popc(__ballot_sync(NUPPN_FULL, k == -1));
+    int slot = -1;
+    for (int j = 0; j < ng; ++j)
+      if (__shfl_sync(NUPPN_FULL, gk, j) == k) slot = j;
+    unsigned pend = __ballot_sync(NUPPN_FULL, k >= 0 && slot < 0);
+    while (pend) {  // keys seen for the first time, in the order of their first lane
+      const int k0 = __shfl_sync(NUPPN_FULL, k, __ffs(pend) - 1);
+      if (ng < 32) {
+        if (lane == ng) gk = k0;
+        lacc[ng] = 0.0;
+        if (k == k0) slot = ng;
+        ++ng;
+      } else {
+        ovf = true;
+      }
+      pend &= ~__ballot_sync(NUPPN_FULL, k == k0);
+    }
+    if (slot >= 0) lacc[slot] += v;
+  }
+  if (!ovf) {
+    double gs = 0.0;
+    for (int j = 0; j < ng; ++j) {
+      double x = lacc[j];
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(NUPPN_FULL, x, o);
+      if (lane == j) gs = x;
+    }
+    if (lane < ng) {
+      gkey[lane] = gk;
+      gval[lane] = gs;
+    }
+    __syncwarp();
+    own = nown;
+    return ng;
+  }
+  int nk = 0;
+  nown = 0;
+  for (int b = t0; b < t1; b += 32) {
+    const int t = b + lane;
+    const int a = t < t1 ? items[t] >> 2 : 0;
+    const int k = t < t1 ? rkey[a] : -2;
+    nown += __popc(__ballot_sync(NUPPN_FULL, k == -1));
+    group_chunk(k >= 0 ? k : -1, k >= 0 ? coefs[t] * rcf[a] : 0.0, K, nk);
+  }
+  group_emit(K, nk, gkey, gval);
+  own = nown;
+  return nk;
+}
+
 __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem, size_t smem_bytes, int *sint) {
   const int tid = GT, nt = GN, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
   const int *sys2c = W.act_tmp;              // system index -> active row (dev_compact), -1 if frozen
   int *cnt = W.act_tmp + 2 * (N.nsys + 1);   // [na+1] gather items per row, then row offsets
   int *off = W.act_tmp + 3 * (N.nsys + 1);   // [na+1] offsets of the rows' static lists
-  int *flag = W.act_itmp;                    // [T+1] own-term flags, then their positions
-  int *fkey = W.rhs_key;                     // [T] group key of each item (-1: own term), then groups
-  double *fval = W.rhs_val;                  // [T] its value, then group sums
+  int *fkey = W.rhs_key;                     // [T] each piece's groups over its first items, then a row's
+  double *fval = W.rhs_val;                  // [T] their sums
+  const int npmax = (N.nsys + 1) + N.ndg_item / kRhsPiece + 1;
   int *pofs = W.rhs_piece;                   // [na+1] first piece of each row
   int *pcnt = W.rhs_piece + (N.nsys + 1);    // [pieces] groups of each piece
+  int *pown = pcnt + npmax;                  // [pieces] own terms of each piece
+  int *poof = pown + npmax;                  // [pieces] own terms of the row's earlier pieces
+  int *rown = poof + npmax;                  // [na] own terms of each row
   int *spc = W.rhs_spc;                      // [nsp] species -> active row, -1 if frozen
   int *rkey = W.rhs_rkey;                    // [nact] each reaction's class: -1 own terms, else group key
   double *rcf = W.rhs_rcf;                   // [nact] its frozen factors' constant
@@ -1187,27 +1242,31 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
     pofs[na] = NP;
   }
   GSYNC();
-  // each piece (a warp): its items classified, own-term flags set, frozen-reactant items grouped
+  // each piece (a warp): its own terms counted, its frozen-reactant items grouped
   for (int P = w; P < NP; P += nw) {
     const int c = seg_of(pofs, na, P);
     const int t0 = off[c] + (P - pofs[c]) * kRhsPiece, t1 = min(t0 + kRhsPiece, off[c + 1]);
     const int base = N.dg_ptr[N.sp_of_sys[A.arow[c]]] - off[c];
-    rhs_classify(rkey, rcf, N.dg_item + base, N.dg_coef + base, t0, t1, flag, fkey, fval);
-    __syncwarp();
-    const int n = group_items(fkey + t0, fval + t0, t1 - t0, K);
-    if (lane == 0) pcnt[P] = n;
+    int own = 0;
+    const int n = rhs_piece(rkey, rcf, N.dg_item + base, N.dg_coef + base, t0, t1, fkey + t0, fval + t0, K, own);
+    if (lane == 0) {
+      pcnt[P] = n;
+      pown[P] = own;
+    }
   }
   GSYNC();
-  const int nS = block_scan_excl(flag, T, sint);
-  if (tid == 0) flag[T] = nS;
-  GSYNC();
-  for (int c = w; c < na; c += nw) {  // rows of several pieces: their pieces' groups grouped again
-    const int npc = pofs[c + 1] - pofs[c];
-    int n = npc == 1 ? pcnt[pofs[c]] : 0;
+  for (int c = w; c < na; c += nw) {  // per row: own terms before each piece; several pieces' groups merged
+    const int p0 = pofs[c], npc = pofs[c + 1] - p0;
+    int own = 0;
+    for (int P = p0; P < p0 + npc; ++P) {
+      if (lane == 0) poof[P] = own;
+      own += pown[P];
+    }
+    int n = npc == 1 ? pcnt[p0] : 0;
     if (npc > 1) {
       // move the pieces' groups together at the row's start, in piece order, then group them
-      for (int P = pofs[c]; P < pofs[c + 1]; ++P) {
-        const int s0 = off[c] + (P - pofs[c]) * kRhsPiece, np = pcnt[P];
+      for (int P = p0; P < p0 + npc; ++P) {
+        const int s0 = off[c] + (P - p0) * kRhsPiece, np = pcnt[P];
         for (int b = 0; b < np; b += 32) {  // s0 >= off[c] + n: moves go down or stay
           const int i = b + lane;
           const int k = i < np ? fkey[s0 + i] : -1;
@@ -1223,7 +1282,10 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
       }
       n = group_items(fkey + off[c], fval + off[c], n, K);
     }
-    if (lane == 0) cnt[c] = (flag[off[c + 1]] - flag[off[c]]) + n;
+    if (lane == 0) {
+      cnt[c] = own + n;
+      rown[c] = own;
+    }
   }
   GSYNC();
   const int ngi = block_scan_excl(cnt, na, sint);
@@ -1246,17 +1308,24 @@ __device__ void dev_compact_rhs(const DevNet &N, const Ws &W, Act &A, char *smem
   for (int P = w; P < NP; P += nw) {  // own terms first, in the static list's order (a warp per piece)
     const int c = seg_of(pofs, na, P);
     const int t0 = off[c] + (P - pofs[c]) * kRhsPiece, t1 = min(t0 + kRhsPiece, off[c + 1]);
-    const int base = N.dg_ptr[N.sp_of_sys[A.arow[c]]] - off[c], q0 = cnt[c] - flag[off[c]];
-    for (int t = t0 + lane; t < t1; t += 32) {
-      if (flag[t + 1] == flag[t]) continue;
-      const int a = N.dg_item[base + t] >> 2, q = q0 + flag[t];
-      A.gcoef[q] = (float)N.dg_coef[base + t];  // -k2, -1, k6 or k8: small integers, exact
-      A.grcv[q] = rcf[a];
-      A.grpk[q] = rpk[a];
+    const int base = N.dg_ptr[N.sp_of_sys[A.arow[c]]] - off[c];
+    int q = cnt[c] + poof[P];
+    for (int b = t0; b < t1; b += 32) {
+      const int t = b + lane;
+      const int a = t < t1 ? N.dg_item[base + t] >> 2 : 0;
+      const bool own = t < t1 && rkey[a] == -1;
+      const unsigned m = __ballot_sync(NUPPN_FULL, own);
+      if (own) {
+        const int qq = q + __popc(m & ((1u << lane) - 1u));
+        A.gcoef[qq] = (float)N.dg_coef[base + t];  // -k2, -1, k6 or k8: small integers, exact
+        A.grcv[qq] = rcf[a];
+        A.grpk[qq] = rpk[a];
+      }
+      q += __popc(m);
     }
   }
   for (int c = w; c < na; c += nw) {  // then the row's groups
-    const int own = flag[off[c + 1]] - flag[off[c]];
+    const int own = rown[c];
     const int q0 = cnt[c] + own, ng = (c + 1 < na ? cnt[c + 1] : ngi) - q0;
     for (int i = lane; i < ng; i += 32) put_group_item(A, q0 + i, fkey[off[c] + i], fval[off[c] + i]);
   }

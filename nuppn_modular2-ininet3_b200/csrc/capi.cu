@@ -195,7 +195,7 @@ nuppn_status upload(nuppn_net *net) {
   D.nc = H.nc; D.nr = H.nr; D.npart = H.npart; D.nv = H.nv;
   D.ngk = H.ngk; D.ngn = H.ngn; D.ngd = H.ngd; D.ffv = H.ffv; D.fft = H.fft; D.ffr = H.ffr;
   D.kdn = H.kdn; D.kde = H.kde;
-  D.njg_long = (int)H.jg_long.size(); D.ndg_long = (int)H.dg_long.size();
+  D.njg_long = (int)H.jg_long.size(); D.ndg_long = (int)H.dg_long.size(); D.ndg_item = (int)H.dg_item.size();
   D.nlvL = (int)H.lvL_ptr.size() - 1; D.nlvU = (int)H.lvU_ptr.size() - 1;
   memcpy(D.nseq, H.nseq, sizeof(D.nseq));
   memcpy(D.bd_a, H.bd_a, sizeof(D.bd_a));
@@ -226,7 +226,6 @@ WsLayout layout(const HostNet &H) {
     size_t ngi = H.dg_item.size();
     L.act_r = take(rhs_bytes(H.nsys, (int)ngi));
     size_t njg = H.jg_item.size();
-    L.act_itmp = take((std::max(ngi, njg) + 1) * sizeof(int));
     L.act_otmp = take(((size_t)H.nnzLU + 1) * sizeof(int));
     L.act_dtmp = take(njg * sizeof(double));
     L.act_btmp = take(njg);
@@ -236,7 +235,8 @@ WsLayout layout(const HostNet &H) {
     const size_t ngi = H.dg_item.size();
     L.rhs_key = take(ngi * sizeof(int));
     L.rhs_val = take(ngi * sizeof(double));
-    L.rhs_piece = take((2 * ((size_t)H.nsys + 1) + ngi / kRhsPiece + 1) * sizeof(int));
+    const size_t npmax = ((size_t)H.nsys + 1) + ngi / kRhsPiece + 1;  // pieces of the active rows, at most
+    L.rhs_piece = take(((size_t)H.nsys + 1 + 4 * npmax) * sizeof(int));
     const size_t keys = (size_t)kRhsWarps * kRhsKeysPerRow * ((size_t)H.nsys + 1);
     L.rhs_acc = take(keys * sizeof(double));
     L.rhs_tag = take(keys * sizeof(int));

@@ -67,6 +67,7 @@ struct DevNet {
   const int *jrow, *jcol, *jdiag;          // jdiag[nsp]: entry of (i,i) or -1
   const int *jg_ptr, *jg_item;             // entry -> (a*8 + s) in reference accumulation order
   const int *jg_oth;                       // per jg item: the other reactant's species, -1 for gamma
+  int ndg_item;                            // dg items of all species
   const int *dg_ptr, *dg_item;             // species -> (a*4 + slot) in scatter order
   const double *dg_coef;                   // coefficient of each dg item: -k2, -1, k6, k8
   int njg_long, ndg_long;
@@ -102,7 +103,7 @@ struct WsLayout {
   size_t y, y_old, y_cur, y_new, y_k, delta_k, y_ext, yscal, qcol, yerr, lu, bsys, xsys, rhs;
   size_t act_tmp, act;           // compaction scratch (ints) and the global fallback of the active LU
   size_t act_r;                  // global fall-back of the restricted right-hand side
-  size_t act_itmp, act_otmp, act_dtmp, act_btmp, bd;  // flattened-gather scratch, compact BD vectors
+  size_t act_otmp, act_dtmp, act_btmp, bd;  // flattened-gather scratch, compact BD vectors
   size_t rhs_key, rhs_val, rhs_piece;  // grouping of the right-hand side's frozen-reactant terms
   size_t rhs_acc, rhs_tag, rhs_list;   // per-warp key accumulators of that grouping
   size_t rhs_spc;                      // species -> active row of the step

@@ -73,7 +73,7 @@ struct Ws {
   char *act_r;   // global fallback of the restricted right-hand side
   int *rhs_key;       // right-hand side items' group keys, then group keys [dg items]
   double *rhs_val;    // their values, then group sums [dg items]
-  int *rhs_piece;     // first piece of each active row [nsys+1], groups of each piece
+  int *rhs_piece;     // first piece of each active row [nsys+1]; per piece groups, own terms, own offsets; per row own terms
   double *rhs_acc;    // key accumulators of the grouping, one per warp [warps * 8 * (nsys+1)]
   int *rhs_spc;       // species -> active row of the current step, -1 if frozen [nsp]
   uint8_t *cache_mask;  // mask of the last build of the active subsystem [nsp]
@@ -84,7 +84,6 @@ struct Ws {
   int *jac_long;      // long Jacobian entries: flags, positions, first pieces [3 * (nnzLU + 1)]
   int *rhs_tag, *rhs_list;
   double *nse_x, *nse_gtot, *nse_mc, *nse_lm, *nse_y1, *nse_sort;  // NSE work arrays
-  int *act_itmp; // flattened-list flags / positions [max(list items) + 1]
   int *act_otmp; // segment offsets of the active Jacobian entries [nnzLU + 1]
   double *act_dtmp;   // flattened Jacobian contributions [jg items]
   uint8_t *act_btmp;  // flattened entry-set flags [jg items]
@@ -127,7 +126,6 @@ __device__ __forceinline__ Ws ws_bind(char *base, const WsLayout &L) {
   w.nse_lm = w.nse_mc + L.nse_stride;
   w.nse_y1 = w.nse_lm + L.nse_stride;
   w.nse_sort = w.nse_y1 + L.nse_stride;
-  w.act_itmp = (int *)(base + L.act_itmp);
   w.act_otmp = (int *)(base + L.act_otmp);
   w.act_dtmp = (double *)(base + L.act_dtmp);
   w.act_btmp = (uint8_t *)(base + L.act_btmp);
