@@ -430,7 +430,8 @@ def run_serve(args, rank, world):
     on the 300-species network (T9 U[0.015, 0.08], rho log-U[1, 1e3], BD over 1e10 s), 20 % tppnp
     trajectories (1109 species, 21 points to 10 s), submitted as they arrive to two servers (one per
     network, 2/3 and 1/3 of the GPU's zone slots) and polled from this thread. The same stream is
-    served twice: by the batched form (one zone per warp) and by the plain form (one zone per CTA).
+    served by the plain form (one zone per CTA) and then by the batched form (one zone per warp),
+    as --serve-shapes lists them. A stream cut at --serve-limit is reported as it stood then.
     value = accepted zone sub-steps of all requests / (last completion - first arrival); latency =
     completion - arrival, from the polling loop."""
     if rank != 0:
@@ -489,10 +490,14 @@ def run_serve(args, rank, world):
         t0 = time.perf_counter()
         nxt = 0
         last_done = t0
+        cut = False
         with ClockSampler(dev) as clk:
             clk.mark()
             while nxt < arrive.size or out:
                 now = time.perf_counter() - t0
+                if now > args.serve_limit:  # stop waiting: report what completed by then
+                    cut = True
+                    break
                 while nxt < arrive.size and arrive[nxt] <= now:
                     out[nxt] = submit(nxt)
                     nxt += 1
@@ -509,37 +514,55 @@ def run_serve(args, rank, world):
                         fails[kinds[i]][str(r[2])] = fails[kinds[i]].get(str(r[2]), 0) + 1
                     del out[i]
                 time.sleep(1e-4)
-        elapsed = last_done - t0 - (arrive[0] if arrive.size else 0.0)
+        elapsed = max(last_done - t0 - (arrive[0] if arrive.size else 0.0), 1e-9)
         info = (s1107.info(), s300.info())
-        s1107.close()
-        s300.close()
-        allv = np.concatenate([np.array(v) for v in lat if v]) if arrive.size else np.zeros(1)
+        done_n = sum(len(v) for v in lat)
+        allv = np.concatenate([np.array(v) for v in lat if v]) if done_n else np.zeros(1)
         pct = lambda v: {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99))} if len(v) else None
-        return {"value": steps / elapsed, "latency_ms": {"all": pct(allv), "heshell_zone": pct(lat[0]),
-                                                         "hburn_zone": pct(lat[1]), "trajectory": pct(lat[2])},
-                "requests_failed": {"heshell_zone": fails[0], "hburn_zone": fails[1], "trajectory": fails[2]},
-                "drain_s": float(elapsed - args.serve_seconds),
-                "zone_slots": {"1107": info[0].slots, "300": info[1].slots},
-                "loop_launches": int(info[0].launches + info[1].launches), "clocks": clk.summary()}
+        res = {"value": steps / elapsed, "latency_ms": {"all": pct(allv), "heshell_zone": pct(lat[0]),
+                                                        "hburn_zone": pct(lat[1]), "trajectory": pct(lat[2])},
+               "requests_failed": {"heshell_zone": fails[0], "hburn_zone": fails[1], "trajectory": fails[2]},
+               "drain_s": float(elapsed - args.serve_seconds),
+               "requests": {"arrived": int(nxt), "completed": int(done_n), "unfinished_at_limit": int(len(out)),
+                            "limit_s": float(args.serve_limit), "cut_at_limit": bool(cut)},
+               "zone_slots": {"1107": info[0].slots, "300": info[1].slots},
+               "in_flight_at_end": {"1107": int(info[0].in_flight), "300": int(info[1].in_flight)},
+               "pending_at_end": {"1107": int(info[0].pending), "300": int(info[1].pending)},
+               "loop_launches": int(info[0].launches + info[1].launches), "clocks": clk.summary()}
+        print(json.dumps({"serve_stream": shape, **res}), file=sys.stderr, flush=True)  # before the servers close
+        if cut:  # requests still on the GPU: leave the servers to the process's exit instead of waiting
+            open_servers.extend([s1107, s300])
+        else:
+            s1107.close()
+            s300.close()
+        return res
 
-    batched = serve_stream({"threads_per_zone": 32})
-    plain = serve_stream({})
-    print(json.dumps({"metric": "zone-timesteps/s", "value": batched["value"], "unit": "zone-timesteps/s",
-                      "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
-                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                      "data": "synthetic",
-                      "config": {"workload": "serve: Poisson stream, 40% heshell-1107 zones, 40% hburn-300 zones, "
-                                             "20% tppnp-1107 trajectories (21 points)",
-                                 "rate_req_per_s": args.rate, "arrival_window_s": args.serve_seconds,
-                                 "requests": int(arrive.size), "form": "one zone per warp, device-resident loop"},
-                      "latency_ms": batched["latency_ms"], "requests_failed": batched["requests_failed"],
-                      "drain_s": batched["drain_s"], "zone_slots": batched["zone_slots"],
-                      "plain_form": {k: plain[k] for k in ("value", "latency_ms", "requests_failed", "drain_s",
-                                                           "zone_slots")},
-                      "batched_over_plain": batched["value"] / plain["value"] if plain["value"] else None,
-                      "e2e": {"value": batched["value"], "unit": "zone-timesteps/s",
-                              "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
-                      "gpu_launches": batched["loop_launches"], "clocks": batched["clocks"]}), flush=True)
+    open_servers = []
+    shapes = args.serve_shapes.split(",")
+    plain = serve_stream({}) if "plain" in shapes else None
+    batched = serve_stream({"threads_per_zone": 32}) if "batched" in shapes and not open_servers else None
+    first = plain if plain is not None else batched
+    form = "one zone per warp" if first is batched else "one zone per CTA"
+    line = {"metric": "zone-timesteps/s", "value": first["value"], "unit": "zone-timesteps/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "serve: Poisson stream, 40% heshell-1107 zones, 40% hburn-300 zones, "
+                                   "20% tppnp-1107 trajectories (21 points)",
+                       "rate_req_per_s": args.rate, "arrival_window_s": args.serve_seconds,
+                       "requests": int(arrive.size), "form": form + ", device-resident loop"},
+            "latency_ms": first["latency_ms"], "requests_failed": first["requests_failed"],
+            "drain_s": first["drain_s"], "requests": first["requests"], "zone_slots": first["zone_slots"],
+            "e2e": {"value": first["value"], "unit": "zone-timesteps/s",
+                    "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+            "gpu_launches": first["loop_launches"], "clocks": first["clocks"]}
+    if batched is not None and plain is not None:
+        line["batched_form"] = {k: batched[k] for k in ("value", "latency_ms", "requests_failed", "drain_s",
+                                                        "requests", "zone_slots")}
+        line["batched_over_plain"] = batched["value"] / plain["value"] if plain["value"] else None
+    print(json.dumps(line), flush=True)
+    if open_servers:  # a stream was cut at its limit: its requests end with the process, not waited for
+        os._exit(0)
 
 
 def run_mixed(args, rank, world):
@@ -697,6 +720,10 @@ def main():
                          "H-burning zone (200 backward-Euler frame steps)")
     ap.add_argument("--rate", type=float, default=2000.0, help="serve: mean requests per second")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="serve: arrival window (s)")
+    ap.add_argument("--serve-limit", type=float, default=600.0,
+                    help="serve: seconds after the first arrival at which the stream stops being waited for")
+    ap.add_argument("--serve-shapes", default="plain,batched",
+                    help="serve: kernel shapes to serve the stream with, in order: plain (zone per CTA), batched")
     args = ap.parse_args()
     if args.nz is None:
         args.nz = 4096 if args.workload == "mixed" else 1024
