@@ -978,9 +978,11 @@ __device__ bool dev_solve_species(const DevNet &N, Act &A, const double *rhs, do
 //    group's constant, the sum over its reactions of coefficient * (1/k2!) * rate * the frozen
 //    reactant's xn (to the power k2 for the first reactant), formed once per step. A group sums in
 //    another order than the reference's loop, which changes the row's sum at the rounding level.
-// Groups are found deterministically: a row's static list is cut into pieces of kRhsPiece items,
-// a warp sums each piece's items per key (a fixed butterfly per key and chunk of 32 items, then the
-// chunks in order), and a warp per row sums its pieces' groups in piece order.
+// Per step: every reaction is classified once (rhs_classify_reactions); a row's static list is cut
+// into pieces of kRhsPiece items, a warp counts a piece's own terms and sums its other items per
+// key (lane-private sums, then a fixed butterfly per key: rhs_piece), a warp per row adds its
+// pieces' groups in piece order (group_items), and the own terms are placed in the static list's
+// order. Every sum depends only on the items' positions, so results are bit-reproducible.
 
 // Every considered reaction classified once per step, block-parallel and coalesced over reactions:
 // rkey[a] = -1 if its reactants are all masked or gamma (each of its slots in a masked row is then a
