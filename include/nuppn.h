@@ -248,6 +248,26 @@ nuppn_status nuppn_networksetup_write(const char *path, const nuppn_netsetup *ns
  * false are marked not considered. */
 nuppn_status nuppn_networksetup_read(const char *path, nuppn_netsetup *ns);
 
+/* -- ppn's per-cycle output files (printonecycle, frames/ppn/source/ppn.F90:431-539), byte for byte,
+ *    in the reference's fixed columns, so NuGrid tools read them unchanged. Host only. --------------- */
+
+/* iso_massf<mmmmm>.DAT (ppn.F90:519-536): the header, the model line (model, dzeit, agej), T9 and rho,
+ * the neutron, proton and alpha number densities (the reference writes X * rho * N_A for n and p and
+ * X(He4) / 4 * rho * N_A for alpha), the total energy flux, then one line per species whose
+ * consider[i] is nonzero (all when consider is NULL): index, Z, A, isomeric state (1 when the array is
+ * NULL), max(X, 1e-99) and the 5-character name (names: [nsp][5], not terminated). */
+nuppn_status nuppn_write_iso_massf(const char *path, int32_t model, double dzeit, double agej, double t9, double rho,
+                                   double densn, double densp, double densa, double total_energy_flux, int32_t nsp,
+                                   const double *z, const double *a, const int32_t *isomeric_state, const double *x,
+                                   const char *names, const uint8_t *consider);
+
+/* flux_<mmmmm>.DAT (ppn.F90:496-510): one line per network reaction i < nreac with Z and A of its
+ * k1, k3, k5 and k7 species (k: [nreac][8] 0-based species indices in the k1..k8 slot order of the
+ * network description), max(flux, 1e-99), max(energy, 1e-99) and max(timescale, 1e99), as the
+ * reference prints them (energy = flux * bind_energy_diff, in erg/(g s)). */
+nuppn_status nuppn_write_flux(const char *path, int32_t nreac, const int32_t *k, const double *z, const double *a,
+                              const double *flux, const double *energy, const double *timescale);
+
 /* Static Jacobian pattern of makemap (jac_rhs.F90:461-540): row/col (0-based) of each COO entry in
  * the reference's row-major numbering, and dns2csr_map[nre][8] (entry index per slot, -1 if the
  * reaction is not considered). Sizes: row/col [nnz_jac]. */

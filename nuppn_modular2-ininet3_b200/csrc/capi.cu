@@ -548,6 +548,32 @@ nuppn_status nuppn_networksetup_read(const char *path, nuppn_netsetup *ns) {
   return NUPPN_OK;
 }
 
+nuppn_status nuppn_write_iso_massf(const char *path, int32_t model, double dzeit, double agej, double t9, double rho,
+                                   double densn, double densp, double densa, double total_energy_flux, int32_t nsp,
+                                   const double *z, const double *a, const int32_t *isomeric_state, const double *x,
+                                   const char *names, const uint8_t *consider) {
+  if (!path || nsp < 0 || (nsp > 0 && (!z || !a || !x || !names))) { set_error("null argument"); return NUPPN_ERR_ARG; }
+  if (!write_iso_massf(path, model, dzeit, agej, t9, rho, densn, densp, densa, total_energy_flux, nsp, z, a,
+                       isomeric_state, x, names, consider)) {
+    set_error(std::string("cannot write ") + path);
+    return NUPPN_ERR_ARG;
+  }
+  return NUPPN_OK;
+}
+
+nuppn_status nuppn_write_flux(const char *path, int32_t nreac, const int32_t *k, const double *z, const double *a,
+                              const double *flux, const double *energy, const double *timescale) {
+  if (!path || nreac < 0 || (nreac > 0 && (!k || !z || !a || !flux || !energy || !timescale))) {
+    set_error("null argument");
+    return NUPPN_ERR_ARG;
+  }
+  if (!write_flux(path, nreac, k, z, a, flux, energy, timescale)) {
+    set_error(std::string("cannot write ") + path);
+    return NUPPN_ERR_ARG;
+  }
+  return NUPPN_OK;
+}
+
 nuppn_status nuppn_jac_pattern(const nuppn_net *net, int32_t *row, int32_t *col, int32_t *map) {
   if (!net) return NUPPN_ERR_ARG;
   const HostNet &H = net->H;

@@ -89,4 +89,11 @@ std::string read_isotope_database(const char *path, int nnn, std::vector<Isotope
 std::string write_networksetup(const char *path, const nuppn_netsetup &ns);
 std::string read_networksetup(const char *path, nuppn_netsetup &ns);
 
+// ppn's per-cycle output files (output.cpp)
+bool write_iso_massf(const char *path, int model, double dzeit, double agej, double t9, double rho, double densn,
+                     double densp, double densa, double total_energy_flux, int nsp, const double *z, const double *a,
+                     const int *isomeric_state, const double *x, const char *names, const uint8_t *consider);
+bool write_flux(const char *path, int nreac, const int *k, const double *z, const double *a, const double *flux,
+                const double *energy, const double *timescale);
+
 }  // namespace nuppn

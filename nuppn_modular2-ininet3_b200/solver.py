@@ -59,6 +59,9 @@ def load_library():
     L.nuppn_networksetup_write.argtypes = [C.c_char_p, vp]
     L.nuppn_networksetup_read.argtypes = [C.c_char_p, vp]
     L.nuppn_isotopedatabase_read.argtypes = [C.c_char_p, i32, vp, vp, vp, C.c_char_p]
+    d = C.c_double
+    L.nuppn_write_iso_massf.argtypes = [C.c_char_p, i32, d, d, d, d, d, d, d, d, i32, vp, vp, vp, vp, vp, vp]
+    L.nuppn_write_flux.argtypes = [C.c_char_p, i32, vp, vp, vp, vp, vp, vp]
     L.nuppn_launch_count.argtypes = [vp]
     L.nuppn_launch_count.restype = i64
     L.nuppn_nse.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp]
@@ -78,7 +81,7 @@ def load_library():
                  "nuppn_serve_open", "nuppn_serve_submit", "nuppn_serve_submit_trajectory", "nuppn_serve_poll",
                  "nuppn_serve_info", "nuppn_serve_close", "nuppn_autotune", "nuppn_integrate_multi",
                  "nuppn_integrate_multi_device", "nuppn_networksetup_write", "nuppn_networksetup_read",
-                 "nuppn_isotopedatabase_read"):
+                 "nuppn_isotopedatabase_read", "nuppn_write_iso_massf", "nuppn_write_flux"):
         getattr(L, name).restype = i32
     _LIB = L
     return L
@@ -317,6 +320,53 @@ def networksetup_read(path):
     arr.update(zis=split(zis, nsp), lab=split(lab, nre), labb=split(labb, nre), t9=ns.t9, rho=ns.rho,
                nisomers=ns.nisomers, nreac_isomers=ns.nreac_isomers)
     return arr
+
+
+AVOGADRO = 6.022140857e23  # constants.F90:29, the value the reference's number densities use
+
+
+def write_iso_massf(path, net, X, model, dzeit, agej, t9, rho, total_energy_flux=0.0, isomeric_state=None):
+    """ppn's iso_massf<mmmmm>.DAT (printonecycle, ppn.F90:519-536) for one zone's abundances X of a
+    network description, byte for byte: the header with the neutron, proton and alpha number
+    densities as the reference computes them (X(n) rho N_A, X(p) rho N_A, X(He4)/4 rho N_A) and one
+    line per considered species. Host only."""
+    L = load_library()
+    X = np.ascontiguousarray(X, np.float64)
+    nsp = net.nsp
+    if X.shape != (nsp,):
+        raise NuppnError(f"X must have {nsp} entries")
+    yn = X[net.species_index("NEUT ")]
+    yp = X[net.species_index("PROT ")]
+    ya = X[net.species_index("HE  4")] * 0.25
+    z = np.ascontiguousarray(net.znetw, np.float64)
+    a = np.ascontiguousarray(net.anetw, np.float64)
+    iso = np.ones(nsp, np.int32) if isomeric_state is None else np.ascontiguousarray(isomeric_state, np.int32)
+    cons = np.ascontiguousarray(net.considerisotope, np.uint8)
+    names = C.create_string_buffer(_str5(net.zis), 5 * nsp)
+    st = L.nuppn_write_iso_massf(str(path).encode(), int(model), float(dzeit), float(agej), float(t9), float(rho),
+                                 yn * rho * AVOGADRO, yp * rho * AVOGADRO, ya * rho * AVOGADRO,
+                                 float(total_energy_flux), nsp, _p(z), _p(a), _p(iso), _p(X),
+                                 C.cast(names, C.c_void_p), _p(cons))
+    if st != 0:
+        raise NuppnError(L.nuppn_last_error().decode())
+
+
+def write_flux(path, net, flux, bind_energy_diff, timescale, nreac=None):
+    """ppn's flux_<mmmmm>.DAT (printonecycle, ppn.F90:496-510), byte for byte: per network reaction
+    (the first nreac slots, all by default) Z and A of k1, k3, k5 and k7, the flux dY/dt, the energy
+    flux * bind_energy_diff and the reaction's time scale, clamped as the reference prints them. Host
+    only."""
+    L = load_library()
+    n = net.nre if nreac is None else int(nreac)
+    flux = np.ascontiguousarray(flux, np.float64)[:n]
+    energy = np.ascontiguousarray(flux * np.asarray(bind_energy_diff, np.float64)[:n])
+    ts = np.ascontiguousarray(timescale, np.float64)[:n]
+    k = np.ascontiguousarray(np.asarray(net.k)[:n], np.int32)
+    z = np.ascontiguousarray(net.znetw, np.float64)
+    a = np.ascontiguousarray(net.anetw, np.float64)
+    st = L.nuppn_write_flux(str(path).encode(), n, _p(k), _p(z), _p(a), _p(flux), _p(energy), _p(ts))
+    if st != 0:
+        raise NuppnError(L.nuppn_last_error().decode())
 
 
 def _handles(solvers):
