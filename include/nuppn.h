@@ -268,6 +268,21 @@ nuppn_status nuppn_write_iso_massf(const char *path, int32_t model, double dzeit
 nuppn_status nuppn_write_flux(const char *path, int32_t nreac, const int32_t *k, const double *z, const double *a,
                               const double *flux, const double *energy, const double *timescale);
 
+/* -- tppnp's binary trajectory input (traj_data_bin_init / read_bin_trajectory,
+ *    frames/tppnp/source/traj_data.F90:73-168): a stream file of the machine's byte order. Host only. */
+
+/* The header: number of tracers and the smallest and largest time-step counts. */
+nuppn_status nuppn_tppnp_header(const char *path, int32_t *num_tracers, int32_t *nsteps_min, int32_t *nsteps_max);
+
+/* The tracer record at byte offset *pos (0: the first). With any of time..x NULL, only pnum, nsteps,
+ * niso, mass, posini[3] and posfin[3] are set (to size the arrays) and *pos is left alone; otherwise
+ * also time[nsteps] (s), t9[nsteps] (the file's temperature / 1e9, as read_trajectory divides it),
+ * rho[nsteps] (g/cm^3), the initial composition a[niso], z[niso], zis[niso][5] (not terminated) and
+ * x[niso], and *pos moves to the next tracer. NUPPN_ERR_ARG if the file is short or malformed. */
+nuppn_status nuppn_tppnp_next(const char *path, int64_t *pos, int32_t *pnum, int32_t *nsteps, int32_t *niso,
+                              double *mass, double *posini, double *posfin, double *time, double *t9, double *rho,
+                              int32_t *a, int32_t *z, char *zis, double *x);
+
 /* Static Jacobian pattern of makemap (jac_rhs.F90:461-540): row/col (0-based) of each COO entry in
  * the reference's row-major numbering, and dns2csr_map[nre][8] (entry index per slot, -1 if the
  * reaction is not considered). Sizes: row/col [nnz_jac]. */

@@ -574,6 +574,26 @@ nuppn_status nuppn_write_flux(const char *path, int32_t nreac, const int32_t *k,
   return NUPPN_OK;
 }
 
+nuppn_status nuppn_tppnp_header(const char *path, int32_t *num_tracers, int32_t *nsteps_min, int32_t *nsteps_max) {
+  if (!path || !num_tracers || !nsteps_min || !nsteps_max) { set_error("null argument"); return NUPPN_ERR_ARG; }
+  int n = 0, lo = 0, hi = 0;
+  const std::string err = tppnp_header(path, &n, &lo, &hi);
+  if (!err.empty()) { set_error(err); return NUPPN_ERR_ARG; }
+  *num_tracers = n; *nsteps_min = lo; *nsteps_max = hi;
+  return NUPPN_OK;
+}
+
+nuppn_status nuppn_tppnp_next(const char *path, int64_t *pos, int32_t *pnum, int32_t *nsteps, int32_t *niso,
+                              double *mass, double *posini, double *posfin, double *time, double *t9, double *rho,
+                              int32_t *a, int32_t *z, char *zis, double *x) {
+  if (!path || !pos || !pnum || !nsteps || !niso) { set_error("null argument"); return NUPPN_ERR_ARG; }
+  int pn = 0, nt = 0, ni = 0;
+  const std::string err = tppnp_next(path, pos, &pn, &nt, &ni, mass, posini, posfin, time, t9, rho, a, z, zis, x);
+  if (!err.empty()) { set_error(err); return NUPPN_ERR_ARG; }
+  *pnum = pn; *nsteps = nt; *niso = ni;
+  return NUPPN_OK;
+}
+
 nuppn_status nuppn_jac_pattern(const nuppn_net *net, int32_t *row, int32_t *col, int32_t *map) {
   if (!net) return NUPPN_ERR_ARG;
   const HostNet &H = net->H;

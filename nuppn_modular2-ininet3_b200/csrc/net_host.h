@@ -96,4 +96,10 @@ bool write_iso_massf(const char *path, int model, double dzeit, double agej, dou
 bool write_flux(const char *path, int nreac, const int *k, const double *z, const double *a, const double *flux,
                 const double *energy, const double *timescale);
 
+// tppnp's binary trajectory input (tppnp_io.cpp); an empty string on success, else the reason
+std::string tppnp_header(const char *path, int *num_tracers, int *nsteps_min, int *nsteps_max);
+std::string tppnp_next(const char *path, int64_t *pos, int *pnum, int *nsteps, int *niso, double *mass,
+                       double *posini, double *posfin, double *time, double *t9, double *rho, int *a, int *z,
+                       char *zis, double *x);
+
 }  // namespace nuppn

@@ -62,6 +62,8 @@ def load_library():
     d = C.c_double
     L.nuppn_write_iso_massf.argtypes = [C.c_char_p, i32, d, d, d, d, d, d, d, d, i32, vp, vp, vp, vp, vp, vp]
     L.nuppn_write_flux.argtypes = [C.c_char_p, i32, vp, vp, vp, vp, vp, vp]
+    L.nuppn_tppnp_header.argtypes = [C.c_char_p, vp, vp, vp]
+    L.nuppn_tppnp_next.argtypes = [C.c_char_p, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.nuppn_launch_count.argtypes = [vp]
     L.nuppn_launch_count.restype = i64
     L.nuppn_nse.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp]
@@ -81,7 +83,7 @@ def load_library():
                  "nuppn_serve_open", "nuppn_serve_submit", "nuppn_serve_submit_trajectory", "nuppn_serve_poll",
                  "nuppn_serve_info", "nuppn_serve_close", "nuppn_autotune", "nuppn_integrate_multi",
                  "nuppn_integrate_multi_device", "nuppn_networksetup_write", "nuppn_networksetup_read",
-                 "nuppn_isotopedatabase_read", "nuppn_write_iso_massf", "nuppn_write_flux"):
+                 "nuppn_isotopedatabase_read", "nuppn_write_iso_massf", "nuppn_write_flux", "nuppn_tppnp_header", "nuppn_tppnp_next"):
         getattr(L, name).restype = i32
     _LIB = L
     return L
@@ -367,6 +369,54 @@ def write_flux(path, net, flux, bind_energy_diff, timescale, nreac=None):
     st = L.nuppn_write_flux(str(path).encode(), n, _p(k), _p(z), _p(a), _p(flux), _p(energy), _p(ts))
     if st != 0:
         raise NuppnError(L.nuppn_last_error().decode())
+
+
+def tppnp_read(path, limit=None):
+    """tppnp's binary trajectory file (traj_data.F90:73-168): a list of dicts, one per tracer (the
+    first `limit`), with pnum, mass, posini, posfin, time (s), t9 (the file's temperature / 1e9),
+    rho (g/cm^3) and the initial composition a, z, zis (5-character names) and x. Host only."""
+    L = load_library()
+    hdr = [C.c_int32() for _ in range(3)]
+    if L.nuppn_tppnp_header(str(path).encode(), *[C.byref(h) for h in hdr]) != 0:
+        raise NuppnError(L.nuppn_last_error().decode())
+    n = hdr[0].value if limit is None else min(int(limit), hdr[0].value)
+    pos = C.c_int64(0)
+    out = []
+    for _ in range(n):
+        pn, nt, ni = C.c_int32(), C.c_int32(), C.c_int32()
+        mass = C.c_double()
+        pi, pf = np.zeros(3), np.zeros(3)
+        args = [C.byref(pos), C.byref(pn), C.byref(nt), C.byref(ni), C.byref(mass), _p(pi), _p(pf)]
+        if L.nuppn_tppnp_next(str(path).encode(), *args, None, None, None, None, None, None, None) != 0:
+            raise NuppnError(L.nuppn_last_error().decode())
+        t, t9, rho = np.zeros(nt.value), np.zeros(nt.value), np.zeros(nt.value)
+        a, z, x = np.zeros(ni.value, np.int32), np.zeros(ni.value, np.int32), np.zeros(ni.value)
+        zis = C.create_string_buffer(5 * max(ni.value, 1))
+        if L.nuppn_tppnp_next(str(path).encode(), *args, _p(t), _p(t9), _p(rho), _p(a), _p(z),
+                              C.cast(zis, C.c_void_p), _p(x)) != 0:
+            raise NuppnError(L.nuppn_last_error().decode())
+        names = [zis.raw[5 * i:5 * i + 5].decode() for i in range(ni.value)]
+        out.append({"pnum": pn.value, "mass": mass.value, "posini": pi, "posfin": pf, "time": t, "t9": t9,
+                    "rho": rho, "a": a, "z": z, "zis": names, "x": x})
+    return out, {"num_tracers": hdr[0].value, "nsteps_min": hdr[1].value, "nsteps_max": hdr[2].value}
+
+
+def tppnp_initial_abundances(net, traj):
+    """A tracer's initial composition on a network's species, matched by (Z, A), as tppnp's
+    abundance initialisation sets x_in = max(x, 1e-99) by species (traj_data.F90:160-163); species
+    the tracer does not list, and listed isotopes the network lacks, are left at 1e-99 / dropped.
+    Returns (X[nsp], the tracer's mass fraction that found no species)."""
+    X = np.full(net.nsp, 1e-99)
+    where = {(int(zz), int(aa)): i for i, (zz, aa) in enumerate(zip(net.znetw, net.anetw))
+             if net.zis[i] != "OOOOO"}
+    lost = 0.0
+    for zz, aa, xx in zip(traj["z"], traj["a"], traj["x"]):
+        i = where.get((int(zz), int(aa)))
+        if i is None:
+            lost += max(float(xx), 0.0)
+        else:
+            X[i] = max(float(xx), 1e-99)
+    return X, lost
 
 
 def _handles(solvers):
