@@ -268,6 +268,32 @@ nuppn_status nuppn_write_iso_massf(const char *path, int32_t model, double dzeit
 nuppn_status nuppn_write_flux(const char *path, int32_t nreac, const int32_t *k, const double *z, const double *a,
                               const double *flux, const double *energy, const double *timescale);
 
+/* -- mppnp's diffusive mixing between mass shells (do_mixing with idifmix = 1,
+ *    frames/mppnp/source/mixing.F90:34-342) ------------------------------------------------------ */
+
+/* mix_calculate_D_Lagrangian (mixing.F90:60-98): d_lagr[j] = d_eul[j] (4 pi Rsun^2 / Msun)^2 exp(2 (2 ln r + ln rho)),
+ * with ln r and ln rho averaged over shells j-1 and j (j > 0); 0 where d_eul <= 0. Host only. */
+nuppn_status nuppn_mix_d_lagrangian(int32_t m, const double *d_eul, const double *rho, const double *rad,
+                                    double *d_lagr);
+
+/* mixdiff08 (mixing.F90:104-146): one fully implicit diffusion step of length dzeit over m shells for
+ * the abundances X[m][ldx] (shell-major, ldx >= nsp), every species 0 .. nsp-2 whose consider[] is
+ * nonzero (all when consider is NULL; the last slot is left alone, as mixdiff08 loops to NSP-1).
+ * mesa = 0: matrixdiffus on the mass coordinates xm[m] (code_source GNV / EVL); mesa = 1:
+ * matrixdiffus_mesa on the shell masses dq[m] (MES). d_lagr[m] (host) is limited in place by
+ * sig_term_limit as those routines limit it. The matrix and its factorization are built on the host;
+ * the substitutions run on the GPU, one thread per species, with tridag's operations in its order
+ * (equal to the reference bit for bit). NUPPN_ERR_ARG for a zero pivot or a zero shell width. */
+nuppn_status nuppn_mix_diffusion(int32_t m, int32_t nsp, double *X, int32_t ldx, const double *xm, const double *dq,
+                                 double *d_lagr, double dzeit, double sig_term_limit, int32_t mesa,
+                                 const uint8_t *consider);
+
+/* The same on device-resident abundances d_X, ordered on `stream` (a cudaStream_t, NULL: the default
+ * stream); returns when the step is done. */
+nuppn_status nuppn_mix_diffusion_device(int32_t m, int32_t nsp, double *d_X, int32_t ldx, const double *xm,
+                                        const double *dq, double *d_lagr, double dzeit, double sig_term_limit,
+                                        int32_t mesa, const uint8_t *consider, void *stream);
+
 /* -- tppnp's binary trajectory input (traj_data_bin_init / read_bin_trajectory,
  *    frames/tppnp/source/traj_data.F90:73-168): a stream file of the machine's byte order. Host only. */
 

@@ -21,7 +21,8 @@ UNITS = [("solver.cu", ["-DNUPPN_GROUP_WARP=0"], "solver_cta.o"),
          ("net_host.cpp", [], "net_host.o"),
          ("netsetup.cpp", [], "netsetup.o"),
          ("output.cpp", [], "output.o"),
-         ("tppnp_io.cpp", [], "tppnp_io.o")]
+         ("tppnp_io.cpp", [], "tppnp_io.o"),
+         ("mixing.cu", [], "mixing.o")]
 # --fmad=false: products are rounded before they are added, as in the reference's CPU build (x86-64
 # without FMA). The Bader-Deuflhard error test of some cooling intervals rests on a cancellation of
 # two rounded products of the same factors (a dX/dt term against U(r, c) x(c) in the back

@@ -96,6 +96,14 @@ bool write_iso_massf(const char *path, int model, double dzeit, double agej, dou
 bool write_flux(const char *path, int nreac, const int *k, const double *z, const double *a, const double *flux,
                 const double *energy, const double *timescale);
 
+// mppnp's diffusive mixing (mixing.cu): Lagrangian coefficient, the step's tridiagonal matrix and
+// its factorization on the host; an empty string on success, else the reason
+std::string mix_d_lagrangian(int m, const double *d_eul, const double *rho, const double *rad, double *d_lagr);
+std::string mix_matrix(int m, const double *xm, const double *dq, double *d, double h, double sig, bool mesa,
+                       std::vector<double> &a, std::vector<double> &b, std::vector<double> &c);
+std::string tridag_factor(int m, const std::vector<double> &a, const std::vector<double> &b,
+                          const std::vector<double> &c, std::vector<double> &gam, std::vector<double> &bet);
+
 // tppnp's binary trajectory input (tppnp_io.cpp); an empty string on success, else the reason
 std::string tppnp_header(const char *path, int *num_tracers, int *nsteps_min, int *nsteps_max);
 std::string tppnp_next(const char *path, int64_t *pos, int *pnum, int *nsteps, int *niso, double *mass,

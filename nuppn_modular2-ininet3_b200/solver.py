@@ -63,6 +63,9 @@ def load_library():
     L.nuppn_write_iso_massf.argtypes = [C.c_char_p, i32, d, d, d, d, d, d, d, d, i32, vp, vp, vp, vp, vp, vp]
     L.nuppn_write_flux.argtypes = [C.c_char_p, i32, vp, vp, vp, vp, vp, vp]
     L.nuppn_tppnp_header.argtypes = [C.c_char_p, vp, vp, vp]
+    L.nuppn_mix_d_lagrangian.argtypes = [i32, vp, vp, vp, vp]
+    L.nuppn_mix_diffusion.argtypes = [i32, i32, vp, i32, vp, vp, vp, d, d, i32, vp]
+    L.nuppn_mix_diffusion_device.argtypes = [i32, i32, vp, i32, vp, vp, vp, d, d, i32, vp, vp]
     L.nuppn_tppnp_next.argtypes = [C.c_char_p, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.nuppn_launch_count.argtypes = [vp]
     L.nuppn_launch_count.restype = i64
@@ -83,7 +86,8 @@ def load_library():
                  "nuppn_serve_open", "nuppn_serve_submit", "nuppn_serve_submit_trajectory", "nuppn_serve_poll",
                  "nuppn_serve_info", "nuppn_serve_close", "nuppn_autotune", "nuppn_integrate_multi",
                  "nuppn_integrate_multi_device", "nuppn_networksetup_write", "nuppn_networksetup_read",
-                 "nuppn_isotopedatabase_read", "nuppn_write_iso_massf", "nuppn_write_flux", "nuppn_tppnp_header", "nuppn_tppnp_next"):
+                 "nuppn_isotopedatabase_read", "nuppn_write_iso_massf", "nuppn_write_flux", "nuppn_tppnp_header", "nuppn_tppnp_next", "nuppn_mix_d_lagrangian", "nuppn_mix_diffusion",
+                 "nuppn_mix_diffusion_device"):
         getattr(L, name).restype = i32
     _LIB = L
     return L
@@ -369,6 +373,56 @@ def write_flux(path, net, flux, bind_energy_diff, timescale, nreac=None):
     st = L.nuppn_write_flux(str(path).encode(), n, _p(k), _p(z), _p(a), _p(flux), _p(energy), _p(ts))
     if st != 0:
         raise NuppnError(L.nuppn_last_error().decode())
+
+
+def mix_d_lagrangian(d_eul, rho, rad):
+    """mppnp's mix_calculate_D_Lagrangian (mixing.F90:60-98): the Lagrangian diffusion coefficient
+    of each shell from the Eulerian one, the density and the radius (solar units). Host only."""
+    L = load_library()
+    d_eul, rho, rad = (np.ascontiguousarray(v, np.float64) for v in (d_eul, rho, rad))
+    out = np.zeros(d_eul.size)
+    if L.nuppn_mix_d_lagrangian(d_eul.size, _p(d_eul), _p(rho), _p(rad), _p(out)) != 0:
+        raise NuppnError(L.nuppn_last_error().decode())
+    return out
+
+
+def mix_diffusion(X, d_lagr, dzeit, sig_term_limit, xm=None, dq=None, consider=None):
+    """mppnp's diffusive mixing step (mixdiff08, mixing.F90:104-146) on the GPU: X[m, nsp] (shells x
+    species) after one fully implicit step of dzeit, by matrixdiffus on the mass coordinates xm, or
+    matrixdiffus_mesa on the shell masses dq when dq is given. Returns (X, d_lagr as limited by
+    sig_term_limit); X is not modified."""
+    L = load_library()
+    X = np.array(X, dtype=np.float64, order="C", copy=True)
+    d = np.array(d_lagr, dtype=np.float64, copy=True)
+    mesa = dq is not None
+    xm_ = None if mesa else np.ascontiguousarray(xm, np.float64)
+    dq_ = np.ascontiguousarray(dq, np.float64) if mesa else None
+    cons = None if consider is None else np.ascontiguousarray(consider, np.uint8)
+    if L.nuppn_mix_diffusion(X.shape[0], X.shape[1], _p(X), X.shape[1], _p(xm_), _p(dq_), _p(d), float(dzeit),
+                             float(sig_term_limit), int(mesa), _p(cons)) != 0:
+        raise NuppnError(L.nuppn_last_error().decode())
+    return X, d
+
+
+def mix_diffusion_device(X, d_lagr, dzeit, sig_term_limit, xm=None, dq=None, consider=None, stream=None):
+    """mix_diffusion on a device-resident float64 tensor X[m, ldx] (shells x species, nsp = the columns
+    to mix + 1 = X.shape[1]), in place, on `stream` (a torch.cuda.Stream or None). Returns d_lagr as
+    limited by sig_term_limit."""
+    import torch
+
+    L = load_library()
+    if not X.is_cuda or X.dtype != torch.float64 or X.dim() != 2 or X.stride(1) != 1:
+        raise NuppnError("mix_diffusion_device: X must be a 2-D float64 CUDA tensor with unit column stride")
+    d = np.array(d_lagr, dtype=np.float64, copy=True)
+    mesa = dq is not None
+    xm_ = None if mesa else np.ascontiguousarray(xm, np.float64)
+    dq_ = np.ascontiguousarray(dq, np.float64) if mesa else None
+    cons = None if consider is None else np.ascontiguousarray(consider, np.uint8)
+    sp = None if stream is None else C.c_void_p(stream.cuda_stream)
+    if L.nuppn_mix_diffusion_device(X.shape[0], X.shape[1], C.c_void_p(X.data_ptr()), X.stride(0), _p(xm_), _p(dq_),
+                                    _p(d), float(dzeit), float(sig_term_limit), int(mesa), _p(cons), sp) != 0:
+        raise NuppnError(L.nuppn_last_error().decode())
+    return d
 
 
 def tppnp_read(path, limit=None):

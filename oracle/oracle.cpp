@@ -1924,6 +1924,113 @@ int oracle_nse(void *net, int32_t nz, const double *t9, const double *rho, const
   return 0;
 }
 double oracle_sortedsum(const double *a, int32_t n) { return sortedsum(a, n); }
+
+// ---- mppnp's diffusive mixing (frames/mppnp/source/mixing.F90), restated per species as the
+// reference runs it: mix_calculate_D_Lagrangian :60-98, matrixdiffus :176-250, matrixdiffus_mesa
+// :254-323 with reduce_term :327-340, and mixdiff08 :104-146 calling tridag :150-174 for every
+// considered species 1 .. NSP-1 (0-based 0 .. nsp-2) on a fresh copy of the matrix.
+void oracle_mix_d_lagrangian(int32_t m, const double *d_eul, const double *rho, const double *rad, double *d_lagr) {
+  const double dconst = 3.0589703419947736e-11;
+  for (int j = 1; j <= m; ++j) {
+    d_lagr[j - 1] = ZERO;
+    if (d_eul[j - 1] <= ZERO) continue;
+    double lnrho, lnrad;
+    if (j == 1) {
+      lnrho = std::log(rho[j - 1]);
+      lnrad = std::log(rad[j - 1]);
+    } else {
+      lnrho = (std::log(rho[j - 1]) + std::log(rho[j - 2])) / TWO;
+      lnrad = (std::log(rad[j - 1]) + std::log(rad[j - 2])) / TWO;
+    }
+    d_lagr[j - 1] = d_eul[j - 1] * std::pow(dconst, TWO) * std::exp(TWO * (TWO * lnrad + lnrho));
+  }
+}
+
+// tridag with 1-based arrays as in the reference; returns nonzero for a zero pivot
+static int tridag_ref(const vector<double> &a, const vector<double> &b, const vector<double> &c,
+                      const vector<double> &r, vector<double> &u, int n) {
+  vector<double> gam(n + 1, ZERO);
+  if (b[1] == ZERO) return 1;
+  double bet = b[1];
+  u[1] = r[1] / bet;
+  for (int j = 2; j <= n; ++j) {
+    gam[j] = c[j - 1] / bet;
+    bet = b[j] - a[j] * gam[j];
+    if (bet == ZERO) return 2;
+    u[j] = (r[j] - a[j] * u[j - 1]) / bet;
+  }
+  for (int j = n - 1; j >= 1; --j) u[j] = u[j] - gam[j + 1] * u[j + 1];
+  return 0;
+}
+
+int oracle_mix_diffusion(int32_t m, int32_t nsp, double *X, int32_t ldx, const double *xm_in, const double *dq_in,
+                         double *d_io, double h, double sig, int32_t mesa, const uint8_t *consider) {
+  if (m < 2) return -1;
+  vector<double> a(m + 1, ZERO), b(m + 1, ZERO), c(m + 1, ZERO), D(m + 1, ZERO);
+  for (int j = 1; j <= m; ++j) D[j] = d_io[j - 1];
+  if (!mesa) {
+    vector<double> xm(m + 1);
+    for (int j = 1; j <= m; ++j) xm[j] = xm_in[j - 1];
+    double xr = xm[2] - xm[1], alpha = D[2] * h / (xr * xr);
+    if (sig < alpha) alpha = sig;
+    a[1] = ZERO; b[1] = ONE + alpha; c[1] = -ONE * alpha;
+    for (int j = 2; j <= m - 1; ++j) {
+      const double xl = xm[j] - xm[j - 1];
+      xr = xm[j + 1] - xm[j];
+      const double xmm = HALF * (xm[j + 1] - xm[j - 1]);
+      alpha = h / xmm;
+      if (sig < D[j + 1] * alpha / xr) D[j + 1] = sig / alpha * xr;
+      a[j] = -ONE * D[j] * alpha / xl;
+      b[j] = ONE + (D[j + 1] / xr + D[j] / xl) * alpha;
+      c[j] = -ONE * D[j + 1] * alpha / xr;
+      if (xl == ZERO || xr == ZERO) return -2;
+    }
+    const double xl = xm[m] - xm[m - 1];
+    alpha = D[m] * h / (xl * xl);
+    a[m] = -ONE * alpha; b[m] = ONE + alpha; c[m] = ZERO;
+    if (xl == ZERO || xr == ZERO) return -2;
+  } else {
+    vector<double> dq(m + 1), dr(m + 1, ZERO);
+    for (int j = 1; j <= m; ++j) dq[j] = dq_in[j - 1];
+    if (!(dq[1] > ZERO)) return -2;
+    auto reduce = [&](double alpha, double onedxr, double &dc) {
+      if (alpha * onedxr * dc > sig) dc = sig / (alpha * onedxr);
+    };
+    dr[1] = D[1];
+    double xr = dq[1], alpha = h / xr, term_c = ONE / xr, dc = D[2];
+    reduce(alpha, term_c, dc);
+    dr[2] = dc;
+    a[1] = ZERO; b[1] = ONE + term_c * alpha * dr[2]; c[1] = -ONE * term_c * alpha * dr[2];
+    for (int j = 2; j <= m - 1; ++j) {
+      const double xl = dq[j - 1];
+      xr = dq[j];
+      const double xmm = HALF * (dq[j] + dq[j - 1]);
+      alpha = h / xmm;
+      const double term_a = ONE / xl;
+      term_c = ONE / xr;
+      dc = D[j + 1];
+      reduce(alpha, term_c, dc);
+      dr[j + 1] = dc;
+      const double term_b = term_c * dr[j + 1] + term_a * dr[j];
+      a[j] = -ONE * term_a * dr[j] * alpha;
+      b[j] = ONE + term_b * alpha;
+      c[j] = -ONE * term_c * dr[j + 1] * alpha;
+    }
+    const double xl = dq[m];
+    alpha = h / (xl * xl);
+    a[m] = -ONE * alpha * D[m]; b[m] = ONE + alpha * D[m]; c[m] = ZERO;
+  }
+  vector<double> r(m + 1), u(m + 1);
+  for (int s = 0; s < nsp - 1; ++s) {
+    if (consider && !consider[s]) continue;
+    for (int j = 1; j <= m; ++j) r[j] = X[(size_t)(j - 1) * ldx + s];
+    const int e = tridag_ref(a, b, c, r, u, m);
+    if (e) return -3;
+    for (int j = 1; j <= m; ++j) X[(size_t)(j - 1) * ldx + s] = u[j];
+  }
+  for (int j = 1; j <= m; ++j) d_io[j - 1] = D[j];
+  return 0;
+}
 void oracle_set_rhs_noise(void *net, int32_t seed) { ((Net *)net)->rhs_noise = seed < 0 ? -1 : seed; }
 void oracle_set_lu_permute(void *net, int32_t seed) { ((Net *)net)->lu_permute = seed < 0 ? -1 : seed; }
 

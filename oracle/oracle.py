@@ -48,6 +48,9 @@ def load():
     L.oracle_sortedsum.restype = d
     L.oracle_set_rhs_noise.argtypes = [vp, i32]
     L.oracle_set_lu_permute.argtypes = [vp, i32]
+    L.oracle_mix_d_lagrangian.argtypes = [i32, vp, vp, vp, vp]
+    L.oracle_mix_diffusion.argtypes = [i32, i32, vp, i32, vp, vp, vp, d, d, i32, vp]
+    L.oracle_mix_diffusion.restype = i32
     L.oracle_nse.argtypes = [vp, i32, vp, vp, vp, vp, i32, vp, vp, vp, vp]
     L.oracle_integrate_trajectories.argtypes = [vp, i32, i32, vp, i32, vp, vp, vp, vp, vp, vp, vp, i32]
     _L = L
@@ -182,6 +185,31 @@ class Oracle:
     def calculate_ye(self, X):
         x = np.ascontiguousarray(X, dtype=np.float64)
         return self.L.oracle_calculate_ye(self.h, _p(x))
+
+
+def mix_d_lagrangian(d_eul, rho, rad):
+    """mix_calculate_D_Lagrangian (mixing.F90:60-98) on the CPU."""
+    L = load()
+    d_eul, rho, rad = (np.ascontiguousarray(v, np.float64) for v in (d_eul, rho, rad))
+    out = np.zeros(d_eul.size)
+    L.oracle_mix_d_lagrangian(d_eul.size, _p(d_eul), _p(rho), _p(rad), _p(out))
+    return out
+
+
+def mix_diffusion(X, d_lagr, dzeit, sig_term_limit, xm=None, dq=None, consider=None):
+    """mixdiff08 (mixing.F90:104-146) on the CPU: one diffusion step of X[m, nsp] (shells x species)
+    by matrixdiffus on xm, or matrixdiffus_mesa on dq when dq is given. Returns (X after the step,
+    d_lagr as the matrix routine limited it, status: 0, or < 0 for a zero width or pivot)."""
+    L = load()
+    X = np.array(X, dtype=np.float64, order="C", copy=True)
+    d = np.array(d_lagr, dtype=np.float64, copy=True)
+    mesa = dq is not None
+    xm_ = None if mesa else np.ascontiguousarray(xm, np.float64)
+    dq_ = np.ascontiguousarray(dq, np.float64) if mesa else None
+    cons = None if consider is None else np.ascontiguousarray(consider, np.uint8)
+    st = L.oracle_mix_diffusion(X.shape[0], X.shape[1], _p(X), X.shape[1], _p(xm_), _p(dq_), _p(d), float(dzeit),
+                                float(sig_term_limit), int(mesa), _p(cons))
+    return X, d, st
 
 
 def sortedsum(a) -> float:
