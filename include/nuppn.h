@@ -277,22 +277,26 @@ nuppn_status nuppn_mix_d_lagrangian(int32_t m, const double *d_eul, const double
                                     double *d_lagr);
 
 /* mixdiff08 (mixing.F90:104-146): one fully implicit diffusion step of length dzeit over m shells for
- * the abundances X[m][ldx] (shell-major, ldx >= nsp), every species 0 .. nsp-2 whose consider[] is
- * nonzero (all when consider is NULL; the last slot is left alone, as mixdiff08 loops to NSP-1).
- * mesa = 0: matrixdiffus on the mass coordinates xm[m] (code_source GNV / EVL); mesa = 1:
- * matrixdiffus_mesa on the shell masses dq[m] (MES). d_lagr[m] (host) is limited in place by
- * sig_term_limit as those routines limit it. The matrix and its factorization are built on the host;
- * the substitutions run on the GPU, one thread per species, with tridag's operations in its order
- * (equal to the reference bit for bit). NUPPN_ERR_ARG for a zero pivot or a zero shell width. */
-nuppn_status nuppn_mix_diffusion(int32_t m, int32_t nsp, double *X, int32_t ldx, const double *xm, const double *dq,
-                                 double *d_lagr, double dzeit, double sig_term_limit, int32_t mesa,
-                                 const uint8_t *consider);
+ * the abundances X, element (shell j, species s) at X[j * shell_stride + s * species_stride]: either
+ * rows of species (species_stride 1, shell_stride >= nsp) or columns of shells (shell_stride 1,
+ * species_stride >= m; mppnp's yps(msl, nsp) passes shell_stride 1, species_stride msl). Every species
+ * 0 .. nsp-2 whose consider[] is nonzero is mixed (all when consider is NULL; the last slot is left
+ * alone, as mixdiff08 loops to NSP-1). mesa = 0: matrixdiffus on the mass coordinates xm[m]
+ * (code_source GNV / EVL); mesa = 1: matrixdiffus_mesa on the shell masses dq[m] (MES). d_lagr[m]
+ * (host) is limited in place by sig_term_limit as those routines limit it. The matrix and its
+ * factorization are built on the host; the substitutions run on the GPU, one thread per species, with
+ * tridag's operations in its order (equal to the reference bit for bit). NUPPN_ERR_ARG for a zero
+ * pivot, a zero shell width or another layout. */
+nuppn_status nuppn_mix_diffusion(int32_t m, int32_t nsp, double *X, int64_t shell_stride, int64_t species_stride,
+                                 const double *xm, const double *dq, double *d_lagr, double dzeit,
+                                 double sig_term_limit, int32_t mesa, const uint8_t *consider);
 
 /* The same on device-resident abundances d_X, ordered on `stream` (a cudaStream_t, NULL: the default
  * stream); returns when the step is done. */
-nuppn_status nuppn_mix_diffusion_device(int32_t m, int32_t nsp, double *d_X, int32_t ldx, const double *xm,
-                                        const double *dq, double *d_lagr, double dzeit, double sig_term_limit,
-                                        int32_t mesa, const uint8_t *consider, void *stream);
+nuppn_status nuppn_mix_diffusion_device(int32_t m, int32_t nsp, double *d_X, int64_t shell_stride,
+                                        int64_t species_stride, const double *xm, const double *dq, double *d_lagr,
+                                        double dzeit, double sig_term_limit, int32_t mesa, const uint8_t *consider,
+                                        void *stream);
 
 /* -- tppnp's binary trajectory input (traj_data_bin_init / read_bin_trajectory,
  *    frames/tppnp/source/traj_data.F90:73-168): a stream file of the machine's byte order. Host only. */

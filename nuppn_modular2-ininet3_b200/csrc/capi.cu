@@ -577,21 +577,30 @@ nuppn_status nuppn_write_flux(const char *path, int32_t nreac, const int32_t *k,
 }  // extern "C"
 
 namespace nuppn {
-cudaError_t launch_mix_columns(int m, int ncol, double *X, int ldx, const double *a, const double *gam,
-                               const double *bet, const unsigned char *cons, cudaStream_t stream);
+cudaError_t launch_mix_columns(int m, int ncol, double *X, long long shell_stride, long long species_stride,
+                               const double *a, const double *gam, const double *bet, const unsigned char *cons,
+                               cudaStream_t stream);
 }
 
 namespace {
 
 // The step's matrix and factorization for nuppn_mix_diffusion*; d_lagr is limited in place as
-// matrixdiffus limits it.
-nuppn_status mix_prepare(int32_t m, int32_t nsp, int32_t ldx, const double *xm, const double *dq, double *d_lagr,
-                         double dzeit, double sig, int32_t mesa, std::vector<double> &a, std::vector<double> &gam,
-                         std::vector<double> &bet) {
-  if (m < 2 || nsp < 1 || ldx < nsp || !d_lagr || (mesa ? !dq : !xm)) {
-    set_error("nuppn_mix_diffusion: m >= 2, ldx >= nsp >= 1, d_lagr and xm (or dq with mesa) required");
+// matrixdiffus limits it. The abundances are either rows of species (species_stride 1, shell_stride >=
+// nsp) or columns of shells (shell_stride 1, species_stride >= m, mppnp's yps(msl, nsp)); *extent is the
+// elements the array spans.
+nuppn_status mix_prepare(int32_t m, int32_t nsp, int64_t shell_stride, int64_t species_stride, const double *xm,
+                         const double *dq, double *d_lagr, double dzeit, double sig, int32_t mesa,
+                         std::vector<double> &a, std::vector<double> &gam, std::vector<double> &bet,
+                         int64_t *extent) {
+  const bool rows = species_stride == 1 && shell_stride >= nsp;
+  const bool cols = shell_stride == 1 && species_stride >= m;
+  if (m < 2 || nsp < 1 || !(rows || cols) || !d_lagr || (mesa ? !dq : !xm)) {
+    set_error("nuppn_mix_diffusion: m >= 2, nsp >= 1, rows of species (species_stride 1, shell_stride >= nsp) "
+              "or columns of shells (shell_stride 1, species_stride >= m), d_lagr and xm (or dq with mesa) "
+              "required");
     return NUPPN_ERR_ARG;
   }
+  *extent = (int64_t)(m - 1) * shell_stride + (int64_t)(nsp - 1) * species_stride + 1;
   std::vector<double> b, c;
   std::string err = mix_matrix(m, xm, dq, d_lagr, dzeit, sig, mesa != 0, a, b, c);
   if (err.empty()) err = tridag_factor(m, a, b, c, gam, bet);
@@ -613,12 +622,15 @@ nuppn_status nuppn_mix_d_lagrangian(int32_t m, const double *d_eul, const double
   return NUPPN_OK;
 }
 
-nuppn_status nuppn_mix_diffusion_device(int32_t m, int32_t nsp, double *d_X, int32_t ldx, const double *xm,
-                                        const double *dq, double *d_lagr, double dzeit, double sig_term_limit,
-                                        int32_t mesa, const uint8_t *consider, void *stream) {
+nuppn_status nuppn_mix_diffusion_device(int32_t m, int32_t nsp, double *d_X, int64_t shell_stride,
+                                        int64_t species_stride, const double *xm, const double *dq, double *d_lagr,
+                                        double dzeit, double sig_term_limit, int32_t mesa, const uint8_t *consider,
+                                        void *stream) {
   if (!d_X) { set_error("null argument"); return NUPPN_ERR_ARG; }
   std::vector<double> a, gam, bet;
-  const nuppn_status st = mix_prepare(m, nsp, ldx, xm, dq, d_lagr, dzeit, sig_term_limit, mesa, a, gam, bet);
+  int64_t extent = 0;
+  const nuppn_status st = mix_prepare(m, nsp, shell_stride, species_stride, xm, dq, d_lagr, dzeit, sig_term_limit,
+                                      mesa, a, gam, bet, &extent);
   if (st != NUPPN_OK) return st;
   cudaStream_t s = (cudaStream_t)stream;
   const size_t vb = (size_t)m * sizeof(double);
@@ -631,7 +643,8 @@ nuppn_status nuppn_mix_diffusion_device(int32_t m, int32_t nsp, double *d_X, int
   if (e == cudaSuccess) e = cudaMemcpyAsync(db, bet.data(), vb, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess && dc) e = cudaMemcpyAsync(dc, consider, (size_t)nsp, cudaMemcpyHostToDevice, s);
   // mixdiff08 (mixing.F90:131-140) mixes species 1 .. NSP-1: the last slot is left alone
-  if (e == cudaSuccess) e = nuppn::launch_mix_columns(m, nsp - 1, d_X, ldx, da, dg, db, dc, s);
+  if (e == cudaSuccess)
+    e = nuppn::launch_mix_columns(m, nsp - 1, d_X, shell_stride, species_stride, da, dg, db, dc, s);
   const cudaError_t f = cudaFreeAsync(buf, s);
   if (e == cudaSuccess) e = f;
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the host vectors of the copies go out of scope
@@ -642,23 +655,25 @@ nuppn_status nuppn_mix_diffusion_device(int32_t m, int32_t nsp, double *d_X, int
   return NUPPN_OK;
 }
 
-nuppn_status nuppn_mix_diffusion(int32_t m, int32_t nsp, double *X, int32_t ldx, const double *xm, const double *dq,
-                                 double *d_lagr, double dzeit, double sig_term_limit, int32_t mesa,
-                                 const uint8_t *consider) {
+nuppn_status nuppn_mix_diffusion(int32_t m, int32_t nsp, double *X, int64_t shell_stride, int64_t species_stride,
+                                 const double *xm, const double *dq, double *d_lagr, double dzeit,
+                                 double sig_term_limit, int32_t mesa, const uint8_t *consider) {
   if (!X) { set_error("null argument"); return NUPPN_ERR_ARG; }
+  int64_t extent = 0;
   {  // the matrix and its factorization first, on a copy of d_lagr: argument errors need no GPU
     std::vector<double> a, gam, bet, dcopy(d_lagr ? d_lagr : nullptr, d_lagr ? d_lagr + std::max(m, 0) : nullptr);
-    const nuppn_status st = mix_prepare(m, nsp, ldx, xm, dq, d_lagr ? dcopy.data() : nullptr, dzeit, sig_term_limit,
-                                        mesa, a, gam, bet);
+    const nuppn_status st = mix_prepare(m, nsp, shell_stride, species_stride, xm, dq, d_lagr ? dcopy.data() : nullptr,
+                                        dzeit, sig_term_limit, mesa, a, gam, bet, &extent);
     if (st != NUPPN_OK) return st;
   }
-  const size_t bytes = (size_t)m * ldx * sizeof(double);
+  const size_t bytes = (size_t)extent * sizeof(double);
   double *dX = nullptr;
   CK(cudaMalloc((void **)&dX, bytes));
   cudaError_t e = cudaMemcpy(dX, X, bytes, cudaMemcpyHostToDevice);
   nuppn_status st = NUPPN_ERR_CUDA;
   if (e == cudaSuccess) {
-    st = nuppn_mix_diffusion_device(m, nsp, dX, ldx, xm, dq, d_lagr, dzeit, sig_term_limit, mesa, consider, nullptr);
+    st = nuppn_mix_diffusion_device(m, nsp, dX, shell_stride, species_stride, xm, dq, d_lagr, dzeit, sig_term_limit,
+                                    mesa, consider, nullptr);
     if (st == NUPPN_OK) {
       e = cudaMemcpy(X, dX, bytes, cudaMemcpyDeviceToHost);
       if (e != cudaSuccess) {

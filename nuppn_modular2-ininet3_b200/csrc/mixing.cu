@@ -10,8 +10,12 @@
 //
 // Here the matrix and its factorization (tridag's bet and gam, the same for every species) are
 // built once on the host in the reference's order of operations, and the device does the
-// substitutions: one thread per species walks the shells down and back up, reading and writing
-// X[shell * ldx + species], so a warp's accesses are consecutive species of one shell. Every
+// substitutions: one thread per species walks the shells down and back up. The abundances are
+// addressed as X[shell * shell_stride + species * species_stride], so both a shell-major array
+// (species_stride 1: a warp reads consecutive species of one shell) and mppnp's own yps(msl, nsp)
+// (shell_stride 1, species_stride msl: each thread walks one contiguous column, 16 shells per 128-byte
+// line) are mixed in place. The recurrence is one FP64 divide per shell and step; the loads of the
+// right-hand side do not depend on it, so each thread keeps the next kMixAhead of them in flight. Every
 // operation is the one tridag performs, in its order, so the result equals the reference's bit for
 // bit (--fmad=false keeps r - a u unfused).
 #include <cuda_runtime.h>
@@ -31,20 +35,44 @@ inline void reduce_term(double alpha, double onedxr, double &d_coeff, double sig
   if (alpha * onedxr * d_coeff > sig) d_coeff = sig / (alpha * onedxr);
 }
 
-__global__ void k_mix_columns(int m, int ncol, double *X, int ldx, const double *a, const double *gam,
-                              const double *bet, const unsigned char *cons) {
+constexpr int kMixAhead = 8;
+
+__global__ void k_mix_columns(int m, int ncol, double *X, long long sh, long long sp, const double *a,
+                              const double *gam, const double *bet, const unsigned char *cons) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ncol || (cons && !cons[s])) return;
-  double *x = X + s;
-  double u = x[0] / bet[0];
-  x[0] = u;
-  for (int j = 1; j < m; ++j) {
-    u = (x[(size_t)j * ldx] - a[j] * u) / bet[j];
-    x[(size_t)j * ldx] = u;
+  double *x = X + (long long)s * sp;
+  double r[kMixAhead];
+  // forward: u(1) = r(1) / bet(1); u(j) = (r(j) - a(j) u(j-1)) / bet(j)
+#pragma unroll
+  for (int k = 0; k < kMixAhead; ++k) r[k] = k < m ? x[k * sh] : 0.0;
+  double u = 0.0;
+  for (int j0 = 0; j0 < m; j0 += kMixAhead) {
+#pragma unroll
+    for (int k = 0; k < kMixAhead; ++k) {
+      const int j = j0 + k;
+      if (j < m) {
+        const double rj = r[k];
+        r[k] = j + kMixAhead < m ? x[(long long)(j + kMixAhead) * sh] : 0.0;
+        u = j == 0 ? rj / bet[0] : (rj - a[j] * u) / bet[j];
+        x[(long long)j * sh] = u;
+      }
+    }
   }
-  for (int j = m - 2; j >= 0; --j) {
-    u = x[(size_t)j * ldx] - gam[j + 1] * u;
-    x[(size_t)j * ldx] = u;
+  // back: u(j) = u(j) - gam(j+1) u(j+1), j = m-2 .. 0 (u holds u(m-1))
+#pragma unroll
+  for (int k = 0; k < kMixAhead; ++k) r[k] = m - 2 - k >= 0 ? x[(long long)(m - 2 - k) * sh] : 0.0;
+  for (int j0 = m - 2; j0 >= 0; j0 -= kMixAhead) {
+#pragma unroll
+    for (int k = 0; k < kMixAhead; ++k) {
+      const int j = j0 - k;
+      if (j >= 0) {
+        const double rj = r[k];
+        r[k] = j - kMixAhead >= 0 ? x[(long long)(j - kMixAhead) * sh] : 0.0;
+        u = rj - gam[j + 1] * u;
+        x[(long long)j * sh] = u;
+      }
+    }
   }
 }
 
@@ -149,11 +177,13 @@ std::string tridag_factor(int m, const std::vector<double> &a, const std::vector
   return std::string();
 }
 
-cudaError_t launch_mix_columns(int m, int ncol, double *X, int ldx, const double *a, const double *gam,
-                               const double *bet, const unsigned char *cons, cudaStream_t stream) {
+cudaError_t launch_mix_columns(int m, int ncol, double *X, long long shell_stride, long long species_stride,
+                               const double *a, const double *gam, const double *bet, const unsigned char *cons,
+                               cudaStream_t stream) {
   if (ncol <= 0) return cudaSuccess;
-  const int block = 128, grid = (ncol + block - 1) / block;
-  k_mix_columns<<<grid, block, 0, stream>>>(m, ncol, X, ldx, a, gam, bet, cons);
+  // one warp per CTA: the ~1100 columns of a large network spread over ~35 SMs instead of ~9
+  const int block = 32, grid = (ncol + block - 1) / block;
+  k_mix_columns<<<grid, block, 0, stream>>>(m, ncol, X, shell_stride, species_stride, a, gam, bet, cons);
   return cudaGetLastError();
 }
 

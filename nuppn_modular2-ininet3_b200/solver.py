@@ -64,8 +64,8 @@ def load_library():
     L.nuppn_write_flux.argtypes = [C.c_char_p, i32, vp, vp, vp, vp, vp, vp]
     L.nuppn_tppnp_header.argtypes = [C.c_char_p, vp, vp, vp]
     L.nuppn_mix_d_lagrangian.argtypes = [i32, vp, vp, vp, vp]
-    L.nuppn_mix_diffusion.argtypes = [i32, i32, vp, i32, vp, vp, vp, d, d, i32, vp]
-    L.nuppn_mix_diffusion_device.argtypes = [i32, i32, vp, i32, vp, vp, vp, d, d, i32, vp, vp]
+    L.nuppn_mix_diffusion.argtypes = [i32, i32, vp, C.c_int64, C.c_int64, vp, vp, vp, d, d, i32, vp]
+    L.nuppn_mix_diffusion_device.argtypes = [i32, i32, vp, C.c_int64, C.c_int64, vp, vp, vp, d, d, i32, vp, vp]
     L.nuppn_tppnp_next.argtypes = [C.c_char_p, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.nuppn_launch_count.argtypes = [vp]
     L.nuppn_launch_count.restype = i64
@@ -386,41 +386,51 @@ def mix_d_lagrangian(d_eul, rho, rad):
     return out
 
 
+def _mix_strides(shape, strides):
+    """(shell_stride, species_stride) in elements of a float64 array X[shells, species]."""
+    sh, sp = (st // 8 for st in strides)
+    return (sh, 1) if shape[1] == 1 and sp != 1 else ((1, sp) if shape[0] == 1 and sh != 1 else (sh, sp))
+
+
 def mix_diffusion(X, d_lagr, dzeit, sig_term_limit, xm=None, dq=None, consider=None):
     """mppnp's diffusive mixing step (mixdiff08, mixing.F90:104-146) on the GPU: X[m, nsp] (shells x
     species) after one fully implicit step of dzeit, by matrixdiffus on the mass coordinates xm, or
-    matrixdiffus_mesa on the shell masses dq when dq is given. Returns (X, d_lagr as limited by
-    sig_term_limit); X is not modified."""
+    matrixdiffus_mesa on the shell masses dq when dq is given. X may be C-ordered (rows of species) or
+    Fortran-ordered (columns of shells, mppnp's yps layout); the result keeps its order. Returns (X,
+    d_lagr as limited by sig_term_limit); X is not modified."""
     L = load_library()
-    X = np.array(X, dtype=np.float64, order="C", copy=True)
+    X = np.array(X, dtype=np.float64, order="F" if np.isfortran(X) else "C", copy=True)
     d = np.array(d_lagr, dtype=np.float64, copy=True)
     mesa = dq is not None
     xm_ = None if mesa else np.ascontiguousarray(xm, np.float64)
     dq_ = np.ascontiguousarray(dq, np.float64) if mesa else None
     cons = None if consider is None else np.ascontiguousarray(consider, np.uint8)
-    if L.nuppn_mix_diffusion(X.shape[0], X.shape[1], _p(X), X.shape[1], _p(xm_), _p(dq_), _p(d), float(dzeit),
+    sh, sp = _mix_strides(X.shape, X.strides)
+    if L.nuppn_mix_diffusion(X.shape[0], X.shape[1], _p(X), sh, sp, _p(xm_), _p(dq_), _p(d), float(dzeit),
                              float(sig_term_limit), int(mesa), _p(cons)) != 0:
         raise NuppnError(L.nuppn_last_error().decode())
     return X, d
 
 
 def mix_diffusion_device(X, d_lagr, dzeit, sig_term_limit, xm=None, dq=None, consider=None, stream=None):
-    """mix_diffusion on a device-resident float64 tensor X[m, ldx] (shells x species, nsp = the columns
-    to mix + 1 = X.shape[1]), in place, on `stream` (a torch.cuda.Stream or None). Returns d_lagr as
-    limited by sig_term_limit."""
+    """mix_diffusion on a device-resident float64 tensor X[m, nsp] (shells x species), in place, on
+    `stream` (a torch.cuda.Stream or None): rows of species (X.stride(1) == 1, e.g. a column slice of
+    a wider array) or columns of shells (X.stride(0) == 1, e.g. the transpose of a [nsp, msl] array).
+    Returns d_lagr as limited by sig_term_limit."""
     import torch
 
     L = load_library()
-    if not X.is_cuda or X.dtype != torch.float64 or X.dim() != 2 or X.stride(1) != 1:
-        raise NuppnError("mix_diffusion_device: X must be a 2-D float64 CUDA tensor with unit column stride")
+    if not X.is_cuda or X.dtype != torch.float64 or X.dim() != 2:
+        raise NuppnError("mix_diffusion_device: X must be a 2-D float64 CUDA tensor")
     d = np.array(d_lagr, dtype=np.float64, copy=True)
     mesa = dq is not None
     xm_ = None if mesa else np.ascontiguousarray(xm, np.float64)
     dq_ = np.ascontiguousarray(dq, np.float64) if mesa else None
     cons = None if consider is None else np.ascontiguousarray(consider, np.uint8)
-    sp = None if stream is None else C.c_void_p(stream.cuda_stream)
-    if L.nuppn_mix_diffusion_device(X.shape[0], X.shape[1], C.c_void_p(X.data_ptr()), X.stride(0), _p(xm_), _p(dq_),
-                                    _p(d), float(dzeit), float(sig_term_limit), int(mesa), _p(cons), sp) != 0:
+    sp_ = None if stream is None else C.c_void_p(stream.cuda_stream)
+    sh, sp = _mix_strides(tuple(X.shape), tuple(8 * st for st in X.stride()))
+    if L.nuppn_mix_diffusion_device(X.shape[0], X.shape[1], C.c_void_p(X.data_ptr()), sh, sp, _p(xm_), _p(dq_),
+                                    _p(d), float(dzeit), float(sig_term_limit), int(mesa), _p(cons), sp_) != 0:
         raise NuppnError(L.nuppn_last_error().decode())
     return d
 

@@ -106,3 +106,24 @@ def test_mixing_argument_errors_need_no_gpu(solver_mod):
         solver_mod.mix_diffusion(X[:1], d[:1], 1e3, 1e30, xm=xm[:1])  # one shell
     with pytest.raises(solver_mod.NuppnError):
         solver_mod.mix_diffusion(X, d, 1e3, 1e30, dq=np.zeros_like(dq))  # dq(1) = 0
+
+
+def test_mixing_layouts_need_no_gpu(solver_mod):
+    """Rows of species and mppnp's columns of shells are the two layouts; the strides come from the
+    array, and any other layout is refused before the GPU is touched."""
+    m, nsp = 8, 5
+    X = np.zeros((m, nsp))
+    assert solver_mod._mix_strides(X.shape, X.strides) == (nsp, 1)
+    F = np.asfortranarray(X)
+    assert solver_mod._mix_strides(F.shape, F.strides) == (1, m)
+    wide = np.zeros((m, nsp + 3))[:, :nsp]
+    assert solver_mod._mix_strides(wide.shape, wide.strides) == (nsp + 3, 1)
+    L = solver_mod.load_library()
+    xm, dq, d, _ = _case(6, m=m, nsp=nsp)
+    buf = np.zeros(4 * m * nsp)
+    for sh, sp in ((2, 2), (nsp - 1, 1), (1, m - 1), (0, 1), (1, 0)):
+        dd = d.copy()
+        st = L.nuppn_mix_diffusion(m, nsp, buf.ctypes.data, sh, sp, xm.ctypes.data, None, dd.ctypes.data, 1e3, 1e30,
+                                   0, None)
+        assert st != 0 and b"shell" in L.nuppn_last_error()
+        assert np.array_equal(dd, d)  # refused before d_lagr is limited
