@@ -366,27 +366,17 @@ struct Stager {
 // One fixed device array holds that entry point's zone counter (first 256 bytes) and its per-CTA
 // workspace slabs, so the call needs no cudaMalloc. In host code the name g_noalloc_scratch is
 // only a host-side stand-in for the symbol: kernels get the address cudaGetSymbolAddress returns,
-// looked up once per device with that device current.
+// looked up on every call with the device current, so neither a device reset nor another context
+// made current on that device leaves a stale address behind.
 static __device__ __align__(256) char g_noalloc_scratch[NUPPN_NOALLOC_SCRATCH_BYTES];
 
 namespace {
 constexpr size_t kNoAllocCounterBytes = 256;
-constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_mu;
-void *g_noalloc_addr[kMaxDevices] = {};
 
-// Device address of the scratch array on `device` (which must be current).
+// Device address of the scratch array in the current context (on `device`, which must be current).
 cudaError_t noalloc_scratch(int device, void **out) {
-  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[device]) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    g_noalloc_addr[device] = p;
-  }
-  *out = g_noalloc_addr[device];
-  return cudaSuccess;
+  if (device < 0) return cudaErrorInvalidDevice;
+  return cudaGetSymbolAddress(out, g_noalloc_scratch);
 }
 }  // namespace
 
