@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define NUPPN_ABI_VERSION 2
+#define NUPPN_ABI_VERSION 3
 
 typedef enum {
   NUPPN_OK = 0,
@@ -160,6 +160,9 @@ typedef struct nuppn_net_desc {
   /* constant rates */
   int32_t nconst;
   const double *const_rate;          /* [nconst]                                                 */
+  /* per VITAL rate: 0 = the template above, k = the reference's own formula for VITAL slot k
+   * (vital.F90:339-569; k in 1-9, 14-17, 73; slot 5 reads X of vt_xfac as XII(IPROT)); NULL: all 0 */
+  const int32_t *vt_form;            /* [vt_nrate]                                               */
 } nuppn_net_desc;
 
 typedef struct nuppn_net nuppn_net;
@@ -388,7 +391,7 @@ nuppn_status nuppn_integrate_multi_device(nuppn_net *const *nets, int32_t nnets,
                                           int32_t *d_ierr, nuppn_zone_stats *d_stats, int32_t *d_bd_state,
                                           void *stream);
 
-/* The trajectory loop of tppnp/* The trajectory loop of tppnp (frames/tppnp/source/tppnp.F90:131-168), batched: every zone z follows
+/* The trajectory loop of tppnp (frames/tppnp/source/tppnp.F90:131-168), batched: every zone z follows
  * its own trajectory of npts points time[z*npts + i], t9[...], rho[...]. The starting composition is
  * renormalised (Kahan sum) if |1 - sum X| > 1e-8; then for each interval i: Ye from the composition
  * (calculate_ye), integrate_network from point i to i+1, stop at the first interval with a non-zero

@@ -90,7 +90,7 @@ class NetDesc(C.Structure):
                 ("ff_nv", C.c_int32), ("ff_nt", C.c_int32), ("ff_nr", C.c_int32),
                 ("ff_t9coo", P_D), ("ff_rhocoo", P_D), ("ff_l10v", P_D),
                 ("kd_n", C.c_int32), ("kd_ne", C.c_int32), ("kd_e", P_D), ("kd_rate", P_D),
-                ("nconst", C.c_int32), ("const_rate", P_D)]
+                ("nconst", C.c_int32), ("const_rate", P_D), ("vt_form", P_I)]
 
 
 class ZoneStats(C.Structure):
@@ -178,5 +178,7 @@ def make_desc(net: sn.Network) -> NetDesc:
     D.kd_n, D.kd_ne = len(net.kd_rate), len(net.kd_e)
     D.kd_e, D.kd_rate = d(net.kd_e), d(net.kd_rate.reshape(-1))
     D.nconst, D.const_rate = len(net.const_rate), d(net.const_rate if len(net.const_rate) else [0.0])
+    vt_form = getattr(net, "vt_form", None)
+    D.vt_form = i(vt_form if vt_form is not None and len(vt_form) else np.zeros(max(len(net.vt_dpow), 1)))
     D._keep = keep
     return D

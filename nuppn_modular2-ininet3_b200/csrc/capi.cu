@@ -140,7 +140,7 @@ nuppn_status upload(nuppn_net *net) {
   P(H.irev); P(H.rev_sp); P(H.rev_kind); P(H.rev_mc); P(H.rev_Q);
   P(H.act_slot); P(H.act_k); P(H.act_ice);
   P(H.rl_first); P(H.rl_a); P(H.rl_info); P(H.rl_part); P(H.pt9); P(H.pval);
-  P(H.vfirst); P(H.vxfac); P(H.vterms); P(H.vdpow);
+  P(H.vfirst); P(H.vxfac); P(H.vterms); P(H.vdpow); P(H.vform);
   P(H.ngt8); P(H.ngl10t8); P(H.ngflag); P(H.ngane); P(H.ngl10v); P(H.ngndata);
   P(H.fft9); P(H.ffrho); P(H.ffl10v); P(H.kdE); P(H.kdcoef); P(H.constr);
   P(H.jrow); P(H.jcol); P(H.jdiag); P(H.jg_ptr); P(H.jg_item); P(H.dg_ptr); P(H.dg_item); P(H.dg_coef);
@@ -170,6 +170,7 @@ nuppn_status upload(nuppn_net *net) {
   D.rl_first = (const int *)nx(); D.rl_a = (const double *)nx(); D.rl_info = (const int *)nx();
   D.rl_part = (const int *)nx(); D.pt9 = (const double *)nx(); D.pval = (const double *)nx();
   D.vfirst = (const int *)nx(); D.vxfac = (const int *)nx(); D.vterms = (const double *)nx(); D.vdpow = (const double *)nx();
+  D.vform = (const int *)nx();
   D.ngt8 = (const double *)nx(); D.ngl10t8 = (const double *)nx(); D.ngflag = (const double *)nx();
   D.ngane = (const double *)nx(); D.ngl10v = (const double *)nx(); D.ngndata = (const int *)nx();
   D.fft9 = (const double *)nx(); D.ffrho = (const double *)nx(); D.ffl10v = (const double *)nx();

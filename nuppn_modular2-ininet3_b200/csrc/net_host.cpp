@@ -289,6 +289,13 @@ std::string build_host_net(const nuppn_net_desc &d, const nuppn_knobs &kn, HostN
   H.nv = d.vt_nrate;
   H.vfirst = cp(d.vt_first, H.nv + 1); H.vterms = cp(d.vt_terms, (size_t)d.vt_nterm * 5);
   H.vdpow = cp(d.vt_dpow, H.nv); H.vxfac = cp(d.vt_xfac, H.nv);
+  H.vform = d.vt_form ? cp(d.vt_form, H.nv) : std::vector<int>(H.nv, 0);
+  for (int i = 0; i < H.nv; ++i) {
+    const int f = H.vform[i];
+    const bool known = f == 0 || (f >= 1 && f <= 9) || (f >= 14 && f <= 17) || f == 73;
+    if (!known) return "descriptor: vt_form names a VITAL slot without a formula here (1-9, 14-17, 73)";
+    if (f == 5 && (H.vxfac[i] < 0 || H.vxfac[i] >= d.nsp)) return "descriptor: VITAL slot 5 needs vt_xfac = protons";
+  }
   H.ngk = d.ng_kgrid; H.ngn = d.ng_nreac; H.ngd = std::max(1, d.ng_ndmax);
   H.ngt8 = cp(d.ng_t8, H.ngk); H.ngflag = cp(d.ng_flag, H.ngn); H.ngndata = cp(d.ng_ndata, H.ngn);
   H.ngane = cp(d.ng_ane, (size_t)H.ngn * H.ngd); H.ngl10v = cp(d.ng_l10v, (size_t)H.ngk * H.ngn * H.ngd);

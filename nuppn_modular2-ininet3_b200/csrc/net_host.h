@@ -39,7 +39,7 @@ struct HostNet {
   int npart = 0;
   std::vector<double> pt9, pval;
   int nv = 0;
-  std::vector<int> vfirst, vxfac;
+  std::vector<int> vfirst, vxfac, vform;
   std::vector<double> vterms, vdpow;
   int ngk = 0, ngn = 0, ngd = 1;
   std::vector<double> ngt8, ngl10t8, ngflag, ngane, ngl10v;

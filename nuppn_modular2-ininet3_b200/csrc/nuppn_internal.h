@@ -50,7 +50,7 @@ struct DevNet {
   const double *pt9, *pval;  // [24], [npart*24]
   // VITAL templates
   int nv;
-  const int *vfirst, *vxfac;
+  const int *vfirst, *vxfac, *vform;
   const double *vterms, *vdpow;
   // NETGEN
   int ngk, ngn, ngd;

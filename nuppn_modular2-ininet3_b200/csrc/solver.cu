@@ -142,6 +142,99 @@ __device__ __forceinline__ double screening(const DevNet &N, const Screen &S, do
   return fmin(f, 1.e30);
 }
 
+// exv (vital.F90:2583-2593): exp with linear continuation beyond |x| = 200
+__device__ __forceinline__ double vital_exv(double x) {
+  if (x > 200.0) return (x - 200.0) * exp(200.0);
+  if (x < -200.0) return -exp(-200.0) / (x + 200.0);
+  return exp(x);
+}
+
+// The reference's own VITAL formulas (vital_calculate_rates, vital.F90:339-569) for the pp chains
+// (slots 1-9; 10-13 are off with IPPIV = 0) and the first CNO reactions (14-17, 73), at the clipped
+// t9 (<= 10), in the reference's order of operations. PROTOFAK is 1; FABE7 reads X(p) = xprot.
+// Not inlined: the integration kernels that evaluate rates keep their own register allocation.
+__device__ __noinline__ double vital_formula(int slot, double t9, double rho, double xprot) {
+  const double third = 1.0 / 3.0, fourth = 1.0 / 4.0, sixth = 1.0 / 6.0;
+  const double five_sixths = 5.0 * sixth, t9ppmax = 10.0, protofak = 1.0;
+  const double tp13 = pow(t9, third), tp14 = pow(t9, fourth), tp12 = tp14 * tp14, tp23 = tp13 * tp13;
+  const double tp32 = t9 * tp12, tp43 = t9 * tp13, tp53 = t9 * tp23;
+  const double tm13 = 1.0 / tp13, tm23 = 1.0 / tp23, tm32 = 1.0 / tp32, t9inv = 1.0 / t9;
+  if (slot == 5) {  // Be7(e-,nu)Li7, CF88, computed at every t9 (:340-343); the rest from T9 >= 0.001 (:364)
+    const double fabe7 = 0.5 * (1.0 + xprot);
+    double v = 1.34e-10 / tp12 * (1.0 - 0.537 * tp13 + 3.86 * tp23 + 0.0027 * t9inv * vital_exv(2.515e-03 * t9inv)) *
+               rho * fabe7;
+    if (t9 < 1.e-03 || t9 > t9ppmax) v = fmin(v, 1.51e-07);
+    return v;
+  }
+  if (!(t9 >= 0.001)) return 0.0;
+  if (slot <= 9) {  // pp I-III (:366-487), 1.2e-3 < T9 < T9PPMAX
+    if (!(t9 > 1.2e-3 && t9 < t9ppmax)) return 0.0;
+    switch (slot) {
+      case 1:
+        return (4.01e-15 * tm23 * vital_exv(-3.380 * tm13) * (1.0 + 0.123 * tp13 + 1.09 * tp23 + 0.938 * t9)) * rho *
+               protofak;
+      case 2:
+        return (2.24e+03 * tm23 * vital_exv(-3.720 * tm13) * (1.0 + 0.112 * tp13 + 3.38 * tp23 + 2.65 * t9)) * rho *
+               protofak;
+      case 3:
+        return (6.04e+10 * tm23 * vital_exv(-12.276 * tm13) *
+                (1.0 + 0.034 * tp13 - 0.522 * tp23 - 0.124 * t9 + 0.353 * tp43 + 0.213 * tp53)) *
+               rho;
+      case 4: {
+        const double tt = t9 / (1.0 + 4.95e-02 * t9), t56 = pow(tt, five_sixths), t13 = pow(tt, third);
+        return (5.61e+06 * t56 / tp32 * vital_exv(-12.826 / t13)) * rho;
+      }
+      case 6: {
+        const double t9a = t9 / (1.0 + 0.759 * t9), t9a13 = pow(t9a, third), t9a56 = pow(t9a, five_sixths);
+        return (1.096e+09 / tp23 * vital_exv(-8.472 / tp13) - 4.83e+08 * t9a56 / tp32 * vital_exv(-8.472 / t9a13) +
+                1.06e+10 / tp32 * vital_exv(-30.442 / t9)) *
+               rho * protofak;
+      }
+      case 7:
+      case 9: {
+        const double v7 =
+            (3.11e5 / tp23 * vital_exv(-10.262 / tp13) + 2.53e3 / tp32 * vital_exv(-7.306 / t9)) * rho * protofak;
+        if (slot == 7) return v7;
+        const double rev = 1.30e+10 * tp32 * vital_exv(-1.595 / t9) / (rho);
+        return rev * v7;
+      }
+      case 8: return 8.96e-1;
+      default: return 0.0;
+    }
+  }
+  if (!(t9 > 5.e-3)) return 0.0;  // CNO (:532-571)
+  switch (slot) {
+    case 14:
+    case 73: {
+      const double q = t9 / 0.46;
+      double v14 = (2.00e+07 * tm23 * vital_exv(-13.692 * tm13 - q * q) *
+                        (1.0 + 9.89 * t9 - 59.8 * t9 * t9 + 266.0 * t9 * t9 * t9) +
+                    1.00e+05 * tm32 * vital_exv(-4.913 / t9) + 4.24e+05 * tm32 * vital_exv(-21.62 / t9));
+      v14 = v14 * rho * protofak;
+      if (slot == 14) return v14;
+      return v14 / (rho * protofak) * 8.84e+09 * tp32 * vital_exv(-22.553 / t9);
+    }
+    case 15:
+      return (9.57e+07 * tm23 * vital_exv(-13.720 * tm13 - t9 * t9) * (1.0 + 3.56 * t9) +
+              1.50e+06 * tm32 * vital_exv(-5.930 / t9) + exp(-12.057 / t9) * 6.83e+05 / pow(t9, 0.864)) *
+             rho * protofak;
+    case 16: {  // RHO*PROTOFAK multiplies the second term only, as the reference writes it
+      const double q = t9 / 1.191;
+      return 4.04e+07 * tm23 * vital_exv(-15.202 * tm13 - q * q) *
+                 (1.0 + 0.027 * tp13 - 0.803 * tp23 - 0.154 * t9 + 5.00 * tp43 + 2.44 * tp53) +
+             2.43e+05 * tm32 * vital_exv(-6.348 / t9) * rho * protofak;
+    }
+    case 17: {
+      const double q = t9 / 3.294;
+      return (4.90e7 / tp23 * vital_exv(-15.228 / tp13 - q * q) *
+                  (1.0 + 0.027 * tp13 - 0.778 * tp23 - 0.149 * t9 + 0.261 * tp43 + 0.127 * tp53) +
+              2.37e3 / tp32 * vital_exv(-3.011 / t9) + 2.19e4 * vital_exv(-12.530 / t9)) *
+             rho * protofak;
+    }
+    default: return 0.0;
+  }
+}
+
 // evaluate_all_rates for the CTA's zone; y = mass fractions (read for screening and VITAL)
 __device__ void dev_eval_rates(const DevNet &N, const Ws &W, double t9, double rho, double ye, const double *y,
                                double *sred) {
@@ -288,6 +381,10 @@ __device__ void dev_eval_rates(const DevNet &N, const Ws &W, double t9, double r
         int i = N.sidx[l];
         switch (N.src[l]) {
           case NUPPN_SRC_VITAL: {
+            if (N.vform[i] > 0) {
+              v = vital_formula(N.vform[i], tv, rho, N.vxfac[i] >= 0 ? y[N.vxfac[i]] : 0.0);
+              break;
+            }
             double s = 0.0;
             for (int t = N.vfirst[i]; t < N.vfirst[i + 1]; ++t) {
               const double *c = N.vterms + (size_t)t * 5;

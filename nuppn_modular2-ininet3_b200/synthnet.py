@@ -178,6 +178,8 @@ class Network:
     kd_rate: np.ndarray        # [nkad, ne]
     # constant rates
     const_rate: np.ndarray
+    # per VITAL rate: 0 = the template above, k = the reference's own formula for VITAL slot k
+    vt_form: np.ndarray | None = None
 
     @property
     def nsp(self):
@@ -227,11 +229,21 @@ def database_isotopes(database: str, nnn: int):
     return [(int(z[i]), int(a[i])) for i in range(nnn) if f[i]]
 
 
+# VITAL slots whose rate the library evaluates by the reference's own formula
+# (physics/source/vital.F90:339-569): the pp chains and the first CNO reactions
+VITAL_FORMULA_SLOTS = (1, 2, 3, 4, 5, 6, 7, 8, 9, 14, 15, 16, 17, 73)
+
+
 def build_network(nnn: int = 1107, seed: int = 20240611, name: str | None = None,
-                  database: str | None = None) -> Network:
+                  database: str | None = None, vital: str = "template") -> Network:
     """Build a synthetic network with ``nnn`` isotope-database entries (the reference's NNN). With
     ``database`` the isotopes are the reference database's (database_isotopes), else a synthetic band
-    around the valley of stability in the same Z-then-A order."""
+    around the valley of stability in the same Z-then-A order. ``vital="reference"`` puts the
+    reactions of VITAL_FORMULA_SLOTS in their slots with the reference's formulas as their rates (the
+    network loop then leaves those reactions to VITAL); the default keeps analytic templates."""
+    if vital not in ("template", "reference"):
+        raise ValueError("vital must be 'template' or 'reference'")
+    vital_ref = vital == "reference"  # the name vital is rebound to a helper below
     rng = np.random.default_rng(seed)
     isos = database_isotopes(database, nnn) if database else _isotope_list(nnn)
 
@@ -313,10 +325,35 @@ def build_network(nnn: int = 1107, seed: int = 20240611, name: str | None = None
              [(4.27e26, -1.5, -84.165, 0.0, 0.0)], 1.0, -1),
         47: ((ibe8, 1, g, 0, g, 0, ihe4, 2), 99, [(1.0e16, 0.0, 0.0, 0.0, 0.0)], 0.0, -1),
     }
+    vt_form = []
+    covered = set()  # (target Z, A, reaction type) that a formula slot carries
+    if vital_ref:
+        ib7, ib8, ili7 = pos[(4, 7)], pos[(5, 8)], pos[(3, 7)]
+        in13, ic13, in14 = pos[(7, 13)], pos[(6, 13)], pos[(7, 14)]
+        ref_defs = {
+            7: ((ib7, 1, iprot, 1, g, 0, ib8, 1), I_PG, (4, 7, I_PG)),
+            8: ((ib8, 1, g, 0, g, 0, ihe4, 2), 99, (5, 8, I_BP)),
+            9: ((ib8, 1, g, 0, iprot, 1, ib7, 1), I_GP, (5, 8, I_GP)),
+            14: ((ic12, 1, iprot, 1, g, 0, in13, 1), I_PG, (6, 12, I_PG)),
+            15: ((ic13, 1, iprot, 1, g, 0, in14, 1), I_PG, (6, 13, I_PG)),
+            73: ((in13, 1, g, 0, iprot, 1, ic12, 1), I_GP, (7, 13, I_GP)),
+        }
+        if (8, 14) in pos:
+            ref_defs[16] = ((in13, 1, iprot, 1, g, 0, pos[(8, 14)], 1), I_PG, (7, 13, I_PG))
+        if (8, 15) in pos:
+            ref_defs[17] = ((in14, 1, iprot, 1, g, 0, pos[(8, 15)], 1), I_PG, (7, 14, I_PG))
+        covered.add((3, 7, I_PA))  # Li7(p,a)He4 is slot 6
+        for slot, (k, ilab, cov) in ref_defs.items():
+            vital_defs[slot] = (k, ilab, [], 0.0, -1)
+            covered.add(cov)
     for slot in range(1, nrcp + 1):
         if slot in vital_defs:
             k, ilab, terms, dpow, xfac = vital_defs[slot]
+            if vital_ref and slot in VITAL_FORMULA_SLOTS:
+                terms, dpow = [], 0.0
+                xfac = iprot if slot == 5 else -1  # XII(IPROT) of FABE7
             vital(k, ilab, terms, dpow, xfac)
+            vt_form.append(slot if vital_ref and slot in VITAL_FORMULA_SLOTS else 0)
         else:
             add_reaction((g, 0, g, 0, g, 0, g, 0), 99, SRC_NONE, -1, cons=0)
 
@@ -442,6 +479,8 @@ def build_network(nnn: int = 1107, seed: int = 20240611, name: str | None = None
         if a <= 4:          # n, p, d, 3He, 4He react through the VITAL block only
             continue
         for rtype in range(1, 17):
+            if (z, a, rtype) in covered:
+                continue
             dz, da = prod_shift[rtype]
             prod = (z + dz, a + da)
             if prod not in pos or prod[1] <= 0 or prod == (z, a):
@@ -551,4 +590,5 @@ def build_network(nnn: int = 1107, seed: int = 20240611, name: str | None = None
         ff_t9coo=np.linspace(-2.0, 1.0, 13), ff_rhocoo=np.linspace(1.0, 11.0, 11),
         ff_l10v=np.array(ff_rows).reshape(-1, 13, 11),
         kd_e=kdE, kd_rate=pad(kd_rows, len(kdE)), const_rate=np.array(const_rate),
+        vt_form=np.array(vt_form, np.int32),
     )

@@ -204,7 +204,7 @@ struct Net {
   vector<double> pt9, pval;
   // vital
   int nv;
-  vector<int> vfirst, vxfac;
+  vector<int> vfirst, vxfac, vform;
   vector<double> vterms, vdpow;
   // netgen
   int ngk, ngn, ngd;
@@ -410,9 +410,68 @@ void reaclib_rates(Zone &Z, double t9in, double rhoin, double yein) {  // reacli
   }
 }
 
+double exv(double x) {  // vital.F90:2583-2593
+  if (x > 200.0) return (x - 200.0) * std::exp(200.0);
+  if (x < -200.0) return -std::exp(-200.0) / (x + 200.0);
+  return std::exp(x);
+}
+
+// vital_calculate_rates (vital.F90:239-569), the slots restated here: v(5) at every T9 (:340-343);
+// for T9 >= 0.001 (:364) and 1.2e-3 < T9 < T9PPMAX (:366) V(1) :379, V(2) :395, V(3) :419, V(4)
+// :442-445, V(6) :468-473, V(7) :478, V(9) :481-482, V(8) :487 (IPPIV = 0 leaves V(10)-V(13) zero);
+// for T9 > 5e-3 (:532) V(14) :540-543 (the second fit replaces the first), V(73) :548, V(15) :556-558
+// (likewise), V(16) :563-565, V(17) :568-571. Every other slot stays zero (:322).
+double vital_reference(int slot, double T9, double RHO, double xprot) {
+  const double THIRD = ONE / 3.0, FOURTH = ONE / 4.0, SIXTH = ONE / 6.0, FIVE_SIXTHS = 5.0 * SIXTH;
+  const double T9PPMAX = 10.0, PROTOFAK = ONE;
+  const double TP13 = std::pow(T9, THIRD), TP14 = std::pow(T9, FOURTH);
+  const double TP12 = TP14 * TP14, TP23 = TP13 * TP13, TP32 = T9 * TP12, TP43 = T9 * TP13, TP53 = T9 * TP23;
+  const double TM13 = ONE / TP13, TM23 = ONE / TP23, TM32 = ONE / TP32, t9inv = ONE / T9;
+  double V[74] = {0.0};
+  const double FABE7 = HALF * (ONE + xprot);
+  V[5] = 1.34e-10 / TP12 * (ONE - 0.537 * TP13 + 3.86 * TP23 + 0.0027 * t9inv * exv(2.515e-03 * t9inv)) * RHO * FABE7;
+  if (T9 < 1.e-03 || T9 > T9PPMAX) V[5] = std::min(V[5], 1.51e-07);
+  if (T9 >= 0.001) {
+    if (T9 > 1.2e-3 && T9 < T9PPMAX) {
+      V[1] = (4.01e-15 * TM23 * exv(-3.380 * TM13) * (ONE + 0.123 * TP13 + 1.09 * TP23 + 0.938 * T9)) * RHO * PROTOFAK;
+      V[2] = (2.24e+03 * TM23 * exv(-3.720 * TM13) * (ONE + 0.112 * TP13 + 3.38 * TP23 + 2.65 * T9)) * RHO * PROTOFAK;
+      V[3] = (6.04e+10 * TM23 * exv(-12.276 * TM13) *
+              (1.0 + 0.034 * TP13 - 0.522 * TP23 - 0.124 * T9 + 0.353 * TP43 + 0.213 * TP53)) * RHO;
+      const double TT = T9 / (ONE + 4.95e-02 * T9);
+      const double T56 = std::pow(TT, FIVE_SIXTHS), T13 = std::pow(TT, THIRD);
+      V[4] = (5.61e+06 * T56 / TP32 * exv(-12.826 / T13)) * RHO;
+      const double T9A = T9 / (ONE + 0.759 * T9);
+      const double T9A13 = std::pow(T9A, THIRD), T9A56 = std::pow(T9A, FIVE_SIXTHS);
+      V[6] = (1.096e+09 / TP23 * exv(-8.472 / TP13) - 4.83e+08 * T9A56 / TP32 * exv(-8.472 / T9A13) +
+              1.06e+10 / TP32 * exv(-30.442 / T9)) * RHO * PROTOFAK;
+      V[7] = (3.11e5 / TP23 * exv(-10.262 / TP13) + 2.53e3 / TP32 * exv(-7.306 / T9)) * RHO * PROTOFAK;
+      const double REV = 1.30e+10 * TP32 * exv(-1.595 / T9) / (RHO);
+      V[9] = REV * V[7];
+      V[8] = 8.96e-1;
+    }
+    if (T9 > 5.e-3) {
+      V[14] = (2.00e+07 * TM23 * exv(-13.692 * TM13 - (T9 / 0.46) * (T9 / 0.46)) *
+                   (1.0 + 9.89 * T9 - 59.8 * T9 * T9 + 266.0 * T9 * T9 * T9) +
+               1.00e+05 * TM32 * exv(-4.913 / T9) + 4.24e+05 * TM32 * exv(-21.62 / T9));
+      V[14] = V[14] * RHO * PROTOFAK;
+      V[73] = V[14] / (RHO * PROTOFAK) * 8.84e+09 * TP32 * exv(-22.553 / T9);
+      V[15] = (9.57e+07 * TM23 * exv(-13.720 * TM13 - T9 * T9) * (1 + 3.56 * T9) + 1.50e+06 * TM32 * exv(-5.930 / T9) +
+               std::exp(-12.057 / T9) * 6.83e+05 / std::pow(T9, 0.864)) * RHO * PROTOFAK;
+      V[16] = 4.04e+07 * TM23 * exv(-15.202 * TM13 - (T9 / 1.191) * (T9 / 1.191)) *
+                  (1.0 + 0.027 * TP13 - 0.803 * TP23 - 0.154 * T9 + 5.00 * TP43 + 2.44 * TP53) +
+              2.43e+05 * TM32 * exv(-6.348 / T9) * RHO * PROTOFAK;
+      V[17] = (4.90e7 / TP23 * exv(-15.228 / TP13 - (T9 / 3.294) * (T9 / 3.294)) *
+                   (ONE + 0.027 * TP13 - 0.778 * TP23 - 0.149 * T9 + 0.261 * TP43 + 0.127 * TP53) +
+               2.37e3 / TP32 * exv(-3.011 / T9) + 2.19e4 * exv(-12.530 / T9)) * RHO * PROTOFAK;
+    }
+  }
+  return (slot >= 1 && slot <= 73) ? V[slot] : 0.0;
+}
+
 double vital_rate(const Net &N, int r, double t9_in, double rho, const double *x) {
-  // analytic template: rho^dpow * xfac * sum c*T9^p*exp(d*T9^(-1/3) + f/T9 + g*T9)
   double t9 = std::min(t9_in, 10.0);  // vital.F90:230
+  if (N.vform[r] > 0) return vital_reference(N.vform[r], t9, rho, N.vxfac[r] >= 0 ? x[N.vxfac[r]] : 0.0);
+  // analytic template: rho^dpow * xfac * sum c*T9^p*exp(d*T9^(-1/3) + f/T9 + g*T9)
   double tm13 = ONE / std::pow(t9, THIRD);
   double s = 0.0;
   for (int t = N.vfirst[r]; t < N.vfirst[r + 1]; ++t) {
@@ -1721,6 +1780,7 @@ void *oracle_net_create(const nuppn_net_desc *d, const nuppn_knobs *kn) {
   N->nv = d->vt_nrate; N->vfirst = cp(d->vt_first, N->nv + 1);
   N->vterms = cp(d->vt_terms, (size_t)d->vt_nterm * 5); N->vdpow = cp(d->vt_dpow, N->nv);
   N->vxfac = cp(d->vt_xfac, N->nv);
+  N->vform = d->vt_form ? cp(d->vt_form, N->nv) : vector<int>(N->nv, 0);
   N->ngk = d->ng_kgrid; N->ngn = d->ng_nreac; N->ngd = d->ng_ndmax;
   N->ngt8 = cp(d->ng_t8, N->ngk); N->ngflag = cp(d->ng_flag, N->ngn);
   N->ngndata = cp(d->ng_ndata, N->ngn); N->ngane = cp(d->ng_ane, (size_t)N->ngn * N->ngd);
@@ -2035,3 +2095,7 @@ void oracle_set_rhs_noise(void *net, int32_t seed) { ((Net *)net)->rhs_noise = s
 void oracle_set_lu_permute(void *net, int32_t seed) { ((Net *)net)->lu_permute = seed < 0 ? -1 : seed; }
 
 }  // extern "C"
+
+extern "C" double oracle_vital_reference(int32_t slot, double t9, double rho, double xprot) {
+  return vital_reference(slot, std::min(t9, 10.0), rho, xprot);
+}

@@ -59,6 +59,8 @@ int oracle_nse(void *net, int32_t nz, const double *t9, const double *rho, const
                int32_t ldx, double *mu_p, double *mu_n, int32_t *iters, int32_t *ierr);
 /* sortedsum (utils.F90:481-501) with the NR heapsort indexx (sort.F90:73-127) */
 double oracle_sortedsum(const double *a, int32_t n);
+/* the reference's VITAL formula for slot 1-9, 14-17 or 73 at T9 (clipped to 10), rho, X(p); 0 otherwise */
+double oracle_vital_reference(int32_t slot, double t9, double rho, double xprot);
 
 #ifdef __cplusplus
 }

@@ -49,6 +49,8 @@ def load():
     L.oracle_set_rhs_noise.argtypes = [vp, i32]
     L.oracle_set_lu_permute.argtypes = [vp, i32]
     L.oracle_mix_d_lagrangian.argtypes = [i32, vp, vp, vp, vp]
+    L.oracle_vital_reference.argtypes = [i32, d, d, d]
+    L.oracle_vital_reference.restype = d
     L.oracle_mix_diffusion.argtypes = [i32, i32, vp, i32, vp, vp, vp, d, d, i32, vp]
     L.oracle_mix_diffusion.restype = i32
     L.oracle_nse.argtypes = [vp, i32, vp, vp, vp, vp, i32, vp, vp, vp, vp]
@@ -185,6 +187,11 @@ class Oracle:
     def calculate_ye(self, X):
         x = np.ascontiguousarray(X, dtype=np.float64)
         return self.L.oracle_calculate_ye(self.h, _p(x))
+
+
+def vital_reference(slot, t9, rho, xprot=0.0) -> float:
+    """The reference's own VITAL formula for one slot (vital.F90:339-571; slots 1-9, 14-17, 73)."""
+    return load().oracle_vital_reference(int(slot), float(t9), float(rho), float(xprot))
 
 
 def mix_d_lagrangian(d_eul, rho, rad):

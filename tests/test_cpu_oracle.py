@@ -228,7 +228,7 @@ def test_library_exports_header_symbols(solver_mod):
     L = solver_mod.load_library()
     for n in names:
         assert hasattr(L, n), n
-    assert L.nuppn_abi_version() == 2
+    assert L.nuppn_abi_version() == 3
 
 
 def test_no_cpu_fallback_in_product(solver_mod):
